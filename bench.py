@@ -1,0 +1,399 @@
+"""Throughput benchmark: chi2 evaluations per second (target x z x template).
+
+Workload (one "step"): 500 synthetic DESI-like targets (cameras b/r/z,
+P = 7958 pixels, 11-diagonal resolution, 5 % masked pixels) scanned against
+the full template set -- GALAXY (10 bases, 3311 z), QSO (4 bases, 3794 z,
+Inoue14 IGM) and 5 STAR subtypes (5 bases, 100 z) -- i.e. 7605 chi2
+evaluations per target, 3.8025 M per step.  A step runs the whole hot path:
+rebin + IGM bases for every template, target packing, and the fused scan
+(chi2, coefficients and [OII] penalty for every target, template and z).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank scans its own 500
+targets (weak scaling, no collective in the data path); the step time is the
+max over ranks.  ``--impl reference`` times the CPU restatement of redrock's
+scan (oracle/) on the host cores instead.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+D_BAND = 11
+WORKLOAD = "zscan-desi-500x(GALAXY3311+QSO3794+5xSTAR100)"
+
+
+def flops_per_eval(nb, npix):
+    """Algorithmic FLOPs of one chi2 evaluation in redrock's formulation:
+    R.T (2 D P n), weighted Gram (P n (n+1)), y (2 P n), solve (n^3/3 + 2n^2),
+    chi2 via b.c (2n)."""
+    return npix * nb * (2 * D_BAND + nb + 3) + nb ** 3 / 3.0 + 2 * nb ** 2 + 2 * nb
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_workload(ntarget, seed):
+    from redrock_b200 import synth
+    from redrock_b200 import targets as T
+    from redrock_b200 import templates as TM
+    tg = synth.make_targets(ntarget, seed=seed)
+    tset = synth.template_set()
+    rtg = T.from_synth(tg)
+    tms = [TM.from_synth(ts) for ts in tset]
+    return tg, rtg, tset, tms
+
+
+def evals_and_flops(rtg, tms):
+    ev = 0
+    fl = 0.0
+    for t in rtg:
+        npix = sum(len(s.wave) for s in t.spectra)
+        for tm in tms:
+            nz = len(tm.redshifts)
+            ev += nz
+            fl += nz * flops_per_eval(tm.nbasis, npix)
+    return ev, fl
+
+
+def measure_fp64_peak(L, torch):
+    from redrock_b200.device import stream_handle
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    blocks, iters = nsm * 8, 2000
+    L.rr_fma_peak(0, blocks, iters, out.data_ptr(), stream_handle())
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        L.rr_fma_peak(0, blocks, iters, out.data_ptr(), stream_handle())
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        best = max(best, 2.0 * 8 * 16 * iters * blocks * 256 / t / 1e12)
+    return best
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of the fused scan kernel from the committed ncu
+    summary (profiles/zscan_fused_traffic.json), if present."""
+    p = os.path.join(ROOT, "profiles", "zscan_fused_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("bytes_per_launch_full_workload")
+        except Exception:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from redrock_b200 import _lib, synth, zscan
+    from redrock_b200 import targets as T
+    from redrock_b200 import templates as TM
+    from redrock_b200.device import StatusWord
+    from redrock_b200.engine import (DeviceBasis, GridLayout, TargetBatch, TargetPack,
+                                     TemplateSource, run_fused)
+
+    torch.cuda.set_device(local_rank)
+    L = _lib.lib()
+    tg, rtg, tset, tms = make_workload(args.ntargets, seed=args.seed + 7919 * rank)
+    evals, flops = evals_and_flops(rtg, tms)
+    layout = GridLayout.from_dwave(synth.camera_grids())
+    srcs = [TemplateSource.from_template(tm) for tm in tms]
+    dbatch = TargetBatch(rtg, layout).to_device()
+    st = StatusWord()
+    ev_fused = []
+
+    def step(record):
+        bases = [DeviceBasis.build(s, layout, status=st) for s in srcs]
+        pack = TargetPack(dbatch, status=st)
+        if record:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        res, _ = run_fused(pack, bases, status=st)
+        if record:
+            e1.record()
+            ev_fused.append((e0, e1))
+        return res
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    st.check("warm-up")
+    launches_per_step = sum(len(layout.keys) for _ in srcs) + 2 + 1
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        step(True)
+    t1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    st.check("timed steps")
+    ms = t0.elapsed_time(t1) / args.steps
+    fused_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_fused]))
+    if world > 1:
+        v = torch.tensor([ms, fused_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        ms, fused_ms = float(v[0]), float(v[1])
+    value = world * evals / (ms / 1e3)
+
+    # ---- end to end through the public API, host buffers ------------------
+    e2e = None
+    if not args.no_e2e:
+        def e2e_step():
+            zscan._pack_cache.clear()
+            zscan._basis_cache.clear()
+            dtg = T.DistTargetsCopy(rtg)
+            dwave = dtg.wavegrids()
+            dts = [TM.DistTemplate(tm, dwave) for tm in tms]
+            res = zscan.calc_zchi2_targets(dtg, dts)
+            return res
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            e2e_step()
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms = a.elapsed_time(b) / args.steps
+        if world > 1:
+            v = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+            e2e_ms = float(v[0])
+        batch = TargetBatch(rtg, layout)
+        h2d = batch.nbytes + sum(s.nbytes for s in srcs) + sum(
+            2 * 8 * (n + 1) for n in layout.npix)
+        d2h = sum(len(rtg) * len(tm.redshifts) * (2 + tm.nbasis) * 8 for tm in tms)
+        e2e = {"value": world * evals / (e2e_ms / 1e3), "unit": "chi2 evals/s",
+               "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "path": "redrock_b200.zscan.calc_zchi2_targets(DistTargetsCopy, [DistTemplate x7])"
+                       " from host numpy arrays"}
+
+    if rank != 0:
+        return None
+    peak = measure_fp64_peak(L, torch)
+    fused_flops = flops
+    achieved = fused_flops / (fused_ms / 1e3) / 1e12
+    out = {
+        "metric": "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3",
+        "value": value, "unit": "chi2 evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded DESI-like targets and "
+        "templates, redrock_b200/synth.py)",
+        "config": {"workload": WORKLOAD, "targets_per_gpu": args.ntargets,
+                   "templates": [tm.full_type for tm in tms],
+                   "evals_per_step_per_gpu": evals, "pixels_per_target": 7958,
+                   "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
+                   "parallelism": f"targets sharded {world}-way, no collective"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic_from_profile(),
+                     "kernel": "zscan_fused_kernel",
+                     "kernel_ms": fused_ms, "flops_per_launch": fused_flops,
+                     "peak_source": "measured FP64 FMA peak (rr_fma_peak) on this GPU"},
+        "e2e": e2e,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement of redrock's scan (oracle), all host cores
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    seed, ntarget, zsub, barrier = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from redrock_b200 import synth
+    tg = synth.make_targets(ntarget, seed=seed)
+    tset = synth.template_set(zsub=zsub)
+    grids = synth.camera_grids()
+    bases = []
+    for ts in tset:
+        bases.append((ts, O.template_basis(ts.wave, ts.flux, ts.redshifts, grids, ts.igm_model),
+                      O.oii_template(ts.wave, ts.flux) if ts.spectype == "GALAXY" else None))
+    ospec = [[O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets)
+              for s in t.spectra] for t in tg]
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    evals = 0
+    for ts, tdata, oii in bases:
+        O.calc_zchi2(ospec, tdata, len(ts.redshifts), ts.flux.shape[0], OIItemplate=oii)
+        evals += len(tg) * len(ts.redshifts)
+    return evals, time.perf_counter() - t0
+
+
+def cpu_scan_sample(nproc, per_worker, zsub, seed=1):
+    """(evals/s, cores, sample description) of the oracle on host cores."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        barrier = mgr.Barrier(nproc) if nproc > 1 else None
+        with ctx.Pool(nproc) as pool:
+            res = pool.map(_cpu_worker, [(seed + i, per_worker, zsub, barrier)
+                                         for i in range(nproc)])
+    evals = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    sample = (f"{nproc} processes x {per_worker} targets x all 7 templates at every "
+              f"{zsub}th redshift ({evals} evals, {wall:.1f} s); bases built before timing")
+    return evals / wall, nproc, sample
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    ncpu = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, cores, sample = cpu_scan_sample(ncpu, args.ref_targets, args.ref_zsub, seed=100 + i)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    return {
+        "metric": "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3",
+        "impl": "reference", "value": value, "unit": "chi2 evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded DESI-like targets and templates)",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": value, "unit": "chi2 evals/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "chi2 evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ntargets", type=int, default=500)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-zsub", type=int, default=5)
+    ap.add_argument("--ref-targets", type=int, default=4)
+    args = ap.parse_args()
+    rank, world, local_rank = env_rank()
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+        if out is not None and world == 1 and not args.no_cpu_baseline:
+            v, cores, sample = cpu_scan_sample(os.cpu_count() or 1, args.ref_targets,
+                                               args.ref_zsub)
+            out["cpu_baseline"] = {"value": v, "unit": "chi2 evals/s", "cores": cores,
+                                   "kind": "port", "sample": sample}
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,235 @@
+/*
+ * redrock-b200: C ABI of the B200 redshift-scan engine.
+ *
+ * Every entry point takes plain device pointers, 64-bit sizes and a CUDA
+ * stream, returns an rr_status code, and allocates no device memory: the
+ * caller owns inputs, outputs and workspace (sizes are given by the
+ * rr_*_workspace_bytes queries or stated per call).  Calls are asynchronous
+ * on `stream`; the optional `status` argument is a device int that kernels
+ * set (first error wins) when they detect bad data or a bounded wait runs
+ * out, so the host can check it after synchronising.
+ *
+ * Reference interfaces replaced (redrock 0.22, py/redrock/...):
+ *   rr_trapz_rebin          rebin.py:212-378 trapz_rebin (batch form
+ *                           _trapz_rebin_batch rebin.py:178-209,
+ *                           _trapz_rebin_1d rebin.py:126-176)
+ *   rr_igm_transmission     igm.py:369-439 transmission_Lyman (array case;
+ *                           Inoue14 igm.py:105-318, Calura12/Kamble20
+ *                           igm.py:321-364)
+ *   rr_build_basis          templates.py:584-597 DistTemplate.__init__
+ *                           (rebin_template rebin.py:453-517 + IGM product)
+ *   rr_pack_targets         zscan.py:192-209 spectral_data and
+ *                           targets.py:85-89 Spectrum.Rcsr (device layout)
+ *   rr_zscan_fused          zscan.py:807-889 calc_zchi2 for every template
+ *                           at once (the inner loop of calc_zchi2_targets
+ *                           zscan.py:910-1105), incl. calc_negOII_penalty
+ *                           zscan.py:783-800
+ *   rr_pack_band_rows,
+ *   rr_zchi2_batch_plain    zscan.py:626-781 calc_zchi2_batch for one
+ *                           target (and zscan.py:213-243 calc_zchi2_one as
+ *                           nz = 1)
+ *   rr_negoii_penalty       zscan.py:783-800 calc_negOII_penalty
+ */
+#ifndef REDROCK_B200_H
+#define REDROCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* same type as cudaStream_t; NULL is the legacy default stream */
+typedef struct CUstream_st* rr_stream_t;
+
+enum rr_status {
+  RR_OK = 0,
+  RR_EINVAL = 1,   /* bad argument (shape, pointer, unsupported layout) */
+  RR_ERANGE = 2,   /* rebin edges outside the redshifted template range
+                      (redrock raises ValueError, rebin.py:340-341) */
+  RR_ECUDA = 3,    /* a CUDA runtime call failed; see rr_last_cuda_error */
+  RR_ETIMEOUT = 4, /* a bounded device-side wait gave up */
+  RR_ENOTSUP = 5   /* valid input this build does not handle */
+};
+
+enum rr_igm_model { /* igm.py:367 igm_models */
+  RR_IGM_NONE = 0,
+  RR_IGM_CALURA12 = 1,
+  RR_IGM_KAMBLE20 = 2,
+  RR_IGM_INOUE14 = 3
+};
+
+enum rr_solve_method { /* zscan.py:1107-1203 solve_matrices */
+  RR_SOLVE_PCA = 0,        /* linear solve; exactly singular -> HUGE_CHI2 */
+  RR_SOLVE_UNSUPPORTED = 1 /* every z gets HUGE_CHI2 and zero coefficients,
+                              as redrock does for NotImplementedError */
+};
+
+#define RR_HUGE_CHI2 9999999.0   /* zscan.py:18 */
+#define RR_HALF_BAND 5           /* resolution offsets handled: -5..5 */
+#define RR_LANES 32              /* targets per target block */
+#define RR_RW 12                 /* doubles per (pixel, lane): 11 band + 1 */
+#define RR_CHUNK 16              /* pixels per scan stage */
+#define RR_MAX_TEMPLATES 16
+#define RR_MAX_NBASIS 10
+
+int rr_version(void);
+const char* rr_status_string(int status);
+/* last cudaError_t seen by a call of this library on this thread */
+int rr_last_cuda_error(void);
+
+/* ------------------------------------------------------------------------
+ * Trapezoidal rebinning of y(x (1+z)) onto bin edges, for every z and basis.
+ *   x[nx] increasing; y[nbasis][nx]; edges[nbin+1]; z[nz]
+ *   out[nz][nbin][nbasis] (the (nz, nbin, nbasis) layout redrock uses)
+ * xmin/xmax/edge_min/edge_max are host copies of x[0]*(1+max z),
+ * x[nx-1]*(1+min z), edges[0], edges[nbin]; RR_ERANGE if
+ * edge_min < xmin or edge_max > xmax (rebin.py:330-341).  Results are bit
+ * identical to redrock's CPU path for the same doubles.
+ * ---------------------------------------------------------------------- */
+int rr_trapz_rebin(const double* x, int64_t nx, const double* y, int64_t nbasis,
+                   const double* edges, int64_t nbin, const double* z, int64_t nz,
+                   double xmin, double xmax, double edge_min, double edge_max,
+                   double* out, int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * IGM transmission T[nz][nwave] for observed wavelengths lobs[nwave] and
+ * redshifts z[nz]; model one of rr_igm_model (RR_IGM_NONE gives ones).
+ * ---------------------------------------------------------------------- */
+int rr_igm_transmission(int model, const double* z, int64_t nz, const double* lobs,
+                        int64_t nwave, double* out, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Basis builder: rebinned (and IGM-attenuated) template for every z on the
+ * union of the targets' wavelength grids, in the padded layout the scan
+ * kernels read:
+ *   basis[z][pix_stride][basis_stride]   (basis_stride >= nbasis, even)
+ * Grid g occupies padded pixels [pix_offset - 5, pix_offset + npix_pad + 5)
+ * with real pixels at [pix_offset, pix_offset + npix); everything else in
+ * that range (and the basis columns >= nbasis) is written as 0.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  const double* edges; /* device, npix + 1 */
+  const double* wave;  /* device, npix pixel centres (IGM is evaluated there) */
+  int64_t npix;
+  int64_t npix_pad;    /* npix rounded up to a multiple of RR_CHUNK */
+  int64_t pix_offset;  /* padded index of the first real pixel (>= 5) */
+  double edge_min;     /* host copy of edges[0] */
+  double edge_max;     /* host copy of edges[npix] */
+  int apply_igm;       /* 0: skip IGM for this grid (redrock's None return) */
+  int pad_;
+} rr_grid_desc;
+
+int rr_build_basis(const double* x, int64_t nx, const double* y, int64_t nbasis,
+                   const double* z, int64_t nz, double xmin, double xmax,
+                   const rr_grid_desc* grids /* host array */, int ngrid, int igm_model,
+                   int64_t pix_stride, int basis_stride, double* basis, int* status,
+                   rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Target packing for the fused scan.  Targets are grouped 32 to a block
+ * (one per lane); each block walks the same list of segments (one
+ * segment = one spectrum slot on one wavelength grid).  Output:
+ *   rw[nblock][npix_block][12][32]: rw[.,p,k,l] = sqrt(w_p) R[p, p+k-5]
+ *     (k < 11) and sqrt(w_p) f_p (k = 11) for the spectrum in (segment,
+ *     lane); zero where a lane has no spectrum in that segment.
+ *   fwf[nblock][32] = sum w f^2,  wsum[nblock][32] = sum w  (FP64).
+ * specs are grouped by target: target t owns specs[target_first[t] ..
+ * target_first[t+1]) (in redrock's spectrum order).  rw, fwf and wsum must
+ * be zeroed by the caller before the call.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int64_t npix;        /* pixels of this spectrum */
+  int64_t data_offset; /* offset of its (ndiag, npix) DIA data in rdata */
+  int64_t pix_offset;  /* offset of its pixels in ivar / flux */
+  int32_t ndiag;       /* diagonals stored */
+  int32_t diag_offset; /* offset of its ndiag offsets in roffsets */
+  int32_t block;       /* target block */
+  int32_t lane;        /* lane in the block */
+  int32_t segment;     /* segment index */
+  int32_t pad_;
+} rr_spectrum_desc;
+
+typedef struct {
+  int64_t npix_pad;     /* segment pixels rounded up to RR_CHUNK */
+  int64_t basis_offset; /* padded basis index of its first pixel */
+  int64_t rw_offset;    /* pixel offset of the segment in a block's rw */
+} rr_segment_desc;
+
+int rr_pack_targets(const rr_spectrum_desc* specs /* device */, int64_t nspec,
+                    const int64_t* target_first /* device, ntarget + 1 */, int64_t ntarget,
+                    const double* rdata, const int32_t* roffsets, const double* ivar,
+                    const double* flux, const rr_segment_desc* segs /* device */, int nseg,
+                    int64_t npix_block, int nblock, double* rw, double* fwf, double* wsum,
+                    int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Fused scan: chi2(z), coefficients(z) and the [OII] penalty for every
+ * (target, template, z) in one persistent launch.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  const double* basis;  /* [nz][pix_stride][basis_stride] from rr_build_basis */
+  int64_t pix_stride;
+  int32_t nz;
+  int32_t nbasis;       /* 1..RR_MAX_NBASIS */
+  int32_t basis_stride;
+  int32_t method;       /* rr_solve_method */
+  const double* prior;  /* nbasis*nbasis added to M before the solve, or NULL */
+  const double* oii;    /* nbasis sums of the [OII] template window, or NULL */
+  double* zchi2;        /* [nrows][nz] */
+  double* zcoeff;       /* [nrows][nz][nbasis] */
+  double* penalty;      /* [nrows][nz] (written only when oii != NULL) */
+} rr_scan_template;
+
+typedef struct {
+  const double* rw;              /* from rr_pack_targets */
+  const double* fwf;
+  const double* wsum;
+  const int32_t* rows;           /* [nblock][32] output row per lane, -1 empty */
+  const rr_segment_desc* segs;   /* host array, nseg entries */
+  int32_t nblock;
+  int32_t nseg;
+  int64_t npix_block;
+} rr_scan_targets;
+
+/* tile_counter: one device int of scratch (reset by the call). */
+int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
+                   int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Plain per-target path (the structure of redrock's own GPU branch: R.T for
+ * all z into a workspace, then M and y, then the solve, then the model and
+ * chi2).  First pack the target's spectra into band rows:
+ *   band[P][11], w[P], wflux[P], flux[P]  (P = sum of spectrum pixels, in
+ *   spectrum order) and seg_basis[P]: padded basis index of each pixel.
+ * ---------------------------------------------------------------------- */
+int rr_pack_band_rows(const rr_spectrum_desc* specs /* device */, int64_t nspec,
+                      const double* rdata, const int32_t* roffsets, int64_t npix_total,
+                      double* band, int* status, rr_stream_t stream);
+
+size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz, int32_t nbasis);
+
+int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflux,
+                         const double* flux, const int64_t* pix_basis, int64_t npix_total,
+                         const double* basis, int64_t pix_stride, int32_t nz, int32_t nbasis,
+                         int32_t basis_stride, const double* prior, int32_t method,
+                         double* zchi2, double* zcoeff, void* workspace, size_t workspace_bytes,
+                         int* status, rr_stream_t stream);
+
+/* penalty[z] = max(0, -sum_b coeff[z][b] oii[b])  (zscan.py:783-800) */
+int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const double* oii,
+                      double* penalty, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * FMA throughput probe (no counterpart in redrock): the roofline
+ * denominator of the FP64-bound scan.  kind 0 = FP64, 1 = FP32; issues
+ * 2*8*16*iters*blocks*256 FLOPs; out is one device element of that type.
+ * ---------------------------------------------------------------------- */
+int rr_fma_peak(int kind, int blocks, int iters, void* out, rr_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REDROCK_B200_H */

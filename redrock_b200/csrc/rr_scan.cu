@@ -1,0 +1,795 @@
+// Redshift scan: chi2(z) and best-fit coefficients of every target against
+// every template basis, with the [OII] penalty.
+//
+// Reference (redrock 0.22):
+//   calc_zchi2_batch  zscan.py:626-781  Tb = R.T, M = Tb^T W Tb, y = Tb^T W f,
+//                                        solve, chi2 = sum w (f - Tb c)^2
+//   calc_zchi2        zscan.py:807-889  loop over targets, all-zero weights
+//                                        -> HUGE_CHI2, [OII] penalty
+//   solve_matrices    zscan.py:1107-1152 (PCA: LAPACK gesv; exactly
+//                                        singular -> LinAlgError -> HUGE)
+//   calc_negOII_penalty zscan.py:783-800
+//
+// Fused path (rr_zscan_fused).  A target's data is first packed as
+//   rw[p][k] = sqrt(w_p) R[p, p+k-5]  (k < 11),  rw[p][11] = sqrt(w_p) f_p
+// so that with Tb' = rw . T_z (the weighted resolution-convolved basis)
+//   M = sum_p Tb'_p Tb'_p^T,  y = sum_p rw[p][11] Tb'_p,
+// which are redrock's M and y.  chi2 = f^T W f - c^T y - c^T P c at the
+// solution of (M + P) c = y equals redrock's sum w (f - Tb c)^2.
+//
+// One CTA = 8 warps; a tile is (template, block of 32 targets, 8 redshifts):
+// warp w scans redshift z0 + w, lane l target l of the block, so each lane
+// owns one (target, z) pair and keeps its 55 (n = 10) Gram entries and y in
+// FP64 registers for the whole pixel sweep.  Pixels stream through shared
+// memory in chunks of 16: one bulk (TMA) copy brings the block's packed
+// resolution rows for the chunk (coalesced over lanes) and one copy per
+// warp brings that redshift's basis window (chunk + 5-pixel halo each side);
+// the basis values are read as warp-wide broadcasts.  Two stages alternate
+// so the copy of chunk c+1 overlaps the arithmetic on chunk c.  Tiles are
+// handed out by an atomic counter (persistent CTAs) across all templates, so
+// templates with different nbasis / nz share one launch.  The epilogue
+// solves the n x n system in registers (LDL^T, no pivoting; an exactly zero
+// pivot is redrock's singular case) and writes chi2, coefficients and the
+// penalty.
+#include <cmath>
+#include <cstring>
+
+#include "rr_common.cuh"
+
+namespace rr {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kChunk = RR_CHUNK;
+constexpr int kWin = kChunk + 2 * kHalfBand;  // basis rows per chunk window
+constexpr int kStages = 2;
+constexpr int kRwChunkDoubles = kChunk * RR_RW * RR_LANES;
+
+struct FusedParams {
+  rr_scan_targets tg;
+  rr_segment_desc segs[16];
+  int nseg;
+  int ntemplate;
+  rr_scan_template tm[RR_MAX_TEMPLATES];
+  int64_t tile_start[RR_MAX_TEMPLATES + 1];
+  int64_t chunks_total;  // pixel chunks per block (over all segments)
+  int max_stride;        // largest basis_stride
+  int* tile_counter;
+  int* status;
+};
+
+struct StageBufs {
+  double* rw[kStages];
+  double* t[kStages];
+  uint64_t* full;  // kStages mbarriers
+};
+
+__device__ __forceinline__ void chunk_segment(const FusedParams& p, int64_t c, int& seg,
+                                              int64_t& p0) {
+  int s = 0;
+  int64_t acc = 0;
+  for (; s < p.nseg; ++s) {
+    const int64_t n = p.segs[s].npix_pad / kChunk;
+    if (c < acc + n) break;
+    acc += n;
+  }
+  seg = s;
+  p0 = (c - acc) * kChunk;
+}
+
+// Thread 0: start the copies of chunk c of (block, template, z0) into stage s.
+__device__ __forceinline__ void issue_chunk(const FusedParams& p, const rr_scan_template& tm,
+                                            int block, int z0, int nzt, int64_t c, int s,
+                                            StageBufs& sb) {
+  int seg;
+  int64_t p0;
+  chunk_segment(p, c, seg, p0);
+  const rr_segment_desc& sd = p.segs[seg];
+  const uint32_t rw_bytes = kRwChunkDoubles * sizeof(double);
+  const uint32_t t_bytes = kWin * tm.basis_stride * sizeof(double);
+  mbar_arrive_expect_tx(&sb.full[s], rw_bytes + nzt * t_bytes);
+  const double* src_rw =
+      p.tg.rw + ((int64_t)block * p.tg.npix_block + sd.rw_offset + p0) * (RR_RW * RR_LANES);
+  bulk_g2s(sb.rw[s], src_rw, rw_bytes, &sb.full[s]);
+  for (int w = 0; w < nzt; ++w) {
+    const double* src_t =
+        tm.basis + ((int64_t)(z0 + w) * tm.pix_stride + sd.basis_offset + p0 - kHalfBand) *
+                       tm.basis_stride;
+    bulk_g2s(sb.t[s] + (int64_t)w * kWin * tm.basis_stride, src_t, t_bytes, &sb.full[s]);
+  }
+}
+
+template <int NB>
+struct Acc {
+  static constexpr int kTri = NB * (NB + 1) / 2;
+  double m[kTri];
+  double y[NB];
+};
+
+// LDL^T of the packed lower triangle a (row-major, a[i(i+1)/2 + j], j <= i)
+// in place, then solve for c.  Returns false on an exactly zero pivot.
+template <int NB>
+__device__ __forceinline__ bool ldlt_solve(double (&a)[NB * (NB + 1) / 2], const double (&y)[NB],
+                                           double (&c)[NB]) {
+#define A(i, j) a[(i) * ((i) + 1) / 2 + (j)]
+  double d[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    double v[NB];
+    double dj = A(j, j);
+#pragma unroll
+    for (int k = 0; k < j; ++k) {
+      v[k] = A(j, k) * d[k];
+      dj -= A(j, k) * v[k];
+    }
+    if (dj == 0.0) return false;
+    d[j] = dj;
+    const double inv = 1.0 / dj;
+#pragma unroll
+    for (int i = j + 1; i < NB; ++i) {
+      double s = A(i, j);
+#pragma unroll
+      for (int k = 0; k < j; ++k) s -= A(i, k) * v[k];
+      A(i, j) = s * inv;
+    }
+  }
+  // L z = y
+#pragma unroll
+  for (int i = 0; i < NB; ++i) {
+    double s = y[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) s -= A(i, k) * c[k];
+    c[i] = s;
+  }
+#pragma unroll
+  for (int i = 0; i < NB; ++i) c[i] /= d[i];
+  // L^T c = z
+#pragma unroll
+  for (int i = NB - 1; i >= 0; --i) {
+    double s = c[i];
+#pragma unroll
+    for (int k = i + 1; k < NB; ++k) s -= A(k, i) * c[k];
+    c[i] = s;
+  }
+#undef A
+  return true;
+}
+
+// Solve, chi2 and penalty for one (target, z); writes the outputs.
+template <int NB>
+__device__ __forceinline__ void finish_eval(const rr_scan_template& tm, int64_t row, int z,
+                                            double (&m)[NB * (NB + 1) / 2], const double (&y)[NB],
+                                            double fwf, double wsum) {
+  double c[NB];
+  double chi2;
+  bool ok = (wsum != 0.0) && (tm.method == RR_SOLVE_PCA);
+  if (ok) {
+    if (tm.prior) {
+#pragma unroll
+      for (int i = 0; i < NB; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) m[i * (i + 1) / 2 + j] += tm.prior[i * NB + j];
+    }
+    ok = ldlt_solve<NB>(m, y, c);
+  }
+  if (ok) {
+    double cy = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) cy = fma(c[i], y[i], cy);
+    double cpc = 0.0;
+    if (tm.prior) {
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) s = fma(tm.prior[i * NB + j], c[j], s);
+        cpc = fma(c[i], s, cpc);
+      }
+    }
+    chi2 = fwf - cy - cpc;
+  } else {
+#pragma unroll
+    for (int i = 0; i < NB; ++i) c[i] = 0.0;
+    chi2 = kHugeChi2;
+  }
+  tm.zchi2[row * tm.nz + z] = chi2;
+  double* co = tm.zcoeff + (row * tm.nz + z) * NB;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) co[i] = c[i];
+  if (tm.oii) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) s = fma(c[i], tm.oii[i], s);
+    // an all-zero-weight target is skipped before the penalty in redrock
+    tm.penalty[row * tm.nz + z] = (wsum != 0.0 && s < 0.0) ? -s : 0.0;
+  }
+}
+
+template <int NB>
+__device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
+                          StageBufs& sb, uint32_t (&uses)[kStages], bool& failed) {
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nzt = min(kWarps, tm.nz - z0);
+  const bool active = warp < nzt;
+  const int stride = tm.basis_stride;
+  constexpr int kTri = NB * (NB + 1) / 2;
+  double m[kTri];
+  double y[NB];
+#pragma unroll
+  for (int i = 0; i < kTri; ++i) m[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) y[i] = 0.0;
+
+  const int64_t nchunk = p.chunks_total;
+  if (threadIdx.x == 0) issue_chunk(p, tm, block, z0, nzt, 0, 0, sb);
+  for (int64_t c = 0; c < nchunk; ++c) {
+    const int s = (int)(c & 1);
+    const bool more = c + 1 < nchunk;
+    if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, c + 1, s ^ 1, sb);
+    const bool ok = mbar_wait(&sb.full[s], uses[s] & 1u, p.status);
+    uses[s]++;
+    if (active && ok) {
+      const double* rws = sb.rw[s];
+      const double* ts = sb.t[s] + (int64_t)warp * kWin * stride;
+#pragma unroll 1
+      for (int q = 0; q < kChunk; ++q) {
+        double r[kBand];
+#pragma unroll
+        for (int k = 0; k < kBand; ++k) r[k] = rws[(q * RR_RW + k) * RR_LANES + lane];
+        const double g = rws[(q * RR_RW + kBand) * RR_LANES + lane];
+        double tb[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) tb[b] = 0.0;
+#pragma unroll
+        for (int k = 0; k < kBand; ++k) {
+          const double* trow = ts + (q + k) * stride;
+#pragma unroll
+          for (int b = 0; b + 1 < NB; b += 2) {
+            const double2 tv = *reinterpret_cast<const double2*>(trow + b);
+            tb[b] = fma(r[k], tv.x, tb[b]);
+            tb[b + 1] = fma(r[k], tv.y, tb[b + 1]);
+          }
+          if (NB & 1) tb[NB - 1] = fma(r[k], trow[NB - 1], tb[NB - 1]);
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) y[b] = fma(g, tb[b], y[b]);
+#pragma unroll
+        for (int a = 0; a < NB; ++a)
+#pragma unroll
+          for (int b = 0; b <= a; ++b)
+            m[a * (a + 1) / 2 + b] = fma(tb[a], tb[b], m[a * (a + 1) / 2 + b]);
+      }
+    }
+    // stage s is free for chunk c + 2 once every warp is past this point;
+    // a timed-out wait anywhere stops the whole CTA
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      // let the copy of chunk c + 1 (if issued) land before leaving
+      if (threadIdx.x == 0 && more) mbar_wait(&sb.full[s ^ 1], uses[s ^ 1] & 1u, p.status);
+      return;
+    }
+  }
+  if (failed || !active) return;
+  const int32_t row = p.tg.rows[block * RR_LANES + lane];
+  if (row < 0) return;
+  const double fwf = p.tg.fwf[block * RR_LANES + lane];
+  const double wsum = p.tg.wsum[block * RR_LANES + lane];
+  finish_eval<NB>(tm, row, z0 + warp, m, y, fwf, wsum);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ int64_t s_tile;
+  StageBufs sb;
+  {
+    double* base = reinterpret_cast<double*>(smem);
+    const int64_t t_doubles = (int64_t)kWarps * kWin * p.max_stride;
+    for (int s = 0; s < kStages; ++s) {
+      sb.rw[s] = base + s * (kRwChunkDoubles + t_doubles);
+      sb.t[s] = sb.rw[s] + kRwChunkDoubles;
+    }
+    sb.full = full;
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t uses[kStages] = {0, 0};
+  bool failed = false;
+  const int64_t ntiles = p.tile_start[p.ntemplate];
+  while (true) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(p.tile_counter, 1);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    __syncthreads();
+    if (tile >= ntiles) break;
+    int t = 0;
+    while (t + 1 < p.ntemplate && tile >= p.tile_start[t + 1]) ++t;
+    const rr_scan_template& tm = p.tm[t];
+    const int64_t local = tile - p.tile_start[t];
+    const int block = (int)(local % p.tg.nblock);
+    const int z0 = (int)(local / p.tg.nblock) * kWarps;
+    switch (tm.nbasis) {
+      case 1: scan_tile<1>(p, tm, block, z0, sb, uses, failed); break;
+      case 2: scan_tile<2>(p, tm, block, z0, sb, uses, failed); break;
+      case 3: scan_tile<3>(p, tm, block, z0, sb, uses, failed); break;
+      case 4: scan_tile<4>(p, tm, block, z0, sb, uses, failed); break;
+      case 5: scan_tile<5>(p, tm, block, z0, sb, uses, failed); break;
+      case 6: scan_tile<6>(p, tm, block, z0, sb, uses, failed); break;
+      case 7: scan_tile<7>(p, tm, block, z0, sb, uses, failed); break;
+      case 8: scan_tile<8>(p, tm, block, z0, sb, uses, failed); break;
+      case 9: scan_tile<9>(p, tm, block, z0, sb, uses, failed); break;
+      case 10: scan_tile<10>(p, tm, block, z0, sb, uses, failed); break;
+      default: set_status(p.status, RR_EINVAL); failed = true; break;
+    }
+    if (failed) break;  // uniform across the CTA
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// packing
+// ---------------------------------------------------------------------------
+
+// One thread per (spectrum pixel): band row of R at that pixel from the DIA
+// data, where data[d][j] = R[j - off_d, j] (scipy dia_matrix convention).
+__device__ __forceinline__ void band_row(const double* __restrict__ rdata,
+                                         const int32_t* __restrict__ roff,
+                                         const rr_spectrum_desc& sd, int64_t i, double (&r)[kBand],
+                                         int* status) {
+#pragma unroll
+  for (int k = 0; k < kBand; ++k) r[k] = 0.0;
+  for (int d = 0; d < sd.ndiag; ++d) {
+    const int off = roff[sd.diag_offset + d];
+    if (off < -kHalfBand || off > kHalfBand) {
+      // only reachable if the host check was bypassed; a nonzero band value
+      // outside the kernel's band would be silently dropped
+      const int64_t j = i + off;
+      if (j >= 0 && j < sd.npix && rdata[sd.data_offset + (int64_t)d * sd.npix + j] != 0.0)
+        set_status(status, RR_ENOTSUP);
+      continue;
+    }
+    const int64_t j = i + off;
+    if (j >= 0 && j < sd.npix) r[off + kHalfBand] += rdata[sd.data_offset + (int64_t)d * sd.npix + j];
+  }
+}
+
+__global__ void pack_targets_kernel(const rr_spectrum_desc* __restrict__ specs, int64_t nspec,
+                                    const double* __restrict__ rdata,
+                                    const int32_t* __restrict__ roff,
+                                    const double* __restrict__ ivar, const double* __restrict__ flux,
+                                    const rr_segment_desc* __restrict__ segs, int64_t npix_block,
+                                    double* __restrict__ rw, int* status) {
+  const int64_t s = blockIdx.y;
+  if (s >= nspec) return;
+  const rr_spectrum_desc sd = specs[s];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= sd.npix) return;
+  const rr_segment_desc seg = segs[sd.segment];
+  if (i >= seg.npix_pad) { set_status(status, RR_EINVAL); return; }
+  double r[kBand];
+  band_row(rdata, roff, sd, i, r, status);
+  const double w = ivar[sd.pix_offset + i];
+  const double sw = sqrt(w);
+  double* o = rw + ((int64_t)sd.block * npix_block + seg.rw_offset + i) * (RR_RW * RR_LANES) + sd.lane;
+#pragma unroll
+  for (int k = 0; k < kBand; ++k) o[k * RR_LANES] = sw * r[k];
+  o[kBand * RR_LANES] = sw * flux[sd.pix_offset + i];
+}
+
+// Per-target sums f^T W f and sum w in FP64.  One CTA per target walks the
+// target's spectra in order (spectra are grouped by target, target t owning
+// specs[first[t] .. first[t+1])), so the summation order is fixed.
+__global__ void pack_sums_kernel(const rr_spectrum_desc* __restrict__ specs,
+                                 const int64_t* __restrict__ first, int64_t ntarget,
+                                 const double* __restrict__ ivar, const double* __restrict__ flux,
+                                 double* __restrict__ fwf, double* __restrict__ wsum) {
+  const int64_t t = blockIdx.x;
+  if (t >= ntarget) return;
+  __shared__ double red[2][256];
+  double tot_a = 0.0, tot_b = 0.0;
+  int64_t slot = -1;
+  for (int64_t s = first[t]; s < first[t + 1]; ++s) {
+    const rr_spectrum_desc sd = specs[s];
+    slot = (int64_t)sd.block * RR_LANES + sd.lane;
+    double a = 0.0, b = 0.0;
+    for (int64_t i = threadIdx.x; i < sd.npix; i += blockDim.x) {
+      const double w = ivar[sd.pix_offset + i];
+      const double f = flux[sd.pix_offset + i];
+      a += w * f * f;
+      b += w;
+    }
+    red[0][threadIdx.x] = a;
+    red[1][threadIdx.x] = b;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+      if (threadIdx.x < h) {
+        red[0][threadIdx.x] += red[0][threadIdx.x + h];
+        red[1][threadIdx.x] += red[1][threadIdx.x + h];
+      }
+      __syncthreads();
+    }
+    tot_a += red[0][0];
+    tot_b += red[1][0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && slot >= 0) {
+    fwf[slot] = tot_a;
+    wsum[slot] = tot_b;
+  }
+}
+
+__global__ void pack_band_rows_kernel(const rr_spectrum_desc* __restrict__ specs, int64_t nspec,
+                                      const double* __restrict__ rdata,
+                                      const int32_t* __restrict__ roff, double* __restrict__ band,
+                                      int* status) {
+  const int64_t s = blockIdx.y;
+  if (s >= nspec) return;
+  const rr_spectrum_desc sd = specs[s];
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= sd.npix) return;
+  double r[kBand];
+  band_row(rdata, roff, sd, i, r, status);
+  double* o = band + (sd.pix_offset + i) * kBand;
+#pragma unroll
+  for (int k = 0; k < kBand; ++k) o[k] = r[k];
+}
+
+// ---------------------------------------------------------------------------
+// plain per-target path
+// ---------------------------------------------------------------------------
+
+// Tb[z][p][b] = sum_k band[p][k] basis[z][pix_basis[p] + k - 5][b]
+__global__ void plain_rt_kernel(const double* __restrict__ band, const int64_t* __restrict__ pix_basis,
+                                int64_t npix, const double* __restrict__ basis, int64_t pix_stride,
+                                int nz, int nb, int stride, double* __restrict__ tb) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)nz * npix * nb;
+  if (i >= total) return;
+  const int b = (int)(i % nb);
+  const int64_t pz = i / nb;
+  const int64_t p = pz % npix;
+  const int64_t z = pz / npix;
+  const double* t = basis + (z * pix_stride + pix_basis[p] - kHalfBand) * stride + b;
+  const double* r = band + p * kBand;
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < kBand; ++k) acc = fma(r[k], t[(int64_t)k * stride], acc);
+  tb[i] = acc;
+}
+
+// One CTA per z: M = Tb^T W Tb (lower triangle) and y = Tb^T (w f),
+// deterministic tree reduction.
+template <int NB>
+__global__ void plain_gram_kernel(const double* __restrict__ tb, const double* __restrict__ w,
+                                  const double* __restrict__ wflux, int64_t npix,
+                                  double* __restrict__ mout, double* __restrict__ yout) {
+  constexpr int kTri = NB * (NB + 1) / 2;
+  const int64_t z = blockIdx.x;
+  const double* t = tb + z * npix * NB;
+  double m[kTri], y[NB];
+#pragma unroll
+  for (int i = 0; i < kTri; ++i) m[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) y[i] = 0.0;
+  for (int64_t p = threadIdx.x; p < npix; p += blockDim.x) {
+    double v[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) v[b] = t[p * NB + b];
+    const double wp = w[p], wf = wflux[p];
+#pragma unroll
+    for (int a = 0; a < NB; ++a) {
+      y[a] = fma(v[a], wf, y[a]);
+      const double wa = wp * v[a];
+#pragma unroll
+      for (int b = 0; b <= a; ++b) m[a * (a + 1) / 2 + b] = fma(wa, v[b], m[a * (a + 1) / 2 + b]);
+    }
+  }
+  __shared__ double red[128];
+#pragma unroll 1
+  for (int e = 0; e < kTri + NB; ++e) {
+    red[threadIdx.x] = e < kTri ? m[e] : y[e - kTri];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+      if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (e < kTri) mout[z * kTri + e] = red[0];
+      else yout[z * NB + (e - kTri)] = red[0];
+    }
+    __syncthreads();
+  }
+}
+
+template <int NB>
+__global__ void plain_solve_kernel(const double* __restrict__ mtri, const double* __restrict__ y,
+                                   int nz, const double* __restrict__ prior, int method,
+                                   double* __restrict__ zcoeff, unsigned char* __restrict__ bad) {
+  constexpr int kTri = NB * (NB + 1) / 2;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= nz) return;
+  double a[kTri], yy[NB], c[NB];
+#pragma unroll
+  for (int i = 0; i < kTri; ++i) a[i] = mtri[(int64_t)z * kTri + i];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) yy[i] = y[(int64_t)z * NB + i];
+  bool ok = method == RR_SOLVE_PCA;
+  if (ok && prior) {
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+#pragma unroll
+      for (int j = 0; j <= i; ++j) a[i * (i + 1) / 2 + j] += prior[i * NB + j];
+  }
+  if (ok) ok = ldlt_solve<NB>(a, yy, c);
+  if (!ok) {
+#pragma unroll
+    for (int i = 0; i < NB; ++i) c[i] = 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < NB; ++i) zcoeff[(int64_t)z * NB + i] = c[i];
+  bad[z] = ok ? 0 : 1;
+}
+
+// chi2[z] = sum_p w (f - Tb c)^2, deterministic reduction; HUGE if bad.
+template <int NB>
+__global__ void plain_chi2_kernel(const double* __restrict__ tb, const double* __restrict__ w,
+                                  const double* __restrict__ flux, int64_t npix,
+                                  const double* __restrict__ zcoeff,
+                                  const unsigned char* __restrict__ bad, double* __restrict__ zchi2) {
+  const int64_t z = blockIdx.x;
+  const double* t = tb + z * npix * NB;
+  double c[NB];
+#pragma unroll
+  for (int i = 0; i < NB; ++i) c[i] = zcoeff[z * NB + i];
+  double acc = 0.0;
+  for (int64_t p = threadIdx.x; p < npix; p += blockDim.x) {
+    double model = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) model = fma(t[p * NB + b], c[b], model);
+    const double r = flux[p] - model;
+    acc = fma(w[p], r * r, acc);
+  }
+  __shared__ double red[128];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) zchi2[z] = bad[z] ? kHugeChi2 : red[0];
+}
+
+__global__ void negoii_kernel(const double* __restrict__ coeff, int64_t nz, int nb,
+                              const double* __restrict__ oii, double* __restrict__ pen) {
+  const int64_t z = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (z >= nz) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s = fma(coeff[z * nb + b], oii[b], s);
+  pen[z] = s < 0.0 ? -s : 0.0;
+}
+
+}  // namespace rr
+
+using namespace rr;
+
+static thread_local int g_last_cuda_error = 0;
+
+extern "C" int rr_last_cuda_error(void) { return g_last_cuda_error; }
+
+extern "C" int rr_version(void) { return 1; }
+
+extern "C" const char* rr_status_string(int status) {
+  switch (status) {
+    case RR_OK: return "ok";
+    case RR_EINVAL: return "invalid argument";
+    case RR_ERANGE: return "edges must be within input x range";
+    case RR_ECUDA: return "CUDA runtime error";
+    case RR_ETIMEOUT: return "bounded device wait timed out";
+    case RR_ENOTSUP: return "unsupported input";
+    default: return "unknown status";
+  }
+}
+
+#undef RR_CUDA_TRY
+#define RR_CUDA_TRY(expr)                        \
+  do {                                           \
+    cudaError_t _e = (expr);                     \
+    if (_e != cudaSuccess) {                     \
+      g_last_cuda_error = (int)_e;               \
+      return RR_ECUDA;                           \
+    }                                            \
+  } while (0)
+
+#undef RR_CHECK_LAUNCH
+#define RR_CHECK_LAUNCH() RR_CUDA_TRY(cudaGetLastError())
+
+static size_t fused_smem_bytes(int max_stride) {
+  return (size_t)kStages * (kRwChunkDoubles + (size_t)kWarps * kWin * max_stride) * sizeof(double);
+}
+
+extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
+                              int ntemplate, int* tile_counter, int* status, rr_stream_t stream) {
+  if (!targets || !templates || !tile_counter) return RR_EINVAL;
+  if (ntemplate < 1 || ntemplate > RR_MAX_TEMPLATES) return RR_EINVAL;
+  if (targets->nblock < 1 || targets->nseg < 1 || targets->nseg > 16) return RR_EINVAL;
+  if (!targets->rw || !targets->fwf || !targets->wsum || !targets->rows || !targets->segs)
+    return RR_EINVAL;
+  FusedParams p;
+  memset(&p, 0, sizeof(p));
+  p.tg = *targets;
+  p.nseg = targets->nseg;
+  int64_t chunks = 0, rw_end = 0;
+  for (int s = 0; s < p.nseg; ++s) {
+    p.segs[s] = targets->segs[s];
+    const rr_segment_desc& sd = p.segs[s];
+    if (sd.npix_pad <= 0 || (sd.npix_pad % kChunk) != 0 || sd.basis_offset < kHalfBand ||
+        sd.rw_offset < 0)
+      return RR_EINVAL;
+    chunks += sd.npix_pad / kChunk;
+    rw_end = sd.rw_offset + sd.npix_pad > rw_end ? sd.rw_offset + sd.npix_pad : rw_end;
+  }
+  if (rw_end > targets->npix_block) return RR_EINVAL;
+  p.chunks_total = chunks;
+  p.ntemplate = ntemplate;
+  p.tile_start[0] = 0;
+  int max_stride = 2;
+  for (int t = 0; t < ntemplate; ++t) {
+    const rr_scan_template& tm = templates[t];
+    if (tm.nbasis < 1 || tm.nbasis > RR_MAX_NBASIS || tm.nz < 0) return RR_EINVAL;
+    if (tm.basis_stride < tm.nbasis || (tm.basis_stride & 1)) return RR_EINVAL;
+    if (tm.nz > 0 && (!tm.basis || !tm.zchi2 || !tm.zcoeff)) return RR_EINVAL;
+    if (tm.oii && !tm.penalty) return RR_EINVAL;
+    if ((reinterpret_cast<uintptr_t>(tm.basis) & 15) != 0) return RR_EINVAL;
+    for (int s = 0; s < p.nseg; ++s)
+      if (p.segs[s].basis_offset + p.segs[s].npix_pad + kHalfBand > tm.pix_stride) return RR_EINVAL;
+    p.tm[t] = tm;
+    const int64_t zt = (tm.nz + kWarps - 1) / kWarps;
+    p.tile_start[t + 1] = p.tile_start[t] + zt * targets->nblock;
+    max_stride = tm.basis_stride > max_stride ? tm.basis_stride : max_stride;
+  }
+  if ((reinterpret_cast<uintptr_t>(targets->rw) & 15) != 0) return RR_EINVAL;
+  p.max_stride = max_stride;
+  p.tile_counter = tile_counter;
+  p.status = status;
+  const int64_t ntiles = p.tile_start[ntemplate];
+  if (ntiles == 0) return RR_OK;
+  const size_t smem = fused_smem_bytes(max_stride);
+  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  int dev = 0, nsm = 0;
+  RR_CUDA_TRY(cudaGetDevice(&dev));
+  RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  RR_CUDA_TRY(cudaMemsetAsync(tile_counter, 0, sizeof(int), (cudaStream_t)stream));
+  const int64_t grid = ntiles < nsm ? ntiles : nsm;
+  zscan_fused_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_pack_targets(const rr_spectrum_desc* specs, int64_t nspec,
+                               const int64_t* target_first, int64_t ntarget, const double* rdata,
+                               const int32_t* roffsets, const double* ivar, const double* flux,
+                               const rr_segment_desc* segs, int nseg, int64_t npix_block,
+                               int nblock, double* rw, double* fwf, double* wsum, int* status,
+                               rr_stream_t stream) {
+  if (nspec < 0 || ntarget < 0 || nseg < 1 || nblock < 1 || npix_block < 1) return RR_EINVAL;
+  if (nspec == 0 || ntarget == 0) return RR_OK;
+  if (!specs || !target_first || !rdata || !roffsets || !ivar || !flux || !segs || !rw || !fwf ||
+      !wsum)
+    return RR_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int64_t s0 = 0; s0 < nspec; s0 += 65535) {
+    const int64_t n = nspec - s0 < 65535 ? nspec - s0 : 65535;
+    dim3 block(128);
+    dim3 grid((unsigned)((npix_block + block.x - 1) / block.x), (unsigned)n);
+    pack_targets_kernel<<<grid, block, 0, st>>>(specs + s0, n, rdata, roffsets, ivar, flux, segs,
+                                                npix_block, rw, status);
+    RR_CHECK_LAUNCH();
+  }
+  pack_sums_kernel<<<(unsigned)ntarget, 256, 0, st>>>(specs, target_first, ntarget, ivar, flux, fwf,
+                                                      wsum);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_pack_band_rows(const rr_spectrum_desc* specs, int64_t nspec, const double* rdata,
+                                 const int32_t* roffsets, int64_t npix_total, double* band,
+                                 int* status, rr_stream_t stream) {
+  if (nspec < 0 || npix_total < 0) return RR_EINVAL;
+  if (nspec == 0) return RR_OK;
+  if (!specs || !rdata || !roffsets || !band || nspec > 65535) return RR_EINVAL;
+  dim3 block(128);
+  dim3 grid((unsigned)((npix_total + block.x - 1) / block.x), (unsigned)nspec);
+  pack_band_rows_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(specs, nspec, rdata, roffsets,
+                                                                  band, status);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz,
+                                                       int32_t nbasis) {
+  const size_t tri = (size_t)nbasis * (nbasis + 1) / 2;
+  return align256((size_t)nz * npix_total * nbasis * sizeof(double)) +
+         align256((size_t)nz * tri * sizeof(double)) +
+         align256((size_t)nz * nbasis * sizeof(double)) + align256((size_t)nz);
+}
+
+template <int NB>
+static int plain_launch(const double* band, const double* w, const double* wflux,
+                        const double* flux, const int64_t* pix_basis, int64_t npix,
+                        const double* basis, int64_t pix_stride, int nz, int stride,
+                        const double* prior, int method, double* zchi2, double* zcoeff,
+                        unsigned char* ws, cudaStream_t st) {
+  constexpr int kTri = NB * (NB + 1) / 2;
+  double* tb = reinterpret_cast<double*>(ws);
+  double* mtri = reinterpret_cast<double*>(ws + align256((size_t)nz * npix * NB * sizeof(double)));
+  double* yv = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(mtri) +
+                                         align256((size_t)nz * kTri * sizeof(double)));
+  unsigned char* bad =
+      reinterpret_cast<unsigned char*>(yv) + align256((size_t)nz * NB * sizeof(double));
+  const int64_t total = (int64_t)nz * npix * NB;
+  plain_rt_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(band, pix_basis, npix, basis,
+                                                                    pix_stride, nz, NB, stride, tb);
+  RR_CHECK_LAUNCH();
+  plain_gram_kernel<NB><<<nz, 128, 0, st>>>(tb, w, wflux, npix, mtri, yv);
+  RR_CHECK_LAUNCH();
+  plain_solve_kernel<NB><<<(nz + 127) / 128, 128, 0, st>>>(mtri, yv, nz, prior, method, zcoeff, bad);
+  RR_CHECK_LAUNCH();
+  plain_chi2_kernel<NB><<<nz, 128, 0, st>>>(tb, w, flux, npix, zcoeff, bad, zchi2);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflux,
+                                    const double* flux, const int64_t* pix_basis,
+                                    int64_t npix_total, const double* basis, int64_t pix_stride,
+                                    int32_t nz, int32_t nbasis, int32_t basis_stride,
+                                    const double* prior, int32_t method, double* zchi2,
+                                    double* zcoeff, void* workspace, size_t workspace_bytes,
+                                    int* status, rr_stream_t stream) {
+  (void)status;
+  if (nz < 0 || npix_total < 1 || nbasis < 1 || nbasis > RR_MAX_NBASIS) return RR_EINVAL;
+  if (basis_stride < nbasis) return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  if (!band || !w || !wflux || !flux || !pix_basis || !basis || !zchi2 || !zcoeff || !workspace)
+    return RR_EINVAL;
+  if (workspace_bytes < rr_zchi2_batch_plain_workspace_bytes(npix_total, nz, nbasis))
+    return RR_EINVAL;
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  cudaStream_t st = (cudaStream_t)stream;
+#define RR_PLAIN_CASE(N)                                                                          \
+  case N:                                                                                         \
+    return plain_launch<N>(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz,    \
+                           basis_stride, prior, method, zchi2, zcoeff, ws, st);
+  switch (nbasis) {
+    RR_PLAIN_CASE(1)
+    RR_PLAIN_CASE(2)
+    RR_PLAIN_CASE(3)
+    RR_PLAIN_CASE(4)
+    RR_PLAIN_CASE(5)
+    RR_PLAIN_CASE(6)
+    RR_PLAIN_CASE(7)
+    RR_PLAIN_CASE(8)
+    RR_PLAIN_CASE(9)
+    RR_PLAIN_CASE(10)
+    default: return RR_EINVAL;
+  }
+#undef RR_PLAIN_CASE
+}
+
+extern "C" int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const double* oii,
+                                 double* penalty, rr_stream_t stream) {
+  if (nz < 0 || nbasis < 1) return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  if (!coeff || !oii || !penalty) return RR_EINVAL;
+  negoii_kernel<<<(unsigned)((nz + 127) / 128), 128, 0, (cudaStream_t)stream>>>(coeff, nz, nbasis,
+                                                                                oii, penalty);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}

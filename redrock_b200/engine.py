@@ -1,0 +1,502 @@
+"""Device-resident scan engine: wavelength-grid layout, template bases,
+packed targets and the fused / plain scan launches.
+
+HBM layout (all FP64):
+
+* basis of one template: ``[nz][pix_stride][stride]``.  The wavelength grids
+  (one per redrock "wavehash") are laid end to end; grid g owns padded
+  pixels ``[pix_offset_g - 5, pix_offset_g + npix_pad_g + 5)``, its real
+  pixels start at ``pix_offset_g``, and the 5-pixel margins and the tail up
+  to ``npix_pad_g`` (a multiple of 16) are zero, so the banded resolution
+  product never reads another grid's values.  ``stride`` is nbasis rounded
+  up to even so every pixel row is 16-byte aligned for the bulk copies.
+* packed targets: ``rw[block][npix_block][12][32]`` -- 32 targets per block,
+  one per lane, the 11 band values of sqrt(w) R and sqrt(w) f for every
+  pixel of every segment (one segment per (grid, spectrum slot)), lanes
+  fastest so the scan's copies are contiguous.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from collections import OrderedDict
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import StatusWord, device, ptr, stream_handle, struct_bytes, to_device
+
+
+def round_up(n, m):
+    return ((n + m - 1) // m) * m
+
+
+def centers2edges(centers):
+    """Bin edges from centres (redrock rebin.py:100-118)."""
+    centers = np.asarray(centers)
+    edges = np.zeros(len(centers) + 1)
+    edges[1:-1] = (centers[0:-1] + centers[1:]) / 2.0
+    edges[0] = centers[0] - (centers[1] - edges[1])
+    edges[-1] = centers[-1] + (centers[-1] - edges[-2])
+    return edges
+
+
+# ---------------------------------------------------------------------------
+# wavelength-grid layout
+# ---------------------------------------------------------------------------
+class GridLayout:
+    """Ordered set of wavelength grids (wavehash -> wave) and their place in
+    the padded basis layout."""
+
+    def __init__(self, grids):
+        # grids: iterable of (key, npix, wave-or-None)
+        self.keys = []
+        self.npix = []
+        self.npix_pad = []
+        self.pix_offset = []
+        self.waves = []
+        start = 0
+        for key, npix, wave in grids:
+            npix = int(npix)
+            npad = round_up(npix, _lib.CHUNK)
+            self.keys.append(key)
+            self.npix.append(npix)
+            self.npix_pad.append(npad)
+            self.pix_offset.append(start + _lib.HALF_BAND)
+            self.waves.append(None if wave is None else np.asarray(wave, dtype=np.float64))
+            start += npad + 2 * _lib.HALF_BAND
+        self.pix_stride = start
+        self.index = {k: i for i, k in enumerate(self.keys)}
+        self._dev = {}
+
+    @classmethod
+    def from_dwave(cls, dwave):
+        return cls((k, len(w), w) for k, w in dwave.items())
+
+    @property
+    def signature(self):
+        return tuple(zip(self.keys, self.npix))
+
+    def device_arrays(self, i):
+        """(edges, wave) device tensors of grid i, cached."""
+        if i not in self._dev:
+            w = self.waves[i]
+            if w is None:
+                raise ValueError(f"grid {self.keys[i]!r} has no wavelength array")
+            e = centers2edges(w)
+            self._dev[i] = (to_device(e), to_device(w), float(e[0]), float(e[-1]))
+        return self._dev[i]
+
+
+# ---------------------------------------------------------------------------
+# template bases on the device
+# ---------------------------------------------------------------------------
+class TemplateSource:
+    """A template's rest-frame arrays and redshift grid, uploaded once."""
+
+    def __init__(self, wave, flux, redshifts, igm_model, oii=None, method=_lib.RR_SOLVE_PCA):
+        wave = np.ascontiguousarray(wave, dtype=np.float64)
+        flux = np.ascontiguousarray(np.atleast_2d(flux), dtype=np.float64)
+        self.nbasis = flux.shape[0]
+        if self.nbasis > _lib.MAX_NBASIS:
+            raise NotImplementedError(f"nbasis {self.nbasis} > {_lib.MAX_NBASIS} is not supported")
+        if igm_model not in _lib.IGM_CODES:
+            raise ValueError(f"Unrecognized model {igm_model}")
+        self.igm = _lib.IGM_CODES[igm_model]
+        self.zhost = np.ascontiguousarray(redshifts, dtype=np.float64)
+        self.nx = len(wave)
+        self.x = to_device(wave)
+        self.y = to_device(flux)
+        self.z = to_device(self.zhost)
+        self.oii = oii
+        self.method = method
+        if len(self.zhost):
+            self.xmin = float(wave[0] * (1 + self.zhost.max()))
+            self.xmax = float(wave[-1] * (1 + self.zhost.min()))
+        self.nbytes = wave.nbytes + flux.nbytes + self.zhost.nbytes
+
+    @classmethod
+    def from_template(cls, template):
+        from .templates import oii_sums, solve_code
+        return cls(template.wave, template.flux, template.redshifts, template.igm_model,
+                   oii=oii_sums(template), method=solve_code(template))
+
+
+class DeviceBasis:
+    """One template's redshifted, resolution-ready basis for all z."""
+
+    def __init__(self, basis, layout, nbasis, redshifts, oii=None, method=_lib.RR_SOLVE_PCA,
+                 prior=None):
+        self.basis = basis
+        self.layout = layout
+        self.nbasis = int(nbasis)
+        self.stride = int(basis.shape[2])
+        self.redshifts = np.asarray(redshifts, dtype=np.float64)
+        self.nz = len(self.redshifts)
+        self.oii = None if oii is None else to_device(oii)
+        self.method = method
+        self.prior = None if prior is None else to_device(prior)
+
+    @classmethod
+    def build(cls, src, layout, stream=None, status=None, **kw):
+        """Fused rebin + IGM for every z (rr_build_basis).
+
+        ``src`` is a TemplateSource (device-resident template arrays).  With
+        a caller-owned ``status`` word the call stays asynchronous; otherwise
+        it synchronises and checks the kernel status.
+        """
+        L = _lib.lib()
+        dev = device()
+        nb = src.nbasis
+        stride = round_up(nb, 2)
+        z = src.zhost
+        basis = torch.empty((len(z), layout.pix_stride, stride), dtype=torch.float64, device=dev)
+        kw.setdefault("oii", src.oii)
+        kw.setdefault("method", src.method)
+        if len(z) == 0:
+            return cls(basis, layout, nb, z, **kw)
+        descs = []
+        for i in range(len(layout.keys)):
+            e, w, emin, emax = layout.device_arrays(i)
+            apply = 0
+            if src.igm != _lib.RR_IGM_NONE:
+                # redrock skips the IGM product when no redshift puts the
+                # grid's bluest pixel below Lyman-alpha (igm.py:396-401)
+                apply = int(not (np.min(layout.waves[i]) / (1. + np.max(z)) > 1215.67))
+            descs.append(_lib.GridDesc(ptr(e), ptr(w), layout.npix[i], layout.npix_pad[i],
+                                       layout.pix_offset[i], emin, emax, apply, 0))
+        st = status or StatusWord(dev)
+        arr = (_lib.GridDesc * len(descs))(*descs)
+        rc = L.rr_build_basis(ptr(src.x), src.nx, ptr(src.y), nb, ptr(src.z), len(z), src.xmin,
+                              src.xmax, arr, len(descs), src.igm, layout.pix_stride, stride,
+                              ptr(basis), st.ptr, stream_handle(stream))
+        _lib.check(rc, "rr_build_basis")
+        if status is None:
+            torch.cuda.current_stream().synchronize()
+            st.check("rr_build_basis")
+        return cls(basis, layout, nb, z, **kw)
+
+    @classmethod
+    def from_tdata(cls, tdata, layout, redshifts=None, **kw):
+        """Device copy of redrock-layout bases dict[wavehash] -> (nz, npix, nb)
+        (numpy or CUDA tensors) into the padded layout."""
+        dev = device()
+        first = next(iter(tdata.values()))
+        nz, _, nb = first.shape
+        if nb > _lib.MAX_NBASIS:
+            raise NotImplementedError(f"nbasis {nb} > {_lib.MAX_NBASIS} is not supported")
+        stride = round_up(nb, 2)
+        basis = torch.zeros((nz, layout.pix_stride, stride), dtype=torch.float64, device=dev)
+        for i, k in enumerate(layout.keys):
+            a = tdata[k]
+            off, n = layout.pix_offset[i], layout.npix[i]
+            if tuple(a.shape) != (nz, n, nb):
+                raise ValueError(f"template data for {k!r} has shape {tuple(a.shape)}, "
+                                 f"expected {(nz, n, nb)}")
+            basis[:, off:off + n, :nb].copy_(to_device(a))
+        z = np.zeros(nz) if redshifts is None else redshifts
+        return cls(basis, layout, nb, z, **kw)
+
+    def data_dict(self, as_numpy=True):
+        """redrock's DistTemplate.local.data view: dict[wavehash] -> (nz, npix, nb)."""
+        out = {}
+        for i, k in enumerate(self.layout.keys):
+            off, n = self.layout.pix_offset[i], self.layout.npix[i]
+            v = self.basis[:, off:off + n, :self.nbasis]
+            out[k] = v.cpu().numpy().copy() if as_numpy else v
+        return out
+
+
+# ---------------------------------------------------------------------------
+# targets on the device
+# ---------------------------------------------------------------------------
+def spectrum_dia(s):
+    """(data[ndiag, npix], offsets[ndiag]) of a redrock Spectrum's R."""
+    npix = len(s.wave)
+    R = getattr(s, "R", None)
+    if R is None and getattr(s, "_mpshared", False):
+        return np.asarray(s.R_data)[:, :npix], np.asarray(s.R_offsets)
+    if R is None:
+        R = getattr(s, "_Rcsr", None)
+    if R is None:
+        raise ValueError("spectrum has no resolution matrix")
+    if not hasattr(R, "offsets"):
+        R = R.todia()
+    return np.asarray(R.data)[:, :npix], np.asarray(R.offsets)
+
+
+class TargetBatch:
+    """Host side of a target batch: the descriptors and the concatenated raw
+    arrays (DIA resolution data, offsets, ivar, flux) that rr_pack_targets
+    reads.  Building it is plain host data preparation (no arithmetic)."""
+
+    def __init__(self, targets, layout):
+        self.layout = layout
+        self.ntarget = len(targets)
+        self.nblock = max(1, (self.ntarget + _lib.LANES - 1) // _lib.LANES)
+        # segments: one per (grid, spectrum slot)
+        slots = [0] * len(layout.keys)
+        per_target = []
+        for t in targets:
+            count = [0] * len(layout.keys)
+            assign = []
+            for s in t.spectra:
+                g = layout.index[s.wavehash]
+                assign.append((g, count[g]))
+                count[g] += 1
+            slots = [max(a, b) for a, b in zip(slots, count)]
+            per_target.append(assign)
+        segs = []
+        seg_index = {}
+        rw_off = 0
+        for g in range(len(layout.keys)):
+            for sl in range(slots[g]):
+                seg_index[(g, sl)] = len(segs)
+                segs.append(_lib.SegmentDesc(layout.npix_pad[g], layout.pix_offset[g], rw_off))
+                rw_off += layout.npix_pad[g]
+        if len(segs) > 16:
+            raise NotImplementedError(f"{len(segs)} spectrum slots per target > 16")
+        self.segs = segs
+        self.npix_block = max(rw_off, 1)
+        descs, rdata, roffs, ivar, flux = [], [], [], [], []
+        first = [0]
+        data_off = pix_off = diag_off = 0
+        for it, (t, assign) in enumerate(zip(targets, per_target)):
+            blk, lane = divmod(it, _lib.LANES)
+            for s, (g, sl) in zip(t.spectra, assign):
+                d, o = spectrum_dia(s)
+                npix = len(s.wave)
+                if npix != layout.npix[g]:
+                    raise ValueError("spectrum length does not match its wavelength grid")
+                wide = np.abs(o) > _lib.HALF_BAND
+                if np.any(wide) and np.any(d[wide] != 0):
+                    raise NotImplementedError("resolution bandwidth > 5 pixels is not supported")
+                descs.append(_lib.SpectrumDesc(npix, data_off, pix_off, d.shape[0], diag_off, blk,
+                                               lane, seg_index[(g, sl)], 0))
+                rdata.append(d)
+                roffs.append(o)
+                ivar.append(s.ivar)
+                flux.append(s.flux)
+                data_off += d.size
+                pix_off += npix
+                diag_off += d.shape[0]
+            first.append(len(descs))
+        self.nspec = len(descs)
+        self.descs = struct_bytes(descs)
+        self.segs_bytes = struct_bytes(segs)
+        self.first = np.asarray(first, dtype=np.int64)
+        self.rows = np.full(self.nblock * _lib.LANES, -1, dtype=np.int32)
+        self.rows[:self.ntarget] = np.arange(self.ntarget, dtype=np.int32)
+        self.rdata = _concat([np.asarray(d, dtype=np.float64).ravel() for d in rdata], np.float64)
+        self.roffs = _concat([np.asarray(o, dtype=np.int32) for o in roffs], np.int32)
+        self.ivar = _concat([np.asarray(v, dtype=np.float64) for v in ivar], np.float64)
+        self.flux = _concat([np.asarray(v, dtype=np.float64) for v in flux], np.float64)
+
+    def host_arrays(self):
+        return (self.descs, self.segs_bytes, self.first, self.rows, self.rdata, self.roffs,
+                self.ivar, self.flux)
+
+    @property
+    def nbytes(self):
+        return sum(a.nbytes for a in self.host_arrays())
+
+    def to_device(self):
+        return DeviceTargetBatch(self)
+
+
+def _concat(parts, dtype):
+    n = sum(p.size for p in parts)
+    out = np.empty(n, dtype=dtype)
+    i = 0
+    for p in parts:
+        out[i:i + p.size] = p
+        i += p.size
+    return out
+
+
+class DeviceTargetBatch:
+    """The raw arrays of a TargetBatch resident on the device."""
+
+    def __init__(self, batch):
+        self.batch = batch
+        self.descs = to_device(batch.descs, torch.uint8)
+        self.segs = to_device(batch.segs_bytes, torch.uint8)
+        self.first = to_device(batch.first, torch.int64)
+        self.rows = to_device(batch.rows, torch.int32)
+        self.rdata = to_device(batch.rdata)
+        self.roffs = to_device(batch.roffs, torch.int32)
+        self.ivar = to_device(batch.ivar)
+        self.flux = to_device(batch.flux)
+
+
+class TargetPack:
+    """Targets packed for the fused scan (rr_pack_targets)."""
+
+    def __init__(self, dbatch, stream=None, status=None):
+        L = _lib.lib()
+        dev = device()
+        b = dbatch.batch
+        self.layout = b.layout
+        self.ntarget = b.ntarget
+        self.nblock = b.nblock
+        self.segs = b.segs
+        self.npix_block = b.npix_block
+        self.rows = dbatch.rows
+        self.rw = torch.zeros((b.nblock, b.npix_block, _lib.RW, _lib.LANES), dtype=torch.float64,
+                              device=dev)
+        self.fwf = torch.zeros(b.nblock * _lib.LANES, dtype=torch.float64, device=dev)
+        self.wsum = torch.zeros(b.nblock * _lib.LANES, dtype=torch.float64, device=dev)
+        self._status = status or StatusWord(dev)
+        if b.nspec:
+            rc = L.rr_pack_targets(ptr(dbatch.descs), b.nspec, ptr(dbatch.first), b.ntarget,
+                                   ptr(dbatch.rdata), ptr(dbatch.roffs), ptr(dbatch.ivar),
+                                   ptr(dbatch.flux), ptr(dbatch.segs), len(b.segs), b.npix_block,
+                                   b.nblock, ptr(self.rw), ptr(self.fwf), ptr(self.wsum),
+                                   self._status.ptr, stream_handle(stream))
+            _lib.check(rc, "rr_pack_targets")
+
+    @classmethod
+    def from_targets(cls, targets, layout, stream=None):
+        return cls(TargetBatch(targets, layout).to_device(), stream=stream)
+
+    def check(self):
+        self._status.check("rr_pack_targets")
+
+    def scan_targets_struct(self):
+        arr = (_lib.SegmentDesc * len(self.segs))(*self.segs)
+        self._segarr = arr
+        return _lib.ScanTargets(ptr(self.rw), ptr(self.fwf), ptr(self.wsum), ptr(self.rows),
+                                ctypes.cast(arr, ctypes.c_void_p).value, self.nblock,
+                                len(self.segs), self.npix_block)
+
+
+class ScanResult:
+    def __init__(self, ntarget, basis, dev):
+        self.zchi2 = torch.empty((ntarget, basis.nz), dtype=torch.float64, device=dev)
+        self.zcoeff = torch.empty((ntarget, basis.nz, basis.nbasis), dtype=torch.float64,
+                                  device=dev)
+        self.penalty = torch.zeros((ntarget, basis.nz), dtype=torch.float64, device=dev)
+
+
+def run_fused(pack, bases, stream=None, status=None):
+    """One persistent launch over every (target, template, z)."""
+    L = _lib.lib()
+    dev = device()
+    results = [ScanResult(pack.ntarget, b, dev) for b in bases]
+    tgs = pack.scan_targets_struct()
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = status or StatusWord(dev)
+    for i0 in range(0, len(bases), _lib.MAX_TEMPLATES):
+        chunk = list(range(i0, min(len(bases), i0 + _lib.MAX_TEMPLATES)))
+        tms = []
+        for i in chunk:
+            b, r = bases[i], results[i]
+            if b.layout.signature != pack.layout.signature:
+                raise ValueError("template basis and targets use different wavelength grids")
+            tms.append(_lib.ScanTemplate(ptr(b.basis), b.layout.pix_stride, b.nz, b.nbasis,
+                                         b.stride, b.method, ptr(b.prior), ptr(b.oii),
+                                         ptr(r.zchi2), ptr(r.zcoeff),
+                                         ptr(r.penalty) if b.oii is not None else None))
+        arr = (_lib.ScanTemplate * len(tms))(*tms)
+        rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
+                              stream_handle(stream))
+        _lib.check(rc, "rr_zscan_fused")
+    return results, st
+
+
+# ---------------------------------------------------------------------------
+# plain per-target path
+# ---------------------------------------------------------------------------
+class PlainTarget:
+    """One target's spectra as band rows for the plain path."""
+
+    def __init__(self, spectra, layout, weights=None, flux=None, wflux=None, stream=None):
+        L = _lib.lib()
+        dev = device()
+        descs, rdata, roffs, pix_basis = [], [], [], []
+        data_off = pix_off = diag_off = 0
+        for s in spectra:
+            g = layout.index[s.wavehash]
+            d, o = spectrum_dia(s)
+            npix = len(s.wave)
+            if np.any(np.abs(o) > _lib.HALF_BAND) and np.any(d[np.abs(o) > _lib.HALF_BAND] != 0):
+                raise NotImplementedError("resolution bandwidth > 5 pixels is not supported")
+            d = np.ascontiguousarray(d, dtype=np.float64)
+            descs.append(_lib.SpectrumDesc(npix, data_off, pix_off, d.shape[0], diag_off, 0, 0, 0,
+                                           0))
+            rdata.append(d.ravel())
+            roffs.append(np.asarray(o, dtype=np.int32))
+            pix_basis.append(layout.pix_offset[g] + np.arange(npix, dtype=np.int64))
+            data_off += d.size
+            pix_off += npix
+            diag_off += d.shape[0]
+        self.npix = pix_off
+        if weights is None:
+            weights = np.concatenate([s.ivar for s in spectra])
+            flux = np.concatenate([s.flux for s in spectra])
+            wflux = weights * flux
+        self.w = to_device(weights)
+        self.flux = to_device(flux)
+        self.wflux = to_device(wflux)
+        self.pix_basis = to_device(np.concatenate(pix_basis), torch.int64)
+        self.band = torch.empty((self.npix, 2 * _lib.HALF_BAND + 1), dtype=torch.float64,
+                                device=dev)
+        dspecs = to_device(struct_bytes(descs), torch.uint8)
+        drdata = to_device(np.concatenate(rdata))
+        droff = to_device(np.concatenate(roffs), torch.int32)
+        st = StatusWord(dev)
+        rc = L.rr_pack_band_rows(ptr(dspecs), len(descs), ptr(drdata), ptr(droff), self.npix,
+                                 ptr(self.band), st.ptr, stream_handle(stream))
+        _lib.check(rc, "rr_pack_band_rows")
+        self._keep = (dspecs, drdata, droff)
+        self._status = st
+
+
+_plain_ws = {}
+
+
+def run_plain(pt, basis, prior=None, method=_lib.RR_SOLVE_PCA, stream=None):
+    """zchi2 (nz,), zcoeff (nz, nb) device tensors for one target."""
+    L = _lib.lib()
+    dev = device()
+    nz, nb = basis.nz, basis.nbasis
+    zchi2 = torch.empty(nz, dtype=torch.float64, device=dev)
+    zcoeff = torch.empty((nz, nb), dtype=torch.float64, device=dev)
+    need = int(L.rr_zchi2_batch_plain_workspace_bytes(pt.npix, nz, nb))
+    ws = _plain_ws.get(dev.index)
+    if ws is None or ws.numel() < need:
+        ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+        _plain_ws[dev.index] = ws
+    dprior = None if prior is None else to_device(prior)
+    rc = L.rr_zchi2_batch_plain(ptr(pt.band), ptr(pt.w), ptr(pt.wflux), ptr(pt.flux),
+                                ptr(pt.pix_basis), pt.npix, ptr(basis.basis),
+                                basis.layout.pix_stride, nz, nb, basis.stride, ptr(dprior), method,
+                                ptr(zchi2), ptr(zcoeff), ptr(ws), ws.numel(), pt._status.ptr,
+                                stream_handle(stream))
+    _lib.check(rc, "rr_zchi2_batch_plain")
+    return zchi2, zcoeff
+
+
+# ---------------------------------------------------------------------------
+# small LRU caches keyed by object identity
+# ---------------------------------------------------------------------------
+class IdCache:
+    def __init__(self, size=8):
+        self.size = size
+        self.d = OrderedDict()
+
+    def get(self, key, objs, make):
+        hit = self.d.get(key)
+        if hit is not None and all(a is b for a, b in zip(hit[0], objs)) and len(hit[0]) == len(objs):
+            self.d.move_to_end(key)
+            return hit[1]
+        val = make()
+        self.d[key] = (list(objs), val)
+        self.d.move_to_end(key)
+        while len(self.d) > self.size:
+            self.d.popitem(last=False)
+        return val
+
+    def clear(self):
+        self.d.clear()

@@ -1,0 +1,231 @@
+"""Drop-in redshift-scan functions (redrock 0.22 zscan.py) on the GPU.
+
+  calc_zchi2          zscan.py:807-889   all targets x all z in one fused
+                                         launch (rr_zscan_fused)
+  calc_zchi2_targets  zscan.py:910-1105  every template in the same launch
+  calc_zchi2_batch    zscan.py:626-781   one target, plain kernel chain
+                                         (rr_zchi2_batch_plain)
+  calc_zchi2_one      zscan.py:213-243   one z (plain chain with nz = 1)
+  calc_negOII_penalty zscan.py:783-800
+  spectral_data       zscan.py:192-209
+
+Inputs are redrock's own objects (or the mirrors in redrock_b200.targets /
+redrock_b200.templates); outputs are the same numpy arrays with the same
+shapes.  Error conventions follow redrock: all-zero weights give HUGE_CHI2
+rows with zero coefficients; an exactly singular normal matrix gives
+HUGE_CHI2 at that z; an unrecognised solve method gives HUGE_CHI2
+everywhere.  Non-negative / bounded solvers (NMF, NNLS, BVLS) raise
+NotImplementedError instead of silently running on the CPU.
+"""
+
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import to_device, to_numpy
+from .engine import DeviceBasis, GridLayout, IdCache, PlainTarget, TargetPack, run_fused, run_plain
+from .templates import oii_sums, solve_code
+
+HUGE_CHI2 = 9999999.0
+
+_pack_cache = IdCache(4)
+_basis_cache = IdCache(32)
+
+
+def spectral_data(spectra):
+    weights = np.concatenate([s.ivar for s in spectra])
+    flux = np.concatenate([s.flux for s in spectra])
+    return (weights, flux, weights * flux)
+
+
+def calc_negOII_penalty(OIItemplate, coeff):
+    """penalty[nz] = max(0, -sum over the [OII] window of the model)."""
+    coeff_t = coeff if isinstance(coeff, torch.Tensor) else to_device(coeff)
+    s = to_device(np.asarray(OIItemplate, dtype=np.float64).sum(axis=1))
+    nz, nb = coeff_t.shape
+    out = torch.empty(nz, dtype=torch.float64, device=coeff_t.device)
+    from .device import ptr, stream_handle
+    rc = _lib.lib().rr_negoii_penalty(ptr(coeff_t.contiguous()), nz, nb, ptr(s), ptr(out),
+                                      stream_handle())
+    _lib.check(rc, "rr_negoii_penalty")
+    return out if isinstance(coeff, torch.Tensor) else out.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def _layout_for(dtemplate, targets):
+    lay = getattr(dtemplate, "layout", None)
+    if isinstance(lay, GridLayout):
+        return lay
+    data = dtemplate.local.data
+    waves = {}
+    for t in targets:
+        for s in t.spectra:
+            waves.setdefault(s.wavehash, s.wave)
+    return GridLayout((k, v.shape[1], waves.get(k)) for k, v in data.items())
+
+
+def _device_basis(dtemplate, layout):
+    b = getattr(dtemplate, "basis", None)
+    if isinstance(b, DeviceBasis):
+        return b
+    tmpl = dtemplate.template
+
+    def make():
+        return DeviceBasis.from_tdata(dtemplate.local.data, layout,
+                                      redshifts=dtemplate.local.redshifts, oii=oii_sums(tmpl),
+                                      method=solve_code(tmpl))
+    return _basis_cache.get(("dt", id(dtemplate), layout.signature), [dtemplate], make)
+
+
+def _pack(targets, layout):
+    def make():
+        p = TargetPack.from_targets(targets, layout)
+        torch.cuda.current_stream().synchronize()
+        p.check()
+        return p
+    return _pack_cache.get(("pack", layout.signature, len(targets)), targets, make)
+
+
+# ---------------------------------------------------------------------------
+# fused scan
+# ---------------------------------------------------------------------------
+def scan_device(targets, dtemplates):
+    """Fused scan of every target against every template.
+
+    Returns a list (one entry per template) of device ScanResult objects
+    with zchi2 (T, nz), zcoeff (T, nz, nbasis), penalty (T, nz).
+    """
+    layout = _layout_for(dtemplates[0], targets)
+    bases = []
+    for dt in dtemplates:
+        b = _device_basis(dt, layout)
+        if b.layout.signature != layout.signature:
+            # templates built on other grids: re-layout through the dict view
+            b = DeviceBasis.from_tdata(dt.local.data, layout, redshifts=dt.local.redshifts,
+                                       oii=oii_sums(dt.template), method=solve_code(dt.template))
+        bases.append(b)
+    pack = _pack(targets, layout)
+    results, st = run_fused(pack, bases)
+    torch.cuda.current_stream().synchronize()
+    st.check("rr_zscan_fused")
+    return results
+
+
+def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False):
+    """chi2 vs redshift of every target for one template (zscan.py:807)."""
+    ntargets = len(target_ids)
+    nz = len(dtemplate.local.redshifts)
+    nbasis = dtemplate.template.nbasis
+    if ntargets == 0:
+        return np.zeros((0, nz)), np.zeros((0, nz, nbasis)), np.zeros((0, nz))
+    res = scan_device(list(target_data), [dtemplate])[0]
+    zchi2 = res.zchi2.cpu().numpy()
+    zcoeff = res.zcoeff.cpu().numpy()
+    pen = res.penalty.cpu().numpy()
+    if dtemplate.comm is None and progress is not None:
+        for _ in range(ntargets):
+            progress.put(1)
+    return zchi2, zcoeff, pen
+
+
+def calc_zchi2_targets(targets, templates, mp_procs=1, use_gpu=True):
+    """All templates for all local targets in one fused launch (zscan.py:910)."""
+    am_root = targets.comm is None or targets.comm.rank == 0
+    tids = list(targets.local_target_ids())
+    results = {tid: {} for tid in tids}
+    if am_root:
+        print("Computing redshifts")
+        sys.stdout.flush()
+    if len(tids) == 0:
+        return results
+    out = scan_device(list(targets.local()), list(templates))
+    for t, r in zip(templates, out):
+        ft = t.template.full_type
+        zc = r.zchi2.cpu().numpy()
+        co = r.zcoeff.cpu().numpy()
+        pe = r.penalty.cpu().numpy()
+        for i, tid in enumerate(tids):
+            results[tid][ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
+                                    zcoeff=co[i])
+    return results
+
+
+# ---------------------------------------------------------------------------
+# plain per-target path
+# ---------------------------------------------------------------------------
+def _plain_layout(spectra, tdata):
+    waves = {}
+    for s in spectra:
+        waves.setdefault(s.wavehash, s.wave)
+    keys = list(dict.fromkeys(s.wavehash for s in spectra))
+    return GridLayout((k, tdata[k].shape[-2], waves[k]) for k in keys)
+
+
+def calc_zchi2_batch(spectra, tdata, weights, flux, wflux, nz, nbasis,
+                     solve_matrices_algorithm=None, solver_args=None, use_gpu=False,
+                     fullprecision=True, prior=None):
+    """chi2 and coefficients of one target for all z (zscan.py:626)."""
+    wh = to_numpy(weights)
+    if wh.sum() == 0:
+        return np.full(nz, HUGE_CHI2), np.zeros((nz, nbasis))
+    method = _lib.RR_SOLVE_PCA
+    if solve_matrices_algorithm is not None:
+        m = str(solve_matrices_algorithm).upper()
+        if m in ('NMF', 'NNLS', 'BVLS'):
+            raise NotImplementedError(f"solve_matrices_algorithm {m} is not implemented by the "
+                                      "GPU scan engine")
+        if m != 'PCA':
+            method = _lib.RR_SOLVE_UNSUPPORTED
+    layout = _plain_layout(spectra, tdata)
+    sub = {k: tdata[k] for k in layout.keys}
+    basis = DeviceBasis.from_tdata(sub, layout)
+    pt = PlainTarget(spectra, layout, weights, flux, wflux)
+    zchi2, zcoeff = run_plain(pt, basis, prior=prior, method=method)
+    torch.cuda.current_stream().synchronize()
+    pt._status.check("rr_zchi2_batch_plain")
+    if use_gpu:
+        return zchi2.cpu().numpy(), zcoeff
+    return zchi2.cpu().numpy(), zcoeff.cpu().numpy()
+
+
+def calc_zchi2_one(spectra, weights, flux, wflux, tdata, solve_matrices_algorithm):
+    """chi2 and coefficients at one redshift (zscan.py:213)."""
+    t3 = {k: (v[None] if isinstance(v, torch.Tensor) else np.asarray(v)[None])
+          for k, v in tdata.items()}
+    nbasis = next(iter(t3.values())).shape[-1]
+    zc, co = calc_zchi2_batch(spectra, t3, weights, flux, wflux, 1, nbasis,
+                              solve_matrices_algorithm)
+    return float(zc[0]), np.asarray(to_numpy(co))[0]
+
+
+def calc_zchi2_plain(target_ids, target_data, dtemplate):
+    """calc_zchi2 through the plain per-target kernel chain (the structure of
+    redrock's own GPU branch: one chain of launches and one host read-back
+    per target).  Used as the comparison path for the fused scan."""
+    ntargets = len(target_ids)
+    nz = len(dtemplate.local.redshifts)
+    nbasis = dtemplate.template.nbasis
+    zchi2 = np.zeros((ntargets, nz))
+    zcoeff = np.zeros((ntargets, nz, nbasis))
+    pen = np.zeros((ntargets, nz))
+    layout = _layout_for(dtemplate, target_data)
+    basis = _device_basis(dtemplate, layout)
+    oii = oii_sums(dtemplate.template)
+    for j, t in enumerate(target_data):
+        w, f, wf = spectral_data(t.spectra)
+        if np.sum(w) == 0:
+            zchi2[j, :] = HUGE_CHI2
+            continue
+        pt = PlainTarget(t.spectra, layout, w, f, wf)
+        zc, co = run_plain(pt, basis, method=basis.method)
+        zchi2[j] = zc.cpu().numpy()
+        zcoeff[j] = co.cpu().numpy()
+        if oii is not None:
+            pen[j] = calc_negOII_penalty(dtemplate.template.OIItemplate, co).cpu().numpy()
+    return zchi2, zcoeff, pen

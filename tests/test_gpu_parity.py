@@ -1,0 +1,297 @@
+"""CUDA path (through the C ABI) against the oracle and redrock's fixtures.
+
+Tolerances (FP64 everywhere on the GPU):
+  * rebin: bit-identical to redrock's CPU rebin (checksums of redrock's own
+    output and the oracle's);
+  * IGM transmission: relative 1e-13 (CUDA pow/exp vs libm, <= 2 ulp each);
+  * chi2: |dchi2| <= 1e-3 absolute (the acceptance bar) and also relative
+    1e-9, identical argmin per target;
+  * coefficients: |dc| <= 1e-5 * max|c| per (target, z).
+"""
+
+import numpy as np
+import pytest
+
+from tests.conftest import cuda_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+from oracle import oracle as O  # noqa: E402
+from redrock_b200 import synth  # noqa: E402
+
+DCHI2_ABS = 1e-3
+DCHI2_REL = 1e-9
+COEFF_REL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def rr():
+    import redrock_b200
+    from redrock_b200 import igm, rebin, targets, templates, zscan
+    return dict(igm=igm, rebin=rebin, targets=targets, templates=templates, zscan=zscan,
+                pkg=redrock_b200)
+
+
+def assert_chi2(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    d = np.abs(a - b)
+    assert d.max() <= DCHI2_ABS, f"max |dchi2| {d.max()}"
+    assert np.all(d <= DCHI2_REL * np.maximum(np.abs(b), 1.0)), f"rel {np.max(d / np.abs(b))}"
+
+
+def assert_coeff(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    scale = np.maximum(np.abs(b).max(axis=-1, keepdims=True), 1e-300)
+    assert np.all(np.abs(a - b) <= COEFF_REL * scale), np.max(np.abs(a - b) / scale)
+
+
+# ---------------------------------------------------------------------------
+# rebin
+# ---------------------------------------------------------------------------
+def test_rebin_known_answers(rr, golden):
+    tr = rr["rebin"].trapz_rebin
+    x = np.arange(10.)
+    y = np.ones((2, 10))
+    y[1] = np.arange(10)
+    np.testing.assert_array_equal(tr(x, y, edges=[0, 2, 4, 6, 8], myz=[0.0, 0.5]),
+                                  golden["rebin_doc"])
+    np.testing.assert_array_equal(tr(x, y, edges=[0, 2, 4, 6, 8]), golden["rebin_doc"][0])
+    xu = np.linspace(0, 10, 100) ** 2
+    np.testing.assert_array_equal(tr(xu, np.sqrt(xu), edges=np.linspace(0, 100, 21)),
+                                  golden["rebin_uneven"])
+    xs = np.linspace(0, 2 * np.pi, 100)
+    np.testing.assert_array_equal(
+        tr(xs, np.sin(xs), edges=[0, 0.5 * np.pi, np.pi, 1.5 * np.pi, 2 * np.pi]),
+        golden["rebin_sin"])
+    # constant density stays exactly 1 for every binning (redrock test_rebin)
+    x = np.arange(10) * 1.1
+    for nedge in range(3, 10):
+        assert np.all(tr(x, np.ones(10), edges=np.linspace(x.min(), x.max(), nedge)) == 1.0)
+
+
+def test_rebin_shapes_and_errors(rr):
+    tr = rr["rebin"].trapz_rebin
+    x = np.arange(10.)
+    y = np.ones(10)
+    assert tr(x, y, edges=[0, 2, 4, 6, 8]).shape == (4,)
+    assert tr(x, y, edges=[0, 2, 4, 6, 8], myz=[0, 0.1]).shape == (2, 4)
+    assert tr(x, y[None], edges=[0, 2, 4, 6, 8], myz=[0, 0.1]).shape == (2, 4, 1)
+    assert tr(x, y, edges=[0, 2, 4], myz=np.array([])).shape == (0, 2, 1)
+    with pytest.raises(ValueError):
+        tr(x, y, edges=np.arange(-1, 9))
+    with pytest.raises(ValueError):
+        tr(x, y, edges=np.arange(1, 11))
+    d = tr(x, y, edges=[0, 2, 4, 6, 8], myz=[0, 0.1], use_gpu=True)
+    assert d.is_cuda
+
+
+@pytest.mark.parametrize("key", ["GALAXY", "QSO", "STAR_G"])
+def test_rebin_bit_exact_desi_grids(rr, golden, key):
+    grids = synth.camera_grids()
+    ts = {t.full_type.replace(":::", "_"): t for t in synth.template_set()}[key]
+    zz = golden[f"basis_{key}_z"]
+    r = rr["rebin"].trapz_rebin(ts.wave, ts.flux, xnew=grids["b"], myz=zz)
+    assert synth.checksum([r]) == str(golden[f"rebin_{key}_b_sha"])
+    # whole grid, every z, against the oracle restatement
+    zfull = ts.redshifts[::37]
+    for cam, w in grids.items():
+        a = rr["rebin"].trapz_rebin(ts.wave, ts.flux, xnew=w, myz=zfull)
+        b = O.trapz_rebin(ts.wave, ts.flux, xnew=w, myz=zfull)
+        np.testing.assert_array_equal(a, b)
+
+
+# ---------------------------------------------------------------------------
+# IGM
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("model", ["Inoue14", "Calura12", "Kamble20"])
+def test_igm(rr, golden, model):
+    T = rr["igm"].transmission_Lyman(golden["igm_z"], golden["igm_lobs"], model=model)
+    np.testing.assert_allclose(T, golden[f"igm_{model}"], rtol=1e-13, atol=1e-300)
+
+
+def test_igm_shapes_high_z(rr, golden):
+    tl = rr["igm"].transmission_Lyman
+    np.testing.assert_allclose(tl(4.2, golden["igm_lobs"], model="Inoue14"),
+                               golden["igm_Inoue14_scalar_z"], rtol=1e-13)
+    np.testing.assert_allclose(tl(golden["igm_z"], 3650.0, model="Inoue14"),
+                               golden["igm_Inoue14_scalar_l"], rtol=1e-13)
+    np.testing.assert_allclose(tl(golden["igm_hi_z"], golden["igm_hi_lobs"], model="Inoue14"),
+                               golden["igm_hi_Inoue14"], rtol=1e-13, atol=1e-300)
+    assert tl(np.array([0.1, 0.2]), np.array([5000.0, 6000.0]), model="Inoue14",
+              always_return_array=False) is None
+    assert tl(np.array([3.0]), np.array([3600.0]), model="None", always_return_array=False) is None
+    assert np.all(tl(np.array([3.0]), np.array([3600.0, 4000.0]), model="None") == 1.0)
+    assert isinstance(tl(3.0, 3600.0, model="Calura12"), float)
+    with pytest.raises(ValueError):
+        tl(1.0, 1000.0, model="bogus")
+
+
+# ---------------------------------------------------------------------------
+# bases (fused rebin + IGM)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("key", ["GALAXY", "QSO", "STAR_G"])
+def test_dist_template_basis(rr, golden, key):
+    grids = synth.camera_grids()
+    ts = {t.full_type.replace(":::", "_"): t for t in synth.template_set()}[key]
+    ts.redshifts = golden[f"basis_{key}_z"]
+    dt = rr["templates"].DistTemplate(rr["templates"].from_synth(ts), grids)
+    data = dt.local.data
+    ref = O.template_basis(ts.wave, ts.flux, ts.redshifts, grids, ts.igm_model)
+    for cam in grids:
+        np.testing.assert_allclose(data[cam][:, ::13], golden[f"basis_{key}_{cam}_sample"],
+                                   rtol=1e-13, atol=0)
+        np.testing.assert_allclose(data[cam], ref[cam], rtol=1e-13, atol=0)
+        if key != "QSO":   # no IGM factor on these grids: rebin only -> bit exact
+            assert synth.checksum([data[cam]]) == str(golden[f"basis_{key}_{cam}_sha"])
+
+
+# ---------------------------------------------------------------------------
+# fused scan
+# ---------------------------------------------------------------------------
+def scan_case():
+    tg = synth.make_targets(4, seed=11, amp=1.0)
+    tg += synth.make_targets(1, seed=12, mask_range=(0.4, 0.4), first_id=2000)
+    tg += synth.make_targets(1, seed=13, drop_camera_frac=1.0, first_id=3000)
+    tg += synth.make_targets(1, seed=14, first_id=4000)
+    for s in tg[-1].spectra:
+        s.ivar[:] = 0.0
+    return tg
+
+
+def ospectra(t):
+    return [O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets) for s in t.spectra]
+
+
+@pytest.mark.parametrize("key", ["GALAXY", "QSO", "STAR_G"])
+def test_calc_zchi2_vs_redrock(rr, golden, key):
+    tg = scan_case()
+    assert synth.targets_checksum(tg) == str(golden["scan_targets_sha"])
+    ts = {t.full_type.replace(":::", "_"): t for t in synth.template_set()}[key]
+    ts.redshifts = golden[f"scan_{key}_z"]
+    T, TM = rr["targets"], rr["templates"]
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    dt = TM.DistTemplate(TM.from_synth(ts), dtg.wavegrids())
+    zc, co, pe = rr["zscan"].calc_zchi2(dtg.local_target_ids(), dtg.local(), dt)
+    assert zc.shape == golden[f"scan_{key}_zchi2"].shape
+    assert_chi2(zc, golden[f"scan_{key}_zchi2"])
+    assert_coeff(co[:-1], golden[f"scan_{key}_zcoeff"][:-1])
+    np.testing.assert_allclose(pe, golden[f"scan_{key}_penalty"], rtol=1e-8, atol=1e-8)
+    assert np.all(zc[-1] == 9999999.0) and np.all(co[-1] == 0.0) and np.all(pe[-1] == 0.0)
+    np.testing.assert_array_equal(np.argmin(zc, axis=1),
+                                  np.argmin(golden[f"scan_{key}_zchi2"], axis=1))
+
+
+def test_calc_zchi2_targets_all_templates_one_launch(rr):
+    tg = synth.make_targets(37, seed=3, mask_range=(0.0, 0.4), drop_camera_frac=0.1)
+    T, TM = rr["targets"], rr["templates"]
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    dwave = dtg.wavegrids()
+    tset = synth.template_set(zsub=97)
+    dts = [TM.DistTemplate(TM.from_synth(ts), dwave) for ts in tset]
+    res = rr["zscan"].calc_zchi2_targets(dtg, dts)
+    grids = synth.camera_grids()
+    pick = [0, 17, 36]   # lanes in the first and second target block
+    for ts in tset:
+        tdata = O.template_basis(ts.wave, ts.flux, ts.redshifts, grids, ts.igm_model)
+        oii = O.oii_template(ts.wave, ts.flux) if ts.spectype == "GALAXY" else None
+        ozc, oco, ope = O.calc_zchi2([ospectra(tg[i]) for i in pick], tdata, len(ts.redshifts),
+                                     ts.flux.shape[0], OIItemplate=oii)
+        for j, i in enumerate(pick):
+            r = res[tg[i].targetid][ts.full_type]
+            assert_chi2(r["zchi2"], ozc[j])
+            assert_coeff(r["zcoeff"], oco[j])
+            np.testing.assert_allclose(r["penalty"], ope[j], rtol=1e-8, atol=1e-8)
+
+
+def test_util_fixture_two_exposures(rr, golden):
+    ut = [synth.util_target(0.2, seed=21, targetid=111),
+          synth.util_target(0.25, seed=22, targetid=222)]
+    T, TM = rr["targets"], rr["templates"]
+    dtg = T.DistTargetsCopy(T.from_synth(ut))
+    uw, uf = synth.util_template()
+    tm = TM.Template(spectype="GALAXY", redshifts=np.linspace(0.15, 0.3, 50), wave=uw, flux=uf,
+                     subtype="")
+    dt = TM.DistTemplate(tm, dtg.wavegrids())
+    res = rr["zscan"].calc_zchi2_targets(dtg, [dt])
+    for t in ut:
+        r = res[t.targetid]["GALAXY"]
+        assert_chi2(r["zchi2"], golden[f"util_{t.targetid}_zchi2"])
+        assert_coeff(r["zcoeff"], golden[f"util_{t.targetid}_zcoeff"])
+        np.testing.assert_allclose(r["penalty"], golden[f"util_{t.targetid}_penalty"], atol=1e-8)
+
+
+def test_singular_and_methods(rr, golden):
+    tg = scan_case()[:1]
+    gal = synth.template_set()[0]
+    T, TM = rr["targets"], rr["templates"]
+    rtg = T.from_synth(tg)
+    dtg = T.DistTargetsCopy(rtg)
+    sflux = gal.flux.copy()
+    sflux[3] = 0.0
+    tm = TM.Template(spectype="GALAXY", redshifts=golden["prior_z"], wave=gal.wave, flux=sflux,
+                     subtype="")
+    dt = TM.DistTemplate(tm, dtg.wavegrids())
+    zc, co, pe = rr["zscan"].calc_zchi2(dtg.local_target_ids(), dtg.local(), dt)
+    np.testing.assert_array_equal(zc, golden["singular_zchi2"])
+    np.testing.assert_array_equal(co, golden["singular_zcoeff"])
+    np.testing.assert_array_equal(pe, golden["singular_penalty"])
+    # NMF has no GPU solver: a clear error instead of a silent CPU run
+    tm2 = TM.Template(spectype="STAR", subtype="X", redshifts=golden["prior_z"], wave=gal.wave,
+                      flux=gal.flux, method="NMF")
+    with pytest.raises(NotImplementedError):
+        TM.DistTemplate(tm2, dtg.wavegrids())
+
+
+def test_plain_batch_prior_and_one(rr, golden):
+    tg = scan_case()[:1]
+    gal = synth.template_set()[0]
+    grids = synth.camera_grids()
+    zb = golden["prior_z"]
+    tdata = O.template_basis(gal.wave, gal.flux, zb, grids, gal.igm_model)
+    T = rr["targets"]
+    sp = T.from_synth(tg)[0].spectra
+    w, f, wf = rr["zscan"].spectral_data(sp)
+    zc, co = rr["zscan"].calc_zchi2_batch(sp, tdata, w, f, wf, len(zb), 10, "PCA",
+                                          prior=golden["prior_matrix"])
+    assert_chi2(zc, golden["prior_zchi2"])
+    assert_coeff(co, golden["prior_zcoeff"])
+    for i in range(len(zb)):
+        c2, c = rr["zscan"].calc_zchi2_one(sp, w, f, wf, {k: v[i] for k, v in tdata.items()},
+                                           "PCA")
+        assert abs(c2 - golden["one_zchi2"][i]) <= DCHI2_ABS
+        assert_coeff(c[None], golden["one_zcoeff"][i][None])
+    zc, co = rr["zscan"].calc_zchi2_batch(sp, tdata, w, f, wf, len(zb), 10, "SOMETHING")
+    assert np.all(zc == 9999999.0)
+    zc, co = rr["zscan"].calc_zchi2_batch(sp, tdata, 0 * w, f, wf, len(zb), 10, "PCA")
+    assert np.all(zc == 9999999.0) and np.all(co == 0)
+
+
+def test_fused_equals_plain_full_grid(rr):
+    """Size-independent property at the full GALAXY/QSO grids: the fused
+    persistent kernel and the plain per-target chain agree."""
+    tg = synth.make_targets(3, seed=7)
+    T, TM = rr["targets"], rr["templates"]
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    dwave = dtg.wavegrids()
+    for ts in synth.template_set(stars=("K",))[:2]:
+        dt = TM.DistTemplate(TM.from_synth(ts), dwave)
+        a = rr["zscan"].calc_zchi2(dtg.local_target_ids(), dtg.local(), dt)
+        b = rr["zscan"].calc_zchi2_plain(dtg.local_target_ids(), dtg.local(), dt)
+        assert_chi2(a[0], b[0])
+        assert_coeff(a[1], b[1])
+        np.testing.assert_allclose(a[2], b[2], rtol=1e-7, atol=1e-7)
+
+
+def test_best_z_recovers_truth_high_snr(rr):
+    tg = synth.make_targets(6, seed=19, amp=8.0, zrange=(0.2, 1.4))
+    T, TM = rr["targets"], rr["templates"]
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    gal = synth.template_set()[0]
+    dt = TM.DistTemplate(TM.from_synth(gal), dtg.wavegrids())
+    zc, co, pe = rr["zscan"].calc_zchi2(dtg.local_target_ids(), dtg.local(), dt)
+    zbest = gal.redshifts[np.argmin(zc, axis=1)]
+    ztrue = np.array([t.ztrue for t in tg])
+    assert np.all(np.abs(np.log1p(zbest) - np.log1p(ztrue)) <= 3e-4)

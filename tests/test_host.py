@@ -1,0 +1,125 @@
+"""Host-side logic that needs no GPU: layouts, packing descriptors, the
+installer, work distribution."""
+import types
+
+import numpy as np
+import pytest
+
+from redrock_b200 import _lib, synth
+from redrock_b200.engine import GridLayout, TargetBatch, centers2edges, round_up
+from redrock_b200.install import PATCHES, install
+from redrock_b200.targets import DistTargetsCopy, distribute_work, from_synth
+
+
+def test_centers2edges_known():
+    assert np.allclose(centers2edges([1, 2, 3]), [0.5, 1.5, 2.5, 3.5])
+    assert np.allclose(centers2edges([1, 3, 5]), [0, 2, 4, 6])
+    assert np.allclose(centers2edges([1, 3, 4]), [0, 2, 3.5, 4.5])
+
+
+def test_grid_layout_padding():
+    lay = GridLayout.from_dwave(synth.camera_grids())
+    assert lay.npix == [2751, 2326, 2881]
+    assert lay.npix_pad == [2752, 2336, 2896]
+    assert lay.pix_offset[0] == 5
+    # each grid owns [offset - 5, offset + npix_pad + 5), end to end
+    for i in range(1, 3):
+        assert lay.pix_offset[i] - 5 == lay.pix_offset[i - 1] + lay.npix_pad[i - 1] + 5
+    assert lay.pix_stride == lay.pix_offset[-1] + lay.npix_pad[-1] + 5
+    assert all(p % _lib.CHUNK == 0 for p in lay.npix_pad)
+
+
+def test_target_batch_descriptors():
+    tg = from_synth(synth.make_targets(35, seed=1, drop_camera_frac=0.2))
+    lay = GridLayout.from_dwave(synth.camera_grids())
+    b = TargetBatch(tg, lay)
+    assert b.nblock == 2
+    assert len(b.segs) == 3
+    assert b.npix_block == sum(lay.npix_pad)
+    descs = np.frombuffer(b.descs.tobytes(), dtype=np.dtype([
+        ("npix", "i8"), ("data_offset", "i8"), ("pix_offset", "i8"), ("ndiag", "i4"),
+        ("diag_offset", "i4"), ("block", "i4"), ("lane", "i4"), ("segment", "i4"),
+        ("pad", "i4")]))
+    assert len(descs) == b.nspec == sum(len(t.spectra) for t in tg)
+    assert b.first[-1] == b.nspec and np.all(np.diff(b.first) >= 2)
+    assert np.all(descs["ndiag"] == 11)
+    assert b.ivar.size == descs["npix"].sum()
+    # target i -> (block, lane) = divmod(i, 32)
+    tid = np.repeat(np.arange(len(tg)), np.diff(b.first))
+    assert np.all(descs["block"] == tid // 32) and np.all(descs["lane"] == tid % 32)
+    assert list(b.rows[:35]) == list(range(35)) and np.all(b.rows[35:] == -1)
+
+
+def test_multi_exposure_segments():
+    ut = from_synth([synth.util_target(0.2, 1, 111), synth.util_target(0.3, 2, 222)])
+    dw = {s.wavehash: s.wave for t in ut for s in t.spectra}
+    lay = GridLayout.from_dwave(dw)
+    b = TargetBatch(ut, lay)
+    # two exposures per camera -> two slots per grid
+    assert len(b.segs) == 4
+
+
+def test_wide_band_rejected():
+    tg = from_synth(synth.make_targets(1, seed=1))
+    s = tg[0].spectra[0]
+    import scipy.sparse
+    n = len(s.wave)
+    data = np.ones((13, n)) / 13
+    s.R = scipy.sparse.dia_matrix((data, np.arange(-6, 7)), shape=(n, n))
+    lay = GridLayout.from_dwave(synth.camera_grids())
+    with pytest.raises(NotImplementedError):
+        TargetBatch(tg, lay)
+
+
+def test_spectrum_masks_low_resolution_rows():
+    # redrock targets.py:33-35: rows whose R integral < 0.99 get ivar 0
+    from redrock_b200.targets import Spectrum
+    import scipy.sparse
+    n = 20
+    d, o = synth.util_R(n)     # not normalised at the edges
+    ivar = np.ones(n)
+    s = Spectrum(np.arange(n, dtype=float), np.zeros(n), ivar,
+                 scipy.sparse.dia_matrix((d, o), shape=(n, n)))
+    assert s.ivar[0] == 0 and s.ivar[n // 2] == 1
+
+
+def test_distribute_work_matches_rule():
+    ids = list(range(10))
+    w = {i: (i % 3) + 1 for i in ids}
+    dist = distribute_work(3, ids, weights=w)
+    loads = [sum(w[i] for i in d) for d in dist]
+    assert sorted(sum(dist, [])) == ids
+    assert max(loads) - min(loads) <= 1
+    # capacities: a process with 3x capacity takes ~3x the load
+    dist = distribute_work(2, list(range(40)), capacities=[3, 1])
+    assert len(dist[0]) == 30 and len(dist[1]) == 10
+
+
+def test_dist_targets_copy_and_wavegrids():
+    tg = from_synth(synth.make_targets(3, seed=2))
+    d = DistTargetsCopy(tg)
+    assert sorted(d.local_target_ids()) == [t.id for t in tg]
+    assert set(d.wavegrids()) == {"b", "r", "z"}
+
+
+def test_installer_rebinds_every_import_site():
+    mods = {}
+    for sub, attr in PATCHES:
+        mods.setdefault(sub, types.SimpleNamespace())
+        setattr(mods[sub], attr, "original")
+    mods.setdefault("zfind", types.SimpleNamespace(calc_zchi2_targets="original"))
+    mods["zscan"].calc_zchi2_targets = "original"
+    done = install(modules=mods)
+    assert len(done) == len(PATCHES) + 2
+    for sub, attr in PATCHES:
+        assert callable(getattr(mods[sub], attr))
+    assert mods["fitz"].calc_zchi2_batch.__module__ == "redrock_b200.zscan"
+    assert mods["templates"].DistTemplate.__module__ == "redrock_b200.templates"
+
+
+def test_flop_model():
+    import bench
+    # SURVEY 8(d) figures at P = 7958
+    assert round(bench.flops_per_eval(10, 7958)) == 2785853
+    assert round(bench.flops_per_eval(4, 7958)) == 923189
+    assert round(bench.flops_per_eval(5, 7958)) == 1193802
