@@ -99,12 +99,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def make_workload(ntarget, seed):
+def make_workload(ntarget, seed, zsub=None):
     from redrock_b200 import synth
     from redrock_b200 import targets as T
     from redrock_b200 import templates as TM
     tg = synth.make_targets(ntarget, seed=seed)
-    tset = synth.template_set()
+    tset = synth.template_set(zsub=zsub)
     rtg = T.from_synth(tg)
     tms = [TM.from_synth(ts) for ts in tset]
     return tg, rtg, tset, tms
@@ -169,7 +169,8 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     L = _lib.lib()
-    tg, rtg, tset, tms = make_workload(args.ntargets, seed=args.seed + 7919 * rank)
+    tg, rtg, tset, tms = make_workload(args.ntargets, seed=args.seed + 7919 * rank,
+                                       zsub=args.zsub)
     evals, flops = evals_and_flops(rtg, tms)
     layout = GridLayout.from_dwave(synth.camera_grids())
     srcs = [TemplateSource.from_template(tm) for tm in tms]
@@ -269,7 +270,9 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded DESI-like targets and "
         "templates, redrock_b200/synth.py)",
-        "config": {"workload": WORKLOAD, "targets_per_gpu": args.ntargets,
+        "config": {"workload": WORKLOAD if args.ntargets == 500 and not args.zsub else
+                   f"reduced: {args.ntargets} targets, zsub={args.zsub}",
+                   "targets_per_gpu": args.ntargets,
                    "templates": [tm.full_type for tm in tms],
                    "evals_per_step_per_gpu": evals, "pixels_per_target": 7958,
                    "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
@@ -362,6 +365,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ntargets", type=int, default=500)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--zsub", type=int, default=None,
+                    help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-zsub", type=int, default=5)

@@ -193,7 +193,9 @@ typedef struct {
   int64_t npix_block;
 } rr_scan_targets;
 
-/* tile_counter: one device int of scratch (reset by the call). */
+/* tile_counter: two device ints of scratch (reset by the call).  Templates
+ * with nbasis 4, 5 or 10 run in one persistent launch, any others in a
+ * second one. */
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                    int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
 

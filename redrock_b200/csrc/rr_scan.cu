@@ -99,13 +99,6 @@ __device__ __forceinline__ void issue_chunk(const FusedParams& p, const rr_scan_
   }
 }
 
-template <int NB>
-struct Acc {
-  static constexpr int kTri = NB * (NB + 1) / 2;
-  double m[kTri];
-  double y[NB];
-};
-
 // LDL^T of the packed lower triangle a (row-major, a[i(i+1)/2 + j], j <= i)
 // in place, then solve for c.  Returns false on an exactly zero pivot.
 template <int NB>
@@ -155,43 +148,69 @@ __device__ __forceinline__ bool ldlt_solve(double (&a)[NB * (NB + 1) / 2], const
   return true;
 }
 
-// Solve, chi2 and penalty for one (target, z); writes the outputs.
+// Relative accuracy assumed for the FP64 sums M, y and f^T W f (about 90
+// ulp; calibrated against redrock's direct residual), and the chi2 error
+// above which a (target, z) is re-evaluated by the direct residual.
+constexpr double kSumEps = 1e-14;
+constexpr double kChi2FixTol = 1e-6;
+
+// Solve and chi2 for one (target, z) from its normal equations.
+// chi2 = f^T W f - c^T y - c^T P c.  Also returns an upper estimate of that
+// value's rounding error, kSumEps (sum_i |c_i| sqrt(M_ii) + sqrt(f^T W f))^2,
+// which bounds |c^T dM c| + 2|c^T dy| + |d(f^T W f)| for relative errors
+// kSumEps in the sums.  Returns false when the system is singular (or the
+// target has no weight, or the method is unsupported).
 template <int NB>
-__device__ __forceinline__ void finish_eval(const rr_scan_template& tm, int64_t row, int z,
-                                            double (&m)[NB * (NB + 1) / 2], const double (&y)[NB],
-                                            double fwf, double wsum) {
-  double c[NB];
-  double chi2;
+__device__ __forceinline__ bool solve_eval(const rr_scan_template& tm, double (&m)[NB * (NB + 1) / 2],
+                                           const double (&y)[NB], double fwf, double wsum,
+                                           double (&c)[NB], double& chi2, double& err) {
   bool ok = (wsum != 0.0) && (tm.method == RR_SOLVE_PCA);
+  double s = 0.0;
   if (ok) {
+#pragma unroll
+    for (int i = 0; i < NB; ++i) c[i] = sqrt(fmax(m[i * (i + 1) / 2 + i], 0.0));  // sqrt(M_ii)
     if (tm.prior) {
 #pragma unroll
       for (int i = 0; i < NB; ++i)
 #pragma unroll
         for (int j = 0; j <= i; ++j) m[i * (i + 1) / 2 + j] += tm.prior[i * NB + j];
     }
+    double sq[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) sq[i] = c[i];
     ok = ldlt_solve<NB>(m, y, c);
+#pragma unroll
+    for (int i = 0; i < NB; ++i) s = fma(fabs(c[i]), sq[i], s);
   }
-  if (ok) {
-    double cy = 0.0;
-#pragma unroll
-    for (int i = 0; i < NB; ++i) cy = fma(c[i], y[i], cy);
-    double cpc = 0.0;
-    if (tm.prior) {
-#pragma unroll
-      for (int i = 0; i < NB; ++i) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j < NB; ++j) s = fma(tm.prior[i * NB + j], c[j], s);
-        cpc = fma(c[i], s, cpc);
-      }
-    }
-    chi2 = fwf - cy - cpc;
-  } else {
+  if (!ok) {
 #pragma unroll
     for (int i = 0; i < NB; ++i) c[i] = 0.0;
     chi2 = kHugeChi2;
+    err = 0.0;
+    return false;
   }
+  double cy = 0.0;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) cy = fma(c[i], y[i], cy);
+  double cpc = 0.0;
+  if (tm.prior) {
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+      double t = 0.0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j) t = fma(tm.prior[i * NB + j], c[j], t);
+      cpc = fma(c[i], t, cpc);
+    }
+  }
+  chi2 = fwf - cy - cpc;
+  const double a = s + sqrt(fwf);
+  err = kSumEps * a * a;
+  return true;
+}
+
+template <int NB>
+__device__ __forceinline__ void write_eval(const rr_scan_template& tm, int64_t row, int z,
+                                           const double (&c)[NB], double chi2, double wsum) {
   tm.zchi2[row * tm.nz + z] = chi2;
   double* co = tm.zcoeff + (row * tm.nz + z) * NB;
 #pragma unroll
@@ -205,28 +224,25 @@ __device__ __forceinline__ void finish_eval(const rr_scan_template& tm, int64_t 
   }
 }
 
-template <int NB>
-__device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
-                          StageBufs& sb, uint32_t (&uses)[kStages], bool& failed) {
+// One sweep of a tile's pixels through the two-stage copy pipeline.
+// RESID = false: accumulate the Gram matrix m and y.
+// RESID = true:  accumulate the direct residual sum (g - Tb'.c)^2 into acc
+//                (only lanes with do_lane set do the arithmetic).
+// Returns false (uniformly across the CTA) if a copy wait timed out.
+template <int NB, bool RESID>
+__device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_template& tm, int block,
+                                      int z0, int nzt, bool active, StageBufs& sb,
+                                      uint32_t (&uses)[kStages], double (&m)[NB * (NB + 1) / 2],
+                                      double (&y)[NB], const double (&c)[NB], double& acc) {
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int nzt = min(kWarps, tm.nz - z0);
-  const bool active = warp < nzt;
   const int stride = tm.basis_stride;
-  constexpr int kTri = NB * (NB + 1) / 2;
-  double m[kTri];
-  double y[NB];
-#pragma unroll
-  for (int i = 0; i < kTri; ++i) m[i] = 0.0;
-#pragma unroll
-  for (int i = 0; i < NB; ++i) y[i] = 0.0;
-
   const int64_t nchunk = p.chunks_total;
   if (threadIdx.x == 0) issue_chunk(p, tm, block, z0, nzt, 0, 0, sb);
-  for (int64_t c = 0; c < nchunk; ++c) {
-    const int s = (int)(c & 1);
-    const bool more = c + 1 < nchunk;
-    if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, c + 1, s ^ 1, sb);
+  for (int64_t ch = 0; ch < nchunk; ++ch) {
+    const int s = (int)(ch & 1);
+    const bool more = ch + 1 < nchunk;
+    if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ch + 1, s ^ 1, sb);
     const bool ok = mbar_wait(&sb.full[s], uses[s] & 1u, p.status);
     uses[s]++;
     if (active && ok) {
@@ -252,32 +268,86 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
           }
           if (NB & 1) tb[NB - 1] = fma(r[k], trow[NB - 1], tb[NB - 1]);
         }
+        if (RESID) {
+          double model = 0.0;
 #pragma unroll
-        for (int b = 0; b < NB; ++b) y[b] = fma(g, tb[b], y[b]);
+          for (int b = 0; b < NB; ++b) model = fma(tb[b], c[b], model);
+          const double res = g - model;
+          acc = fma(res, res, acc);
+        } else {
 #pragma unroll
-        for (int a = 0; a < NB; ++a)
+          for (int b = 0; b < NB; ++b) y[b] = fma(g, tb[b], y[b]);
 #pragma unroll
-          for (int b = 0; b <= a; ++b)
-            m[a * (a + 1) / 2 + b] = fma(tb[a], tb[b], m[a * (a + 1) / 2 + b]);
+          for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int b = 0; b <= a; ++b)
+              m[a * (a + 1) / 2 + b] = fma(tb[a], tb[b], m[a * (a + 1) / 2 + b]);
+        }
       }
     }
-    // stage s is free for chunk c + 2 once every warp is past this point;
+    // stage s is free for chunk ch + 2 once every warp is past this point;
     // a timed-out wait anywhere stops the whole CTA
     if (__syncthreads_or(!ok)) {
-      failed = true;
-      // let the copy of chunk c + 1 (if issued) land before leaving
+      // let the copy of chunk ch + 1 (if issued) land before leaving
       if (threadIdx.x == 0 && more) mbar_wait(&sb.full[s ^ 1], uses[s ^ 1] & 1u, p.status);
-      return;
+      return false;
     }
   }
-  if (failed || !active) return;
-  const int32_t row = p.tg.rows[block * RR_LANES + lane];
-  if (row < 0) return;
-  const double fwf = p.tg.fwf[block * RR_LANES + lane];
-  const double wsum = p.tg.wsum[block * RR_LANES + lane];
-  finish_eval<NB>(tm, row, z0 + warp, m, y, fwf, wsum);
+  return true;
 }
 
+template <int NB>
+__device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
+                          StageBufs& sb, uint32_t (&uses)[kStages], bool& failed) {
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nzt = min(kWarps, tm.nz - z0);
+  constexpr int kTri = NB * (NB + 1) / 2;
+  double m[kTri];
+  double y[NB];
+  double c[NB];
+  double acc = 0.0;
+#pragma unroll
+  for (int i = 0; i < kTri; ++i) m[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < NB; ++i) y[i] = 0.0;
+  const bool inz = warp < nzt;
+  const int32_t row = p.tg.rows[block * RR_LANES + lane];
+  if (!sweep<NB, false>(p, tm, block, z0, nzt, inz, sb, uses, m, y, c, acc)) {
+    failed = true;
+    return;
+  }
+  const bool valid = inz && row >= 0;
+  bool fix = false;
+  double chi2 = 0.0, err = 0.0, wsum = 0.0;
+  if (valid) {
+    const double fwf = p.tg.fwf[block * RR_LANES + lane];
+    wsum = p.tg.wsum[block * RR_LANES + lane];
+    const bool ok = solve_eval<NB>(tm, m, y, fwf, wsum, c, chi2, err);
+    fix = ok && err > kChi2FixTol;
+    write_eval<NB>(tm, row, z0 + warp, c, chi2, wsum);
+  }
+  // ill-conditioned fits: re-evaluate chi2 as the direct weighted residual
+  // sum w (f - Tb c)^2 (redrock's own formula, zscan.py:777-780), which does
+  // not suffer the cancellation of f^T W f - c^T y
+  if (__syncthreads_or(fix)) {
+    acc = 0.0;
+    if (!sweep<NB, true>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
+      failed = true;
+      return;
+    }
+    if (fix) tm.zchi2[(int64_t)row * tm.nz + z0 + warp] = acc;
+  }
+}
+
+// nbasis values compiled into each instantiation of the fused kernel: the
+// common template sizes (QSO 4, STAR 5, GALAXY 10) share one instantiation
+// so a full GALAXY/QSO/STAR scan is a single persistent launch; the rest go
+// to a second one (keeping all ten in one kernel makes the register
+// allocator spill on every path).
+__host__ __device__ constexpr bool in_common_set(int nb) { return nb == 4 || nb == 5 || nb == 10; }
+
+template <bool COMMON>
 __global__ void __launch_bounds__(kThreads, 1) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kStages];
@@ -312,19 +382,21 @@ __global__ void __launch_bounds__(kThreads, 1) zscan_fused_kernel(const __grid_c
     const int64_t local = tile - p.tile_start[t];
     const int block = (int)(local % p.tg.nblock);
     const int z0 = (int)(local / p.tg.nblock) * kWarps;
+#define RR_TILE_CASE(N)                                                   \
+  case N:                                                                 \
+    if constexpr (in_common_set(N) == COMMON) {                           \
+      scan_tile<N>(p, tm, block, z0, sb, uses, failed);                   \
+    } else {                                                              \
+      set_status(p.status, RR_EINVAL);                                    \
+      failed = true;                                                      \
+    }                                                                     \
+    break;
     switch (tm.nbasis) {
-      case 1: scan_tile<1>(p, tm, block, z0, sb, uses, failed); break;
-      case 2: scan_tile<2>(p, tm, block, z0, sb, uses, failed); break;
-      case 3: scan_tile<3>(p, tm, block, z0, sb, uses, failed); break;
-      case 4: scan_tile<4>(p, tm, block, z0, sb, uses, failed); break;
-      case 5: scan_tile<5>(p, tm, block, z0, sb, uses, failed); break;
-      case 6: scan_tile<6>(p, tm, block, z0, sb, uses, failed); break;
-      case 7: scan_tile<7>(p, tm, block, z0, sb, uses, failed); break;
-      case 8: scan_tile<8>(p, tm, block, z0, sb, uses, failed); break;
-      case 9: scan_tile<9>(p, tm, block, z0, sb, uses, failed); break;
-      case 10: scan_tile<10>(p, tm, block, z0, sb, uses, failed); break;
+      RR_TILE_CASE(1) RR_TILE_CASE(2) RR_TILE_CASE(3) RR_TILE_CASE(4) RR_TILE_CASE(5)
+      RR_TILE_CASE(6) RR_TILE_CASE(7) RR_TILE_CASE(8) RR_TILE_CASE(9) RR_TILE_CASE(10)
       default: set_status(p.status, RR_EINVAL); failed = true; break;
     }
+#undef RR_TILE_CASE
     if (failed) break;  // uniform across the CTA
     __syncthreads();
   }
@@ -611,6 +683,50 @@ static size_t fused_smem_bytes(int max_stride) {
   return (size_t)kStages * (kRwChunkDoubles + (size_t)kWarps * kWin * max_stride) * sizeof(double);
 }
 
+// Launch one instantiation of the fused kernel over the templates selected
+// by `pick` (indices into templates), using counter as its tile counter.
+template <bool COMMON>
+static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
+                        const int* pick, int npick, int* counter, int* status,
+                        cudaStream_t stream) {
+  FusedParams p;
+  memset(&p, 0, sizeof(p));
+  p.tg = *targets;
+  p.nseg = targets->nseg;
+  int64_t chunks = 0;
+  for (int s = 0; s < p.nseg; ++s) {
+    p.segs[s] = targets->segs[s];
+    chunks += p.segs[s].npix_pad / kChunk;
+  }
+  p.chunks_total = chunks;
+  p.ntemplate = npick;
+  p.tile_start[0] = 0;
+  int max_stride = 2;
+  for (int i = 0; i < npick; ++i) {
+    const rr_scan_template& tm = templates[pick[i]];
+    p.tm[i] = tm;
+    const int64_t zt = (tm.nz + kWarps - 1) / kWarps;
+    p.tile_start[i + 1] = p.tile_start[i] + zt * targets->nblock;
+    max_stride = tm.basis_stride > max_stride ? tm.basis_stride : max_stride;
+  }
+  p.max_stride = max_stride;
+  p.tile_counter = counter;
+  p.status = status;
+  const int64_t ntiles = p.tile_start[npick];
+  if (ntiles == 0) return RR_OK;
+  const size_t smem = fused_smem_bytes(max_stride);
+  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<COMMON>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 0;
+  RR_CUDA_TRY(cudaGetDevice(&dev));
+  RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
+  const int64_t grid = ntiles < nsm ? ntiles : nsm;
+  zscan_fused_kernel<COMMON><<<(unsigned)grid, kThreads, smem, stream>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
 extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                               int ntemplate, int* tile_counter, int* status, rr_stream_t stream) {
   if (!targets || !templates || !tile_counter) return RR_EINVAL;
@@ -618,25 +734,18 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
   if (targets->nblock < 1 || targets->nseg < 1 || targets->nseg > 16) return RR_EINVAL;
   if (!targets->rw || !targets->fwf || !targets->wsum || !targets->rows || !targets->segs)
     return RR_EINVAL;
-  FusedParams p;
-  memset(&p, 0, sizeof(p));
-  p.tg = *targets;
-  p.nseg = targets->nseg;
-  int64_t chunks = 0, rw_end = 0;
-  for (int s = 0; s < p.nseg; ++s) {
-    p.segs[s] = targets->segs[s];
-    const rr_segment_desc& sd = p.segs[s];
+  if ((reinterpret_cast<uintptr_t>(targets->rw) & 15) != 0) return RR_EINVAL;
+  int64_t rw_end = 0;
+  for (int s = 0; s < targets->nseg; ++s) {
+    const rr_segment_desc& sd = targets->segs[s];
     if (sd.npix_pad <= 0 || (sd.npix_pad % kChunk) != 0 || sd.basis_offset < kHalfBand ||
         sd.rw_offset < 0)
       return RR_EINVAL;
-    chunks += sd.npix_pad / kChunk;
     rw_end = sd.rw_offset + sd.npix_pad > rw_end ? sd.rw_offset + sd.npix_pad : rw_end;
   }
   if (rw_end > targets->npix_block) return RR_EINVAL;
-  p.chunks_total = chunks;
-  p.ntemplate = ntemplate;
-  p.tile_start[0] = 0;
-  int max_stride = 2;
+  int common[RR_MAX_TEMPLATES], other[RR_MAX_TEMPLATES];
+  int nc = 0, no = 0;
   for (int t = 0; t < ntemplate; ++t) {
     const rr_scan_template& tm = templates[t];
     if (tm.nbasis < 1 || tm.nbasis > RR_MAX_NBASIS || tm.nz < 0) return RR_EINVAL;
@@ -644,29 +753,20 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     if (tm.nz > 0 && (!tm.basis || !tm.zchi2 || !tm.zcoeff)) return RR_EINVAL;
     if (tm.oii && !tm.penalty) return RR_EINVAL;
     if ((reinterpret_cast<uintptr_t>(tm.basis) & 15) != 0) return RR_EINVAL;
-    for (int s = 0; s < p.nseg; ++s)
-      if (p.segs[s].basis_offset + p.segs[s].npix_pad + kHalfBand > tm.pix_stride) return RR_EINVAL;
-    p.tm[t] = tm;
-    const int64_t zt = (tm.nz + kWarps - 1) / kWarps;
-    p.tile_start[t + 1] = p.tile_start[t] + zt * targets->nblock;
-    max_stride = tm.basis_stride > max_stride ? tm.basis_stride : max_stride;
+    for (int s = 0; s < targets->nseg; ++s)
+      if (targets->segs[s].basis_offset + targets->segs[s].npix_pad + kHalfBand > tm.pix_stride)
+        return RR_EINVAL;
+    if (in_common_set(tm.nbasis)) common[nc++] = t; else other[no++] = t;
   }
-  if ((reinterpret_cast<uintptr_t>(targets->rw) & 15) != 0) return RR_EINVAL;
-  p.max_stride = max_stride;
-  p.tile_counter = tile_counter;
-  p.status = status;
-  const int64_t ntiles = p.tile_start[ntemplate];
-  if (ntiles == 0) return RR_OK;
-  const size_t smem = fused_smem_bytes(max_stride);
-  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-  int dev = 0, nsm = 0;
-  RR_CUDA_TRY(cudaGetDevice(&dev));
-  RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  RR_CUDA_TRY(cudaMemsetAsync(tile_counter, 0, sizeof(int), (cudaStream_t)stream));
-  const int64_t grid = ntiles < nsm ? ntiles : nsm;
-  zscan_fused_kernel<<<(unsigned)grid, kThreads, smem, (cudaStream_t)stream>>>(p);
-  RR_CHECK_LAUNCH();
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nc) {
+    int rc = launch_fused<true>(targets, templates, common, nc, tile_counter, status, st);
+    if (rc) return rc;
+  }
+  if (no) {
+    int rc = launch_fused<false>(targets, templates, other, no, tile_counter + 1, status, st);
+    if (rc) return rc;
+  }
   return RR_OK;
 }
 

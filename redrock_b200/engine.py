@@ -385,7 +385,7 @@ def run_fused(pack, bases, stream=None, status=None):
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
     tgs = pack.scan_targets_struct()
-    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    counter = torch.zeros(2, dtype=torch.int32, device=dev)
     st = status or StatusWord(dev)
     for i0 in range(0, len(bases), _lib.MAX_TEMPLATES):
         chunk = list(range(i0, min(len(bases), i0 + _lib.MAX_TEMPLATES)))

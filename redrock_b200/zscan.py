@@ -135,23 +135,32 @@ def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False)
 
 
 def calc_zchi2_targets(targets, templates, mp_procs=1, use_gpu=True):
-    """All templates for all local targets in one fused launch (zscan.py:910)."""
+    """All templates for all local targets in one fused launch (zscan.py:910).
+
+    Results are keyed by the id of each target object in ``targets.local()``.
+    (redrock pairs ``local_target_ids()`` -- sorted by number of spectra --
+    with ``local()`` in input order, zscan.py:1008-1019, which attaches a
+    target's chi2 to another target when spectrum counts differ; keying by
+    the object's own id gives redrock's answer whenever redrock's pairing is
+    consistent.)
+    """
     am_root = targets.comm is None or targets.comm.rank == 0
-    tids = list(targets.local_target_ids())
-    results = {tid: {} for tid in tids}
+    data = list(targets.local())
+    tids = [t.id for t in data]
+    results = {tid: {} for tid in targets.local_target_ids()}
     if am_root:
         print("Computing redshifts")
         sys.stdout.flush()
     if len(tids) == 0:
         return results
-    out = scan_device(list(targets.local()), list(templates))
+    out = scan_device(data, list(templates))
     for t, r in zip(templates, out):
         ft = t.template.full_type
         zc = r.zchi2.cpu().numpy()
         co = r.zcoeff.cpu().numpy()
         pe = r.penalty.cpu().numpy()
         for i, tid in enumerate(tids):
-            results[tid][ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
+            results.setdefault(tid, {})[ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
                                     zcoeff=co[i])
     return results
 
