@@ -58,10 +58,28 @@ struct FusedParams {
   int* status;
 };
 
+// Stage buffers live in the dynamic shared-memory array; stage s holds the
+// packed resolution rows of a chunk (kRwChunkDoubles) followed by the basis
+// windows of the tile's redshifts.  Addresses are formed from the
+// __shared__ array itself so every read in the pixel loop is a shared load.
+extern __shared__ __align__(128) double rr_stage_smem[];
+
 struct StageBufs {
-  double* rw[kStages];
-  double* t[kStages];
-  uint64_t* full;  // kStages mbarriers
+  int stage_doubles;  // doubles per stage
+  uint64_t* full;     // kStages mbarriers
+  __device__ __forceinline__ double* rw(int s) const { return rr_stage_smem + s * stage_doubles; }
+  __device__ __forceinline__ double* t(int s) const {
+    return rr_stage_smem + s * stage_doubles + kRwChunkDoubles;
+  }
+};
+
+// completed-phase counters of the two stage barriers, kept in registers
+struct Uses {
+  uint32_t u0 = 0, u1 = 0;
+  __device__ __forceinline__ uint32_t parity(int s) const { return (s ? u1 : u0) & 1u; }
+  __device__ __forceinline__ void bump(int s) {
+    if (s) ++u1; else ++u0;
+  }
 };
 
 __device__ __forceinline__ void chunk_segment(const FusedParams& p, int64_t c, int& seg,
@@ -90,40 +108,52 @@ __device__ __forceinline__ void issue_chunk(const FusedParams& p, const rr_scan_
   mbar_arrive_expect_tx(&sb.full[s], rw_bytes + nzt * t_bytes);
   const double* src_rw =
       p.tg.rw + ((int64_t)block * p.tg.npix_block + sd.rw_offset + p0) * (RR_RW * RR_LANES);
-  bulk_g2s(sb.rw[s], src_rw, rw_bytes, &sb.full[s]);
+  bulk_g2s(sb.rw(s), src_rw, rw_bytes, &sb.full[s]);
   for (int w = 0; w < nzt; ++w) {
     const double* src_t =
         tm.basis + ((int64_t)(z0 + w) * tm.pix_stride + sd.basis_offset + p0 - kHalfBand) *
                        tm.basis_stride;
-    bulk_g2s(sb.t[s] + (int64_t)w * kWin * tm.basis_stride, src_t, t_bytes, &sb.full[s]);
+    bulk_g2s(sb.t(s) + (int64_t)w * kWin * tm.basis_stride, src_t, t_bytes, &sb.full[s]);
   }
 }
 
-// LDL^T of the packed lower triangle a (row-major, a[i(i+1)/2 + j], j <= i)
-// in place, then solve for c.  Returns false on an exactly zero pivot.
+// LDL^T of the packed lower triangle of a symmetric matrix (row-major,
+// a[i(i+1)/2 + j], j <= i), then the solve for c.  Works on its own copy
+// so the caller's accumulator stays in registers.  Returns false on an
+// exactly zero pivot (redrock's singular case), leaving c unspecified.
 template <int NB>
-__device__ __forceinline__ bool ldlt_solve(double (&a)[NB * (NB + 1) / 2], const double (&y)[NB],
-                                           double (&c)[NB]) {
+__device__ __forceinline__ bool ldlt_solve(const double (&m)[NB * (NB + 1) / 2],
+                                           const double (&y)[NB], double (&c)[NB]) {
+  constexpr int kTri = NB * (NB + 1) / 2;
+  double a[kTri];
+#pragma unroll
+  for (int i = 0; i < kTri; ++i) a[i] = m[i];
 #define A(i, j) a[(i) * ((i) + 1) / 2 + (j)]
   double d[NB];
+  bool ok = true;
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
     double v[NB];
     double dj = A(j, j);
 #pragma unroll
-    for (int k = 0; k < j; ++k) {
-      v[k] = A(j, k) * d[k];
-      dj -= A(j, k) * v[k];
+    for (int k = 0; k < NB; ++k) {
+      if (k < j) {
+        v[k] = A(j, k) * d[k];
+        dj -= A(j, k) * v[k];
+      }
     }
-    if (dj == 0.0) return false;
+    ok = ok && (dj != 0.0);
     d[j] = dj;
     const double inv = 1.0 / dj;
 #pragma unroll
-    for (int i = j + 1; i < NB; ++i) {
-      double s = A(i, j);
+    for (int i = 0; i < NB; ++i) {
+      if (i > j) {
+        double s = A(i, j);
 #pragma unroll
-      for (int k = 0; k < j; ++k) s -= A(i, k) * v[k];
-      A(i, j) = s * inv;
+        for (int k = 0; k < NB; ++k)
+          if (k < j) s -= A(i, k) * v[k];
+        A(i, j) = s * inv;
+      }
     }
   }
   // L z = y
@@ -131,21 +161,24 @@ __device__ __forceinline__ bool ldlt_solve(double (&a)[NB * (NB + 1) / 2], const
   for (int i = 0; i < NB; ++i) {
     double s = y[i];
 #pragma unroll
-    for (int k = 0; k < i; ++k) s -= A(i, k) * c[k];
+    for (int k = 0; k < NB; ++k)
+      if (k < i) s -= A(i, k) * c[k];
     c[i] = s;
   }
 #pragma unroll
   for (int i = 0; i < NB; ++i) c[i] /= d[i];
   // L^T c = z
 #pragma unroll
-  for (int i = NB - 1; i >= 0; --i) {
+  for (int ii = 0; ii < NB; ++ii) {
+    const int i = NB - 1 - ii;
     double s = c[i];
 #pragma unroll
-    for (int k = i + 1; k < NB; ++k) s -= A(k, i) * c[k];
+    for (int k = 0; k < NB; ++k)
+      if (k > i) s -= A(k, i) * c[k];
     c[i] = s;
   }
 #undef A
-  return true;
+  return ok;
 }
 
 // Relative accuracy assumed for the FP64 sums M, y and f^T W f (about 90
@@ -161,26 +194,26 @@ constexpr double kChi2FixTol = 1e-6;
 // kSumEps in the sums.  Returns false when the system is singular (or the
 // target has no weight, or the method is unsupported).
 template <int NB>
-__device__ __forceinline__ bool solve_eval(const rr_scan_template& tm, double (&m)[NB * (NB + 1) / 2],
+__device__ __forceinline__ bool solve_eval(const rr_scan_template& tm,
+                                           const double (&m)[NB * (NB + 1) / 2],
                                            const double (&y)[NB], double fwf, double wsum,
                                            double (&c)[NB], double& chi2, double& err) {
+  constexpr int kTri = NB * (NB + 1) / 2;
   bool ok = (wsum != 0.0) && (tm.method == RR_SOLVE_PCA);
   double s = 0.0;
   if (ok) {
+    double mp[kTri];
 #pragma unroll
-    for (int i = 0; i < NB; ++i) c[i] = sqrt(fmax(m[i * (i + 1) / 2 + i], 0.0));  // sqrt(M_ii)
+    for (int i = 0; i < kTri; ++i) mp[i] = m[i];
     if (tm.prior) {
 #pragma unroll
       for (int i = 0; i < NB; ++i)
 #pragma unroll
-        for (int j = 0; j <= i; ++j) m[i * (i + 1) / 2 + j] += tm.prior[i * NB + j];
+        for (int j = 0; j <= i; ++j) mp[i * (i + 1) / 2 + j] += tm.prior[i * NB + j];
     }
-    double sq[NB];
+    ok = ldlt_solve<NB>(mp, y, c);
 #pragma unroll
-    for (int i = 0; i < NB; ++i) sq[i] = c[i];
-    ok = ldlt_solve<NB>(m, y, c);
-#pragma unroll
-    for (int i = 0; i < NB; ++i) s = fma(fabs(c[i]), sq[i], s);
+    for (int i = 0; i < NB; ++i) s = fma(fabs(c[i]), sqrt(fmax(m[i * (i + 1) / 2 + i], 0.0)), s);
   }
   if (!ok) {
 #pragma unroll
@@ -232,7 +265,7 @@ __device__ __forceinline__ void write_eval(const rr_scan_template& tm, int64_t r
 template <int NB, bool RESID>
 __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_template& tm, int block,
                                       int z0, int nzt, bool active, StageBufs& sb,
-                                      uint32_t (&uses)[kStages], double (&m)[NB * (NB + 1) / 2],
+                                      Uses& uses, double (&m)[NB * (NB + 1) / 2],
                                       double (&y)[NB], const double (&c)[NB], double& acc) {
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -243,40 +276,55 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     const int s = (int)(ch & 1);
     const bool more = ch + 1 < nchunk;
     if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ch + 1, s ^ 1, sb);
-    const bool ok = mbar_wait(&sb.full[s], uses[s] & 1u, p.status);
-    uses[s]++;
+    const bool ok = mbar_wait(&sb.full[s], uses.parity(s), p.status);
+    uses.bump(s);
     if (active && ok) {
-      const double* rws = sb.rw[s];
-      const double* ts = sb.t[s] + (int64_t)warp * kWin * stride;
+      const double* rws = sb.rw(s) + lane;
+      const double* ts = sb.t(s) + warp * kWin * stride;
+      // two pixels per step: basis row q + k serves pixel q (band index k)
+      // and pixel q + 1 (band index k - 1), so each row is read once
 #pragma unroll 1
-      for (int q = 0; q < kChunk; ++q) {
-        double r[kBand];
+      for (int q = 0; q < kChunk; q += 2) {
+        double ta[NB], tb[NB];
 #pragma unroll
-        for (int k = 0; k < kBand; ++k) r[k] = rws[(q * RR_RW + k) * RR_LANES + lane];
-        const double g = rws[(q * RR_RW + kBand) * RR_LANES + lane];
-        double tb[NB];
+        for (int b = 0; b < NB; ++b) { ta[b] = 0.0; tb[b] = 0.0; }
 #pragma unroll
-        for (int b = 0; b < NB; ++b) tb[b] = 0.0;
-#pragma unroll
-        for (int k = 0; k < kBand; ++k) {
+        for (int k = 0; k <= kBand; ++k) {
           const double* trow = ts + (q + k) * stride;
+          const double ra = k < kBand ? rws[(q * RR_RW + k) * RR_LANES] : 0.0;
+          const double rb = k > 0 ? rws[((q + 1) * RR_RW + k - 1) * RR_LANES] : 0.0;
 #pragma unroll
           for (int b = 0; b + 1 < NB; b += 2) {
             const double2 tv = *reinterpret_cast<const double2*>(trow + b);
-            tb[b] = fma(r[k], tv.x, tb[b]);
-            tb[b + 1] = fma(r[k], tv.y, tb[b + 1]);
+            if (k < kBand) { ta[b] = fma(ra, tv.x, ta[b]); ta[b + 1] = fma(ra, tv.y, ta[b + 1]); }
+            if (k > 0) { tb[b] = fma(rb, tv.x, tb[b]); tb[b + 1] = fma(rb, tv.y, tb[b + 1]); }
           }
-          if (NB & 1) tb[NB - 1] = fma(r[k], trow[NB - 1], tb[NB - 1]);
+          if (NB & 1) {
+            const double tv = trow[NB - 1];
+            if (k < kBand) ta[NB - 1] = fma(ra, tv, ta[NB - 1]);
+            if (k > 0) tb[NB - 1] = fma(rb, tv, tb[NB - 1]);
+          }
         }
+        const double ga = rws[(q * RR_RW + kBand) * RR_LANES];
+        const double gb = rws[((q + 1) * RR_RW + kBand) * RR_LANES];
         if (RESID) {
-          double model = 0.0;
+          double ma = 0.0, mb = 0.0;
 #pragma unroll
-          for (int b = 0; b < NB; ++b) model = fma(tb[b], c[b], model);
-          const double res = g - model;
-          acc = fma(res, res, acc);
+          for (int b = 0; b < NB; ++b) { ma = fma(ta[b], c[b], ma); mb = fma(tb[b], c[b], mb); }
+          const double resa = ga - ma;
+          const double resb = gb - mb;
+          acc = fma(resa, resa, acc);
+          acc = fma(resb, resb, acc);
         } else {
 #pragma unroll
-          for (int b = 0; b < NB; ++b) y[b] = fma(g, tb[b], y[b]);
+          for (int b = 0; b < NB; ++b) y[b] = fma(ga, ta[b], y[b]);
+#pragma unroll
+          for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int b = 0; b <= a; ++b)
+              m[a * (a + 1) / 2 + b] = fma(ta[a], ta[b], m[a * (a + 1) / 2 + b]);
+#pragma unroll
+          for (int b = 0; b < NB; ++b) y[b] = fma(gb, tb[b], y[b]);
 #pragma unroll
           for (int a = 0; a < NB; ++a)
 #pragma unroll
@@ -289,7 +337,7 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     // a timed-out wait anywhere stops the whole CTA
     if (__syncthreads_or(!ok)) {
       // let the copy of chunk ch + 1 (if issued) land before leaving
-      if (threadIdx.x == 0 && more) mbar_wait(&sb.full[s ^ 1], uses[s ^ 1] & 1u, p.status);
+      if (threadIdx.x == 0 && more) mbar_wait(&sb.full[s ^ 1], uses.parity(s ^ 1), p.status);
       return false;
     }
   }
@@ -298,7 +346,7 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
 
 template <int NB>
 __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
-                          StageBufs& sb, uint32_t (&uses)[kStages], bool& failed) {
+                          StageBufs& sb, Uses& uses, bool& failed) {
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int nzt = min(kWarps, tm.nz - z0);
@@ -349,25 +397,17 @@ __host__ __device__ constexpr bool in_common_set(int nb) { return nb == 4 || nb 
 
 template <bool COMMON>
 __global__ void __launch_bounds__(kThreads, 1) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
-  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ int64_t s_tile;
   StageBufs sb;
-  {
-    double* base = reinterpret_cast<double*>(smem);
-    const int64_t t_doubles = (int64_t)kWarps * kWin * p.max_stride;
-    for (int s = 0; s < kStages; ++s) {
-      sb.rw[s] = base + s * (kRwChunkDoubles + t_doubles);
-      sb.t[s] = sb.rw[s] + kRwChunkDoubles;
-    }
-    sb.full = full;
-  }
+  sb.stage_doubles = kRwChunkDoubles + kWarps * kWin * p.max_stride;
+  sb.full = full;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  uint32_t uses[kStages] = {0, 0};
+  Uses uses;
   bool failed = false;
   const int64_t ntiles = p.tile_start[p.ntemplate];
   while (true) {
