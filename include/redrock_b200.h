@@ -50,7 +50,9 @@ enum rr_status {
                       (redrock raises ValueError, rebin.py:340-341) */
   RR_ECUDA = 3,    /* a CUDA runtime call failed; see rr_last_cuda_error */
   RR_ETIMEOUT = 4, /* a bounded device-side wait gave up */
-  RR_ENOTSUP = 5   /* valid input this build does not handle */
+  RR_ENOTSUP = 5,  /* valid input this build does not handle */
+  RR_ESCRATCH = 6  /* request larger than rr_zchi2_batch_plain_noalloc's
+                      fixed scratch (RR_NOALLOC_SCRATCH_BYTES) */
 };
 
 enum rr_igm_model { /* igm.py:367 igm_models */
@@ -218,6 +220,29 @@ int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflu
                          int32_t basis_stride, const double* prior, int32_t method,
                          double* zchi2, double* zcoeff, void* workspace, size_t workspace_bytes,
                          int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * rr_zchi2_batch_plain without a caller-provided workspace.  No counterpart
+ * in redrock.  For callers that cannot allocate device memory themselves --
+ * programs whose own memory manager already owns the GPU's memory, or
+ * latency-bound loops in which cudaMalloc / cudaFree could synchronise the
+ * device -- it works in a fixed scratch array compiled into the library
+ * (every GPU that loads the library holds RR_NOALLOC_SCRATCH_BYTES until
+ * exit) and allocates nothing.  Requests with
+ * rr_zchi2_batch_plain_workspace_bytes(npix_total, nz, nbasis) >
+ * RR_NOALLOC_SCRATCH_BYTES return RR_ESCRATCH.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * The first call on a device looks up the array's address; make it before
+ * any stream capture.
+ * ---------------------------------------------------------------------- */
+#define RR_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+int rr_zchi2_batch_plain_noalloc(const double* band, const double* w, const double* wflux,
+                                 const double* flux, const int64_t* pix_basis,
+                                 int64_t npix_total, const double* basis, int64_t pix_stride,
+                                 int32_t nz, int32_t nbasis, int32_t basis_stride,
+                                 const double* prior, int32_t method, double* zchi2,
+                                 double* zcoeff, int* status, rr_stream_t stream);
 
 /* penalty[z] = max(0, -sum_b coeff[z][b] oii[b])  (zscan.py:783-800) */
 int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const double* oii,

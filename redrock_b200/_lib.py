@@ -13,7 +13,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "librr_b200.so")
 
-RR_OK, RR_EINVAL, RR_ERANGE, RR_ECUDA, RR_ETIMEOUT, RR_ENOTSUP = range(6)
+RR_OK, RR_EINVAL, RR_ERANGE, RR_ECUDA, RR_ETIMEOUT, RR_ENOTSUP, RR_ESCRATCH = range(7)
 RR_IGM_NONE, RR_IGM_CALURA12, RR_IGM_KAMBLE20, RR_IGM_INOUE14 = range(4)
 RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED = 0, 1
 HALF_BAND = 5
@@ -95,6 +95,10 @@ _SIGNATURES = {
                                      c_void_p, c_int64, c_int32, c_int32, c_int32, c_void_p,
                                      c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
                                      c_void_p]),
+    "rr_zchi2_batch_plain_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                             c_int64, c_void_p, c_int64, c_int32, c_int32,
+                                             c_int32, c_void_p, c_int32, c_void_p, c_void_p,
+                                             c_void_p, c_void_p]),
     "rr_negoii_penalty": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
     "rr_fma_peak": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p]),
 }
@@ -127,7 +131,9 @@ def status_string(code):
     except Exception:
         return {0: "ok", 1: "invalid argument", 2: "edges must be within input x range",
                 3: "CUDA runtime error", 4: "bounded device wait timed out",
-                5: "unsupported input"}.get(code, "unknown")
+                5: "unsupported input",
+                6: "request exceeds the fixed scratch of the no-allocation entry point"
+                }.get(code, "unknown")
 
 
 def check(code, what):

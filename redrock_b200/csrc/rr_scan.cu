@@ -33,6 +33,7 @@
 // penalty.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "rr_common.cuh"
 
@@ -702,6 +703,8 @@ extern "C" const char* rr_status_string(int status) {
     case RR_ECUDA: return "CUDA runtime error";
     case RR_ETIMEOUT: return "bounded device wait timed out";
     case RR_ENOTSUP: return "unsupported input";
+    case RR_ESCRATCH:
+      return "request exceeds the fixed scratch of the no-allocation entry point";
     default: return "unknown status";
   }
 }
@@ -921,6 +924,74 @@ extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const d
     default: return RR_EINVAL;
   }
 #undef RR_PLAIN_CASE
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation variant of the plain per-target chain.
+//
+// For callers that cannot allocate device memory themselves: programs whose
+// own memory manager already owns the GPU's memory (a raw cudaMalloc there
+// may fail or fragment it), or latency-bound loops in which a cudaMalloc /
+// cudaFree could synchronise the device.  Its scratch is the file-scope
+// array below, created when the library is loaded and kept on every GPU
+// that loads the library until the process exits.
+//
+// * Maximum request: rr_zchi2_batch_plain_workspace_bytes(npix, nz, nbasis)
+//   <= RR_NOALLOC_SCRATCH_BYTES (16 MiB; e.g. 15 redshifts x 8000 pixels x
+//   10 bases); larger requests return RR_ESCRATCH before any launch.
+// * All calls share the one array.  It keeps the previous call's contents;
+//   every byte a call reads is written earlier in the same call, so nothing
+//   needs clearing.  Calls that overlap on the GPU (different streams or
+//   host threads, same device) race on it and must be serialised by the
+//   caller.
+// * The first call on each device looks up the array's device address
+//   (cudaGetSymbolAddress) with that device current and caches it; make
+//   that first call before any stream capture.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char rr_noalloc_scratch[RR_NOALLOC_SCRATCH_BYTES];
+
+static void* noalloc_scratch_ptr(int dev, int* rc) {
+  constexpr int kMaxDev = 64;
+  static std::mutex mu;
+  static void* ptrs[kMaxDev] = {nullptr};
+  *rc = RR_OK;
+  if (dev < 0 || dev >= kMaxDev) {
+    *rc = RR_EINVAL;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, rr_noalloc_scratch);
+    if (e != cudaSuccess) {
+      g_last_cuda_error = (int)e;
+      *rc = RR_ECUDA;
+      return nullptr;
+    }
+    ptrs[dev] = p;
+  }
+  return ptrs[dev];
+}
+
+extern "C" int rr_zchi2_batch_plain_noalloc(const double* band, const double* w,
+                                            const double* wflux, const double* flux,
+                                            const int64_t* pix_basis, int64_t npix_total,
+                                            const double* basis, int64_t pix_stride, int32_t nz,
+                                            int32_t nbasis, int32_t basis_stride,
+                                            const double* prior, int32_t method, double* zchi2,
+                                            double* zcoeff, int* status, rr_stream_t stream) {
+  if (nz < 0 || npix_total < 1 || nbasis < 1 || nbasis > RR_MAX_NBASIS) return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  const size_t need = rr_zchi2_batch_plain_workspace_bytes(npix_total, nz, nbasis);
+  if (need > (size_t)RR_NOALLOC_SCRATCH_BYTES) return RR_ESCRATCH;
+  int dev = 0;
+  RR_CUDA_TRY(cudaGetDevice(&dev));
+  int rc = RR_OK;
+  void* ws = noalloc_scratch_ptr(dev, &rc);
+  if (rc) return rc;
+  return rr_zchi2_batch_plain(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz,
+                              nbasis, basis_stride, prior, method, zchi2, zcoeff, ws,
+                              (size_t)RR_NOALLOC_SCRATCH_BYTES, status, stream);
 }
 
 extern "C" int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const double* oii,
