@@ -259,6 +259,29 @@ def run_ours(args, rank, world, local_rank):
                "path": "redrock_b200.zscan.calc_zchi2_targets(DistTargetsCopy, [DistTemplate x7])"
                        " from host numpy arrays"}
 
+    # ---- plain per-target chain on a sample (the "plain" of fused vs plain)
+    plain = None
+    if not args.no_plain and rank == 0:
+        sample = rtg[:args.plain_targets]
+        dtg = T.DistTargetsCopy(sample)
+        dts = [TM.DistTemplate(tm, dtg.wavegrids()) for tm in tms]
+        ids = [t.id for t in sample]
+        zscan.calc_zchi2_plain(ids[:1], sample[:1], dts[0])    # warm-up
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for dt in dts:
+            zscan.calc_zchi2_plain(ids, sample, dt)
+        b.record()
+        torch.cuda.synchronize()
+        pev = len(sample) * sum(len(tm.redshifts) for tm in tms)
+        pv = pev / (a.elapsed_time(b) / 1e3)
+        plain = {"value": pv, "unit": "chi2 evals/s", "targets": len(sample),
+                 "fused_over_plain": (evals / (ms / 1e3)) / pv,
+                 "path": "redrock_b200.zscan.calc_zchi2_plain: per target and template, "
+                         "R.T -> Gram/y -> solve -> residual chi2 launches + host read-back"}
+
     if rank != 0:
         return None
     peak = measure_fp64_peak(L, torch)
@@ -283,6 +306,7 @@ def run_ours(args, rank, world, local_rank):
                      "kernel_ms": fused_ms, "flops_per_launch": fused_flops,
                      "peak_source": "measured FP64 FMA peak (rr_fma_peak) on this GPU"},
         "e2e": e2e,
+        "plain": plain,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
@@ -369,6 +393,8 @@ def main():
                     help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--plain-targets", type=int, default=8)
     ap.add_argument("--ref-zsub", type=int, default=5)
     ap.add_argument("--ref-targets", type=int, default=4)
     args = ap.parse_args()
