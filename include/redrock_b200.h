@@ -29,6 +29,9 @@
  *                           target (and zscan.py:213-243 calc_zchi2_one as
  *                           nz = 1)
  *   rr_negoii_penalty       zscan.py:783-800 calc_negOII_penalty
+ *   rr_pack_rows,
+ *   rr_zscan_pairs          fitz.py:133-395 fine-grid refinement (every
+ *                           target's own redshifts, batched)
  */
 #ifndef REDROCK_B200_H
 #define REDROCK_B200_H
@@ -200,6 +203,52 @@ typedef struct {
  * second one. */
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                    int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Pair scan: chi2, coefficients and penalty for an arbitrary list of
+ * (target, redshift) pairs, the template rebinned (+ IGM) on the fly for
+ * each pair -- the batched form of fitz's fine-grid refinement
+ * (fitz.py:133-395: rebin_template + transmission_Lyman + calc_zchi2_batch
+ * on a 15-point grid per minimum, then a single-z fit).  Targets are packed
+ * target-major by rr_pack_rows:
+ *   rows[ntarget][npix_row][12] (sqrt(w) R band rows, sqrt(w) f), segment s
+ *   of a target at rows[t][segs[s].rw_offset ...]; fwf[t], wsum[t].
+ * Pairs whose redshift puts a bin edge outside the template range set
+ * RR_ERANGE in status and get NaN outputs (check them on the host first:
+ * edge_min >= x_first (1+z) and edge_max <= x_last (1+z)).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  const double* x;      /* device, template rest wavelengths [nx] */
+  int64_t nx;
+  const double* y;      /* device, [nbasis][nx] */
+  int32_t nbasis;
+  int32_t igm_model;    /* rr_igm_model */
+  int32_t method;       /* rr_solve_method */
+  int32_t pad_;
+  const double* prior;  /* device nbasis*nbasis or NULL */
+  const double* oii;    /* device nbasis [OII] window sums or NULL */
+} rr_pair_template;
+
+typedef struct {
+  const double* edges;  /* device, npix + 1 bin edges of this segment's grid */
+  const double* wave;   /* device, npix pixel centres */
+  int64_t npix;
+  int64_t row_offset;   /* pixel offset of the segment in a target's rows */
+  double wave_min;      /* host copy of min(wave) */
+} rr_pair_segment;
+
+int rr_pack_rows(const rr_spectrum_desc* specs /* device */, int64_t nspec,
+                 const int64_t* target_first /* device, ntarget + 1 */, int64_t ntarget,
+                 const double* rdata, const int32_t* roffsets, const double* ivar,
+                 const double* flux, const rr_segment_desc* segs /* device */, int nseg,
+                 int64_t npix_row, double* rows, double* fwf, double* wsum, int* status,
+                 rr_stream_t stream);
+
+int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segment* segs /* host, <= 16 */,
+                   int nseg, const double* rows, const double* fwf, const double* wsum,
+                   int64_t npix_row, const int32_t* pair_target, const double* pair_z,
+                   int64_t npairs, double* chi2, double* coeff /* [npairs][nbasis] */,
+                   double* penalty /* [npairs] or NULL */, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Plain per-target path (the structure of redrock's own GPU branch: R.T for

@@ -63,6 +63,17 @@ class ScanTargets(ctypes.Structure):
                 ("npix_block", c_int64)]
 
 
+class PairTemplate(ctypes.Structure):
+    _fields_ = [("x", c_void_p), ("nx", c_int64), ("y", c_void_p), ("nbasis", c_int32),
+                ("igm_model", c_int32), ("method", c_int32), ("pad_", c_int32),
+                ("prior", c_void_p), ("oii", c_void_p)]
+
+
+class PairSegment(ctypes.Structure):
+    _fields_ = [("edges", c_void_p), ("wave", c_void_p), ("npix", c_int64),
+                ("row_offset", c_int64), ("wave_min", c_double)]
+
+
 class RRError(RuntimeError):
     def __init__(self, code, what):
         self.code = code
@@ -88,6 +99,12 @@ _SIGNATURES = {
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_zscan_fused": (c_int, [ctypes.POINTER(ScanTargets), ctypes.POINTER(ScanTemplate), c_int,
                                c_void_p, c_void_p, c_void_p]),
+    "rr_pack_rows": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                             c_void_p, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_void_p,
+                             c_void_p, c_void_p]),
+    "rr_zscan_pairs": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment), c_int,
+                               c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
+                               c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_pack_band_rows": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p,
                                   c_void_p, c_void_p]),
     "rr_zchi2_batch_plain_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32]),

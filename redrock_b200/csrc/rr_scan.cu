@@ -36,14 +36,27 @@
 #include <mutex>
 
 #include "rr_common.cuh"
+#include "rr_solve_dev.cuh"
 
 namespace rr {
 
-constexpr int kWarps = 8;
+#ifndef RR_Q_UNROLL
+#define RR_Q_UNROLL 1
+#endif
+
+#ifndef RR_SCAN_WARPS
+#define RR_SCAN_WARPS 8
+#endif
+#ifndef RR_SCAN_STAGES
+#define RR_SCAN_STAGES 2
+#endif
+
+constexpr int kQUnroll = RR_Q_UNROLL;
+constexpr int kWarps = RR_SCAN_WARPS;  // redshifts per tile (one per warp)
 constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = RR_CHUNK;
 constexpr int kWin = kChunk + 2 * kHalfBand;  // basis rows per chunk window
-constexpr int kStages = 2;
+constexpr int kStages = RR_SCAN_STAGES;      // copy pipeline depth
 constexpr int kRwChunkDoubles = kChunk * RR_RW * RR_LANES;
 
 struct FusedParams {
@@ -74,13 +87,11 @@ struct StageBufs {
   }
 };
 
-// completed-phase counters of the two stage barriers, kept in registers
+// phase parity of each stage barrier (bit s), kept in a register
 struct Uses {
-  uint32_t u0 = 0, u1 = 0;
-  __device__ __forceinline__ uint32_t parity(int s) const { return (s ? u1 : u0) & 1u; }
-  __device__ __forceinline__ void bump(int s) {
-    if (s) ++u1; else ++u0;
-  }
+  uint32_t bits = 0;
+  __device__ __forceinline__ uint32_t parity(int s) const { return (bits >> s) & 1u; }
+  __device__ __forceinline__ void bump(int s) { bits ^= 1u << s; }
 };
 
 __device__ __forceinline__ void chunk_segment(const FusedParams& p, int64_t c, int& seg,
@@ -118,130 +129,6 @@ __device__ __forceinline__ void issue_chunk(const FusedParams& p, const rr_scan_
   }
 }
 
-// LDL^T of the packed lower triangle of a symmetric matrix (row-major,
-// a[i(i+1)/2 + j], j <= i), then the solve for c.  Works on its own copy
-// so the caller's accumulator stays in registers.  Returns false on an
-// exactly zero pivot (redrock's singular case), leaving c unspecified.
-template <int NB>
-__device__ __forceinline__ bool ldlt_solve(const double (&m)[NB * (NB + 1) / 2],
-                                           const double (&y)[NB], double (&c)[NB]) {
-  constexpr int kTri = NB * (NB + 1) / 2;
-  double a[kTri];
-#pragma unroll
-  for (int i = 0; i < kTri; ++i) a[i] = m[i];
-#define A(i, j) a[(i) * ((i) + 1) / 2 + (j)]
-  double d[NB];
-  bool ok = true;
-#pragma unroll
-  for (int j = 0; j < NB; ++j) {
-    double v[NB];
-    double dj = A(j, j);
-#pragma unroll
-    for (int k = 0; k < NB; ++k) {
-      if (k < j) {
-        v[k] = A(j, k) * d[k];
-        dj -= A(j, k) * v[k];
-      }
-    }
-    ok = ok && (dj != 0.0);
-    d[j] = dj;
-    const double inv = 1.0 / dj;
-#pragma unroll
-    for (int i = 0; i < NB; ++i) {
-      if (i > j) {
-        double s = A(i, j);
-#pragma unroll
-        for (int k = 0; k < NB; ++k)
-          if (k < j) s -= A(i, k) * v[k];
-        A(i, j) = s * inv;
-      }
-    }
-  }
-  // L z = y
-#pragma unroll
-  for (int i = 0; i < NB; ++i) {
-    double s = y[i];
-#pragma unroll
-    for (int k = 0; k < NB; ++k)
-      if (k < i) s -= A(i, k) * c[k];
-    c[i] = s;
-  }
-#pragma unroll
-  for (int i = 0; i < NB; ++i) c[i] /= d[i];
-  // L^T c = z
-#pragma unroll
-  for (int ii = 0; ii < NB; ++ii) {
-    const int i = NB - 1 - ii;
-    double s = c[i];
-#pragma unroll
-    for (int k = 0; k < NB; ++k)
-      if (k > i) s -= A(k, i) * c[k];
-    c[i] = s;
-  }
-#undef A
-  return ok;
-}
-
-// Relative accuracy assumed for the FP64 sums M, y and f^T W f (about 90
-// ulp; calibrated against redrock's direct residual), and the chi2 error
-// above which a (target, z) is re-evaluated by the direct residual.
-constexpr double kSumEps = 1e-14;
-constexpr double kChi2FixTol = 1e-6;
-
-// Solve and chi2 for one (target, z) from its normal equations.
-// chi2 = f^T W f - c^T y - c^T P c.  Also returns an upper estimate of that
-// value's rounding error, kSumEps (sum_i |c_i| sqrt(M_ii) + sqrt(f^T W f))^2,
-// which bounds |c^T dM c| + 2|c^T dy| + |d(f^T W f)| for relative errors
-// kSumEps in the sums.  Returns false when the system is singular (or the
-// target has no weight, or the method is unsupported).
-template <int NB>
-__device__ __forceinline__ bool solve_eval(const rr_scan_template& tm,
-                                           const double (&m)[NB * (NB + 1) / 2],
-                                           const double (&y)[NB], double fwf, double wsum,
-                                           double (&c)[NB], double& chi2, double& err) {
-  constexpr int kTri = NB * (NB + 1) / 2;
-  bool ok = (wsum != 0.0) && (tm.method == RR_SOLVE_PCA);
-  double s = 0.0;
-  if (ok) {
-    double mp[kTri];
-#pragma unroll
-    for (int i = 0; i < kTri; ++i) mp[i] = m[i];
-    if (tm.prior) {
-#pragma unroll
-      for (int i = 0; i < NB; ++i)
-#pragma unroll
-        for (int j = 0; j <= i; ++j) mp[i * (i + 1) / 2 + j] += tm.prior[i * NB + j];
-    }
-    ok = ldlt_solve<NB>(mp, y, c);
-#pragma unroll
-    for (int i = 0; i < NB; ++i) s = fma(fabs(c[i]), sqrt(fmax(m[i * (i + 1) / 2 + i], 0.0)), s);
-  }
-  if (!ok) {
-#pragma unroll
-    for (int i = 0; i < NB; ++i) c[i] = 0.0;
-    chi2 = kHugeChi2;
-    err = 0.0;
-    return false;
-  }
-  double cy = 0.0;
-#pragma unroll
-  for (int i = 0; i < NB; ++i) cy = fma(c[i], y[i], cy);
-  double cpc = 0.0;
-  if (tm.prior) {
-#pragma unroll
-    for (int i = 0; i < NB; ++i) {
-      double t = 0.0;
-#pragma unroll
-      for (int j = 0; j < NB; ++j) t = fma(tm.prior[i * NB + j], c[j], t);
-      cpc = fma(c[i], t, cpc);
-    }
-  }
-  chi2 = fwf - cy - cpc;
-  const double a = s + sqrt(fwf);
-  err = kSumEps * a * a;
-  return true;
-}
-
 template <int NB>
 __device__ __forceinline__ void write_eval(const rr_scan_template& tm, int64_t row, int z,
                                            const double (&c)[NB], double chi2, double wsum) {
@@ -272,11 +159,15 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
   const int lane = threadIdx.x & 31;
   const int stride = tm.basis_stride;
   const int64_t nchunk = p.chunks_total;
-  if (threadIdx.x == 0) issue_chunk(p, tm, block, z0, nzt, 0, 0, sb);
+  // prologue: the first kStages - 1 chunks in flight
+  if (threadIdx.x == 0)
+    for (int i = 0; i < kStages - 1 && i < nchunk; ++i) issue_chunk(p, tm, block, z0, nzt, i, i, sb);
+  int s = 0;
   for (int64_t ch = 0; ch < nchunk; ++ch) {
-    const int s = (int)(ch & 1);
-    const bool more = ch + 1 < nchunk;
-    if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ch + 1, s ^ 1, sb);
+    const int64_t ahead = ch + kStages - 1;
+    const bool more = ahead < nchunk;
+    const int s_ahead = (s + kStages - 1) % kStages;
+    if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ahead, s_ahead, sb);
     const bool ok = mbar_wait(&sb.full[s], uses.parity(s), p.status);
     uses.bump(s);
     if (active && ok) {
@@ -284,7 +175,7 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
       const double* ts = sb.t(s) + warp * kWin * stride;
       // two pixels per step: basis row q + k serves pixel q (band index k)
       // and pixel q + 1 (band index k - 1), so each row is read once
-#pragma unroll 1
+#pragma unroll kQUnroll
       for (int q = 0; q < kChunk; q += 2) {
         double ta[NB], tb[NB];
 #pragma unroll
@@ -334,13 +225,19 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
         }
       }
     }
-    // stage s is free for chunk ch + 2 once every warp is past this point;
-    // a timed-out wait anywhere stops the whole CTA
+    // stage s is free for chunk ch + kStages once every warp is past this
+    // point; a timed-out wait anywhere stops the whole CTA
     if (__syncthreads_or(!ok)) {
-      // let the copy of chunk ch + 1 (if issued) land before leaving
-      if (threadIdx.x == 0 && more) mbar_wait(&sb.full[s ^ 1], uses.parity(s ^ 1), p.status);
+      // let the copies already issued land before leaving
+      if (threadIdx.x == 0)
+        for (int64_t i = ch + 1; i < nchunk && i <= ahead; ++i) {
+          const int si = (int)((s + (i - ch)) % kStages);
+          mbar_wait(&sb.full[si], uses.parity(si), p.status);
+          uses.bump(si);
+        }
       return false;
     }
+    s = (s + 1 == kStages) ? 0 : s + 1;
   }
   return true;
 }
@@ -372,7 +269,7 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   if (valid) {
     const double fwf = p.tg.fwf[block * RR_LANES + lane];
     wsum = p.tg.wsum[block * RR_LANES + lane];
-    const bool ok = solve_eval<NB>(tm, m, y, fwf, wsum, c, chi2, err);
+    const bool ok = solve_eval<NB>(tm.method, tm.prior, m, y, fwf, wsum, c, chi2, err);
     fix = ok && err > kChi2FixTol;
     write_eval<NB>(tm, row, z0 + warp, c, chi2, wsum);
   }
@@ -397,7 +294,7 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
 __host__ __device__ constexpr bool in_common_set(int nb) { return nb == 4 || nb == 5 || nb == 10; }
 
 template <bool COMMON>
-__global__ void __launch_bounds__(kThreads, 1) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
+__global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ int64_t s_tile;
   StageBufs sb;
@@ -764,7 +661,12 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   RR_CUDA_TRY(cudaGetDevice(&dev));
   RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
-  const int64_t grid = ntiles < nsm ? ntiles : nsm;
+  int per_sm = 1;
+  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<COMMON>,
+                                                            kThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  const int64_t slots = (int64_t)nsm * per_sm;
+  const int64_t grid = ntiles < slots ? ntiles : slots;
   zscan_fused_kernel<COMMON><<<(unsigned)grid, kThreads, smem, stream>>>(p);
   RR_CHECK_LAUNCH();
   return RR_OK;

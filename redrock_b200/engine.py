@@ -111,6 +111,8 @@ class TemplateSource:
         self.z = to_device(self.zhost)
         self.oii = oii
         self.method = method
+        self.x_first = float(wave[0])
+        self.x_last = float(wave[-1])
         if len(self.zhost):
             self.xmin = float(wave[0] * (1 + self.zhost.max()))
             self.xmax = float(wave[-1] * (1 + self.zhost.min()))
@@ -403,6 +405,91 @@ def run_fused(pack, bases, stream=None, status=None):
                               stream_handle(stream))
         _lib.check(rc, "rr_zscan_fused")
     return results, st
+
+
+# ---------------------------------------------------------------------------
+# pair scan: arbitrary (target, z) pairs, template rebinned on the fly
+# ---------------------------------------------------------------------------
+class RowPack:
+    """Targets packed target-major for the pair scan (rr_pack_rows)."""
+
+    def __init__(self, dbatch, stream=None, status=None):
+        L = _lib.lib()
+        dev = device()
+        b = dbatch.batch
+        self.batch = b
+        self.layout = b.layout
+        self.ntarget = b.ntarget
+        self.npix_row = b.npix_block
+        self.rows = torch.zeros((b.ntarget, b.npix_block, _lib.RW), dtype=torch.float64, device=dev)
+        self.fwf = torch.zeros(max(b.ntarget, 1), dtype=torch.float64, device=dev)
+        self.wsum = torch.zeros(max(b.ntarget, 1), dtype=torch.float64, device=dev)
+        self._status = status or StatusWord(dev)
+        if b.nspec:
+            rc = L.rr_pack_rows(ptr(dbatch.descs), b.nspec, ptr(dbatch.first), b.ntarget,
+                                ptr(dbatch.rdata), ptr(dbatch.roffs), ptr(dbatch.ivar),
+                                ptr(dbatch.flux), ptr(dbatch.segs), len(b.segs), b.npix_block,
+                                ptr(self.rows), ptr(self.fwf), ptr(self.wsum), self._status.ptr,
+                                stream_handle(stream))
+            _lib.check(rc, "rr_pack_rows")
+        # pair segments: one per (grid, slot) segment, with its grid arrays
+        self.segments = []
+        for sd in b.segs:
+            g = self.layout.pix_offset.index(sd.basis_offset)
+            e, w, _, _ = self.layout.device_arrays(g)
+            self.segments.append(_lib.PairSegment(ptr(e), ptr(w), self.layout.npix[g],
+                                                  sd.rw_offset,
+                                                  float(np.min(self.layout.waves[g]))))
+
+    @classmethod
+    def from_targets(cls, targets, layout, stream=None):
+        return cls(TargetBatch(targets, layout).to_device(), stream=stream)
+
+    def check(self):
+        self._status.check("rr_pack_rows")
+
+
+def pair_ranges_ok(src, layout, z):
+    """Host check of redrock's rebin range rule (rebin.py:330-341) for each
+    redshift: every grid's edges inside [x0 (1+z), x_end (1+z)]."""
+    z = np.asarray(z, dtype=np.float64)
+    x0 = float(src.x_first)
+    x1 = float(src.x_last)
+    ok = np.ones(len(z), dtype=bool)
+    for i in range(len(layout.keys)):
+        _, _, emin, emax = layout.device_arrays(i)
+        ok &= ~((emin < x0 * (1 + z)) | (emax > x1 * (1 + z)))
+    return ok
+
+
+def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
+    """chi2 (n,), coeff (n, nbasis), penalty (n,) device tensors for the
+    pairs (target index into the packed targets, redshift)."""
+    L = _lib.lib()
+    dev = device()
+    n = len(pair_z)
+    nb = src.nbasis
+    chi2 = torch.empty(n, dtype=torch.float64, device=dev)
+    coeff = torch.empty((n, nb), dtype=torch.float64, device=dev)
+    pen = torch.zeros(n, dtype=torch.float64, device=dev)
+    if n == 0:
+        return chi2, coeff, pen
+    dt = to_device(np.asarray(pair_target, dtype=np.int32), torch.int32)
+    dz = to_device(np.asarray(pair_z, dtype=np.float64))
+    oii = None if src.oii is None else to_device(src.oii)
+    prior = None if getattr(src, "prior", None) is None else to_device(src.prior)
+    tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0,
+                           ptr(prior), ptr(oii))
+    segs = (_lib.PairSegment * len(rowpack.segments))(*rowpack.segments)
+    st = status or StatusWord(dev)
+    rc = L.rr_zscan_pairs(ctypes.byref(tm), segs, len(rowpack.segments), ptr(rowpack.rows),
+                          ptr(rowpack.fwf), ptr(rowpack.wsum), rowpack.npix_row, ptr(dt), ptr(dz),
+                          n, ptr(chi2), ptr(coeff), ptr(pen), st.ptr, stream_handle(stream))
+    _lib.check(rc, "rr_zscan_pairs")
+    if status is None:
+        torch.cuda.current_stream().synchronize()
+        st.check("rr_zscan_pairs")
+    return chi2, coeff, pen
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,248 @@
+"""Fine-grid refinement of the coarse chi2 minima on the GPU (redrock fitz).
+
+Same contract as redrock 0.22 ``fitz.fitz`` (fitz.py:133-395) for PCA
+templates: for each coarse minimum (best first) that is more than
+max_velo_diff away from the results so far, scan a ``zminfit_npoints`` grid
+between its neighbours, fit a parabola to the three points around the best
+one, fit the template once more at the parabola minimum, set ZWARN bits, and
+return the results sorted by chi2.
+
+All chi2 evaluations run in the pair-scan kernel (``rr_zscan_pairs``): one
+launch per template evaluates the fine grids of every target's candidate
+minima (each target at its own redshifts), and one more launch does the
+single-z fits at the parabola minima.  The sequential candidate logic is
+replayed on the host with the precomputed fine grids (candidates beyond the
+first batch are fetched in further launches only for targets that need
+them), so the decisions are redrock's.
+
+``fitz_targets`` is the batched entry point (many targets, one template);
+``fitz`` keeps redrock's single-target signature.  Archetype fits are not
+implemented (NotImplementedError).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .engine import GridLayout, RowPack, TemplateSource, pair_ranges_ok, run_pairs
+
+C_KMS = 299792.458          # scipy.constants.speed_of_light / 1000
+MAX_VELO_DIFF = 1000.0      # constants.py:7
+MAX_VELO_DIFF_STAR = 100.0  # constants.py:8
+Z_FITLIMIT = 2 ** 5         # zwarning.py:20
+BAD_MINFIT = 2 ** 10        # zwarning.py:25
+
+
+def get_dv(z, zref):
+    """Velocity difference in km/s (fitz.py:28-43)."""
+    return C_KMS * (z - zref) / (1.0 + zref)
+
+
+def find_minima(x):
+    """Indices of local minima including edges, sorted by value (fitz.py:46-67)."""
+    x = np.asarray(x)
+    ii = np.where(np.r_[True, x[1:] <= x[:-1]] & np.r_[x[:-1] <= x[1:], True])[0]
+    jj = np.argsort(x[ii])
+    return ii[jj]
+
+
+def minfit(x, y):
+    """y = y0 + ((x - x0)/xerr)^2 through 3 points (fitz.py:70-110)."""
+    if len(x) < 3:
+        return (-1, -1, -1, BAD_MINFIT)
+    try:
+        a, b, c = np.polyfit(x, y, 2)
+    except np.linalg.LinAlgError:
+        return (-1, -1, -1, BAD_MINFIT)
+    if a == 0.0:
+        return (-1, -1, -1, BAD_MINFIT)
+    x0 = -b / (2 * a)
+    y0 = -(b ** 2) / (4 * a) + c
+    zwarn = 0
+    if (x0 <= np.min(x)) or (np.max(x) <= x0):
+        zwarn |= BAD_MINFIT
+    if (y0 <= 0.):
+        zwarn |= BAD_MINFIT
+    if a > 0.0:
+        xerr = 1 / np.sqrt(a)
+    else:
+        xerr = 1 / np.sqrt(-a)
+        zwarn |= BAD_MINFIT
+    return (x0, xerr, y0, zwarn)
+
+
+class _Refiner:
+    """Device state shared by the pair launches of one fitz_targets call."""
+
+    def __init__(self, targets, template, layout=None, rowpack=None):
+        if layout is None:
+            dwave = {}
+            for t in targets:
+                for s in t.spectra:
+                    dwave.setdefault(s.wavehash, s.wave)
+            layout = GridLayout.from_dwave(dwave)
+        self.layout = layout
+        self.rows = rowpack or RowPack.from_targets(targets, layout)
+        self.src = TemplateSource.from_template(template)
+        self.oii = getattr(template, "OIItemplate", None)
+
+    def scan(self, tidx, z):
+        """chi2 (+ [OII] penalty for the fine grids) and coefficients at the
+        given (target, z) pairs; pairs outside the template range -> None."""
+        z = np.asarray(z, dtype=np.float64)
+        tidx = np.asarray(tidx, dtype=np.int32)
+        ok = pair_ranges_ok(self.src, self.layout, z)
+        chi2 = np.full(len(z), np.nan)
+        pen = np.zeros(len(z))
+        coeff = np.full((len(z), self.src.nbasis), np.nan)
+        sel = np.nonzero(ok)[0]
+        if len(sel):
+            c2, co, pe = run_pairs(self.rows, self.src, tidx[sel], z[sel])
+            chi2[sel] = c2.cpu().numpy()
+            coeff[sel] = co.cpu().numpy()
+            pen[sel] = pe.cpu().numpy()
+        return chi2, coeff, pen, ok
+
+
+def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=None,
+                 use_gpu=True, deg_legendre=None, zminfit_npoints=15, per_camera=False,
+                 n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=2):
+    """redrock's fitz for many targets of one template; returns a list of
+    per-target result dicts (the same dict-of-arrays fitz returns)."""
+    if archetype is not None:
+        raise NotImplementedError("archetype refinement is not implemented by the GPU engine")
+    redshifts = np.asarray(redshifts)
+    nz = 15 if zminfit_npoints is None else zminfit_npoints
+    maxv = MAX_VELO_DIFF_STAR if template.template_type == 'STAR' else MAX_VELO_DIFF
+    ref = _Refiner(targets, template, layout, rowpack)
+    has_oii = ref.oii is not None
+
+    ntg = len(targets)
+    cands = [find_minima(np.asarray(z)) for z in zchi2_list]
+    pos = [0] * ntg           # next candidate to evaluate
+    fine = [dict() for _ in range(ntg)]   # imin -> (zz, zzchi2)
+    results = [list() for _ in range(ntg)]
+    state = [dict(ci=0) for _ in range(ntg)]   # replay cursor per target
+    done = [False] * ntg
+    want = nminima + batch_extra
+
+    def fetch(tlist, count):
+        tid, zs, key = [], [], []
+        for j in tlist:
+            c = cands[j]
+            for imin in c[pos[j]:pos[j] + count]:
+                ilo = max(0, imin - 1)
+                ihi = min(imin + 1, len(redshifts) - 1)
+                zz = np.linspace(redshifts[ilo], redshifts[ihi], nz)
+                tid += [j] * nz
+                zs.append(zz)
+                key.append((j, imin, zz))
+            pos[j] = min(len(c), pos[j] + count)
+        if not key:
+            return
+        chi2, _, pen, ok = ref.scan(tid, np.concatenate(zs))
+        if not np.all(ok):
+            raise ValueError('edges must be within input x range')
+        off = 0
+        for j, imin, zz in key:
+            zzchi2 = chi2[off:off + nz].copy()
+            if has_oii:
+                zzchi2 += pen[off:off + nz]
+            fine[j][imin] = (zz, zzchi2)
+            off += nz
+
+    pending_final = []   # (target, result dict, zmin)
+    active = list(range(ntg))
+    fetch(active, want)
+    while active:
+        need_more = []
+        for j in active:
+            c = cands[j]
+            st = state[j]
+            while st['ci'] < len(c) and len(results[j]) < nminima:
+                imin = c[st['ci']]
+                if imin not in fine[j]:
+                    break        # not fetched yet
+                st['ci'] += 1
+                zprev = np.array([tmp['z'] for tmp in results[j]])
+                dv = get_dv(z=redshifts[imin], zref=zprev)
+                if np.any(np.abs(dv) < maxv):
+                    continue
+                zz, zzchi2 = fine[j][imin]
+                i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
+                zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])
+                zbest = zmin
+                zerr = sigma
+                if zbest < zz[0] or zbest > zz[-1]:
+                    zwarn |= BAD_MINFIT
+                    k = np.where(zzchi2 == np.min(zzchi2))[0][0]
+                    zbest = zz[k]
+                    chi2min = zzchi2[k]
+                if zbest < redshifts[1] or zbest > redshifts[-2]:
+                    zwarn |= Z_FITLIMIT
+                if zmin < redshifts[1] or zmin > redshifts[-2]:
+                    zwarn |= Z_FITLIMIT
+                zprev = np.array([tmp['z'] for tmp in results[j]])
+                dv = get_dv(z=zbest, zref=zprev)
+                if np.any(np.abs(dv) < maxv):
+                    continue
+                r = dict(z=zbest, zerr=zerr, zwarn=zwarn, chi2=chi2min, zz=zz, zzchi2=zzchi2,
+                         coeff=None, fitmethod=template.method)
+                results[j].append(r)
+                pending_final.append((j, r, zmin))
+            if len(results[j]) < nminima and st['ci'] < len(c):
+                need_more.append(j)
+        if need_more:
+            fetch(need_more, want)
+        active = need_more
+
+    # single-z fits at the parabola minima (fitz.py:263-293); a minimum
+    # outside the template's valid range gets zero coefficients and
+    # Z_FITLIMIT | BAD_MINFIT when it is also outside the scanned range
+    if pending_final:
+        tj = [p[0] for p in pending_final]
+        zm = np.array([p[2] for p in pending_final], dtype=np.float64)
+        _, coeff, _, ok = ref.scan(tj, zm)
+        for (j, r, zmin), co, good in zip(pending_final, coeff, ok):
+            if good:
+                r['coeff'] = co[None, :]
+            elif zmin < redshifts[0] or redshifts[-1] < zmin:
+                r['coeff'] = np.zeros(template.nbasis)
+                r['zwarn'] |= Z_FITLIMIT
+                r['zwarn'] |= BAD_MINFIT
+            else:
+                raise ValueError('edges must be within input x range')
+
+    out = []
+    for j, t in enumerate(targets):
+        res = results[j]
+        ii = np.argsort([tmp['chi2'] for tmp in res])
+        res = [res[i] for i in ii]
+        if len(res) == 0:
+            xfloat = np.zeros((0, 1), dtype=float)
+            xint = np.zeros((0, 1), dtype=int)
+            xstr = np.zeros((0, 1), dtype=str)
+            out.append(dict(z=xfloat, zerr=xfloat, zwarn=xint, chi2=xfloat, zz=xfloat,
+                            zzchi2=xfloat, coeff=xfloat, fitmethod=xstr, npixels=xint))
+            continue
+        npix = 0
+        for s in t.spectra:
+            npix += (np.asarray(s.ivar) > 0.).sum()
+        for r in res:
+            r['npixels'] = npix
+        tmp = {}
+        for k in res[0].keys():
+            tmp[k] = np.vstack([r[k] for r in res])
+        out.append(tmp)
+    return out
+
+
+def fitz(zchi2, redshifts, target, template, nminima=3, archetype=None, use_gpu=False,
+         deg_legendre=None, zminfit_npoints=15, per_camera=False, n_nearest=None,
+         prior_sigma=None):
+    """redrock's single-target fitz signature (fitz.py:133)."""
+    return fitz_targets([zchi2], redshifts, [target], template, nminima=nminima,
+                        archetype=archetype, use_gpu=use_gpu, deg_legendre=deg_legendre,
+                        zminfit_npoints=zminfit_npoints, per_camera=per_camera,
+                        n_nearest=n_nearest, prior_sigma=prior_sigma)[0]

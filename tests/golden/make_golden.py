@@ -38,6 +38,7 @@ def import_redrock():
     import redrock.igm
     import redrock.templates
     import redrock.targets
+    import redrock.fitz
     return redrock
 
 
@@ -143,6 +144,11 @@ def main():
         out[f"scan_{key}_zchi2"] = zc
         out[f"scan_{key}_zcoeff"] = co
         out[f"scan_{key}_penalty"] = pe
+        # fitz on the coarse results (zfind.py:356-363 passes zchi2 + penalty)
+        for j, tg_ in enumerate(rtg):
+            zf = rr.fitz.fitz(zc[j] + pe[j], tmpl.redshifts, tg_, tmpl, nminima=3)
+            for k in ("z", "zerr", "zwarn", "chi2", "coeff", "npixels"):
+                out[f"fitz_{key}_{j}_{k}"] = np.asarray(zf[k])
     # --- scan: redrock's test-utility fixture (2 exposures per camera) -------
     ut = [synth.util_target(0.2, seed=21, targetid=111), synth.util_target(0.25, seed=22,
                                                                             targetid=222)]
