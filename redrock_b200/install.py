@@ -26,6 +26,8 @@ PATCHES = {
     ("fitz", "calc_zchi2_one"): ("zscan", "calc_zchi2_one"),
     ("fitz", "calc_zchi2_batch"): ("zscan", "calc_zchi2_batch"),
     ("fitz", "transmission_Lyman"): ("igm", "transmission_Lyman"),
+    ("fitz", "fitz"): ("fitz", "fitz"),
+    ("zfind", "fitz"): ("fitz", "fitz"),
     ("archetypes", "trapz_rebin"): ("rebin", "trapz_rebin"),
     ("archetypes", "transmission_Lyman"): ("igm", "transmission_Lyman"),
 }

@@ -1,0 +1,191 @@
+"""Redshift finding driver on the GPU engine (redrock zfind.py:220-711).
+
+``zfind(targets, templates, nminima=3, ...)`` runs, for the local targets:
+
+  1. the coarse scan of every template in one fused launch
+     (``calc_zchi2_targets``),
+  2. the fine-grid refinement of every target's minima, one batched pair-scan
+     launch group per template (``fitz_targets``),
+  3. redrock's finalisation: NODATA / LITTLE_COVERAGE bits, sort by badfit
+     bits then chi2, keep ``nminima`` per spectral type, delta-chi2 and
+     SMALL_DELTA_CHI2 (``calc_deltachi2``, zfind.py:103-155).
+
+It returns ``(allresults, allzfit)`` like redrock, except that ``allzfit`` is
+a dict of numpy columns (``astropy.table.Table(allzfit)`` gives redrock's
+table) with redrock's column names and order of rows.  Single-process only
+(``targets.comm`` None); archetypes and priors are not supported.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import fitz as _fitz
+from .templates import parse_fulltype
+from .zscan import calc_zchi2_targets
+
+MAX_VELO_DIFF = 1000.0
+MAX_VELO_DIFF_STAR = 100.0
+MIN_DELTACHI2 = 9.0                 # constants.py:10
+SMALL_DELTA_CHI2 = 2 ** 2           # zwarning.py:17
+LITTLE_COVERAGE = 2 ** 1
+NODATA = 2 ** 9
+NEGATIVE_MODEL = 2 ** 3
+MANY_OUTLIERS = 2 ** 4
+Z_FITLIMIT = 2 ** 5
+NEGATIVE_EMISSION = 2 ** 6
+BAD_MINFIT = 2 ** 10
+BADFIT_MASK = NEGATIVE_MODEL | MANY_OUTLIERS | Z_FITLIMIT | NEGATIVE_EMISSION | BAD_MINFIT
+
+
+def calc_deltachi2(chi2, z, zwarn, dvlimit=MAX_VELO_DIFF):
+    """chi2 difference to the next good fit farther than dvlimit; and which
+    fits have another good fit within MIN_DELTACHI2 (zfind.py:103-155)."""
+    nz = len(chi2)
+    deltachi2 = np.zeros(nz)
+    okfit = (zwarn & BADFIT_MASK) == 0
+    if np.isscalar(dvlimit):
+        dvlimit = np.full(nz, dvlimit)
+    for i in range(len(chi2) - 1):
+        dv = _fitz.get_dv(z[i + 1:], z[i])
+        ii = (np.abs(dv) > np.minimum(dvlimit[i], dvlimit[i + 1:])) & okfit[i + 1:]
+        if np.any(ii):
+            dchi2 = chi2[i + 1:] - chi2[i]
+            deltachi2[i] = np.min(dchi2[ii])
+    noti = np.ones(nz, dtype=bool)
+    setzwarn = np.zeros(nz, dtype=bool)
+    for i in range(nz):
+        noti[:] = True
+        noti[i] = False
+        alldeltachi2 = np.absolute(chi2[noti] - chi2[i])
+        alldv = np.absolute(_fitz.get_dv(z=z[noti], zref=z[i]))
+        alldvlimit = np.minimum(dvlimit[i], dvlimit[noti])
+        if np.any(okfit[noti] & (alldeltachi2 < MIN_DELTACHI2) & (alldv >= alldvlimit)):
+            setzwarn[i] = True
+    return deltachi2, setzwarn
+
+
+def sort_dict_by_cols(d, colnames, sort_first_column_first=True):
+    """Stable multi-key sort of a dict of arrays (zfind.py:53-80)."""
+    vals = tuple(d[c] for c in colnames)
+    if sort_first_column_first:
+        vals = vals[::-1]
+    idx = np.lexsort(vals, axis=0).flatten()
+    for k in d.keys():
+        d[k] = d[k][idx]
+
+
+def sort_zfit_dict(zfit):
+    """Sort by badfit bits, then chi2 (zfind.py:206-218)."""
+    zfit['__badfit__'] = (zfit['zwarn'] & BADFIT_MASK) != 0
+    sort_dict_by_cols(zfit, ('__badfit__', 'chi2'), sort_first_column_first=True)
+    zfit.pop('__badfit__')
+
+
+def _finalise_target(tid, fits, nminima):
+    tzfit = []
+    for fulltype, tmp in fits:
+        nmin = len(tmp['chi2'])
+        if nmin == 0:
+            print(f'WARNING: no {fulltype} chi2 vs. z minima for targetid {tid}')
+            continue
+        spectype, subtype = parse_fulltype(fulltype)
+        tmp = dict(tmp)
+        tmp['spectype'] = np.full((nmin, 1), spectype)
+        tmp['subtype'] = np.full((nmin, 1), subtype)
+        tmp['ncoeff'] = np.array([tmp['coeff'].shape[1]] * nmin).reshape((nmin, 1))
+        mv = MAX_VELO_DIFF_STAR if spectype.upper() == 'STAR' else MAX_VELO_DIFF
+        tmp['max_velo_diff'] = np.full((nmin, 1), mv)
+        tzfit.append(tmp)
+    maxncoeff = max(t['coeff'].shape[1] for t in tzfit)
+    for t in tzfit:
+        if t['coeff'].shape[1] < maxncoeff:
+            n = maxncoeff - t['coeff'].shape[1]
+            t['coeff'] = np.append(t['coeff'], np.zeros((t['coeff'].shape[0], n)), axis=1)
+    out = {}
+    for k in tzfit[0].keys():
+        out[k] = np.vstack([t[k] for t in tzfit])
+        if k != 'coeff' and out[k].shape[1] == 1:
+            out[k] = out[k].flatten()
+    n = len(out['chi2'])
+    out['targetid'] = np.array([tid] * n)
+    out['zwarn'][out['npixels'] == 0] |= NODATA
+    out['zwarn'][out['npixels'] < 10 * out['ncoeff']] |= LITTLE_COVERAGE
+    sort_zfit_dict(out)
+    keep = []
+    for spectype in np.unique(out['spectype']):
+        keep.extend(np.where(out['spectype'] == spectype)[0][0:nminima])
+    if len(keep) < n:
+        for k in out.keys():
+            out[k] = out[k][keep]
+        sort_zfit_dict(out)
+    n = len(out['chi2'])
+    out['znum'] = np.arange(n)
+    deltachi2, setzwarn = calc_deltachi2(out['chi2'], out['z'], out['zwarn'],
+                                         dvlimit=out['max_velo_diff'])
+    out['deltachi2'] = deltachi2
+    out['zwarn'][setzwarn] |= SMALL_DELTA_CHI2
+    del out['max_velo_diff']
+    return out
+
+
+def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
+          chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
+          n_nearest=None, prior_sigma=None):
+    if archetypes or priors is not None or chi2_scan is not None:
+        raise NotImplementedError("archetypes, priors and chi2_scan input are not supported by "
+                                  "the GPU zfind driver")
+    if targets.comm is not None and targets.comm.size > 1:
+        raise NotImplementedError("use one process per GPU with its own targets (see "
+                                  "redrock_b200.shard) instead of an MPI communicator")
+    results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
+    local = list(targets.local())
+    sort = np.array([t.template.full_type for t in templates]).argsort()
+    for t in np.array(list(templates), dtype=object)[sort]:
+        ft = t.template.full_type
+        chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
+        fits = _fitz.fitz_targets(chi2, t.template.redshifts, local, t.template,
+                                  nminima=nminima, zminfit_npoints=zminfit_npoints)
+        for tg, zf in zip(local, fits):
+            results[tg.id][ft]['zfit'] = zf
+    for tg in local:
+        results[tg.id]['meta'] = tg.meta
+    allresults = results
+    rows = []
+    for tid in targets.all_target_ids:
+        fits = [(ft, allresults[tid][ft]['zfit']) for ft in allresults[tid] if ft != 'meta']
+        for ft in allresults[tid]:
+            if ft != 'meta':
+                del allresults[tid][ft]['zfit']
+        rows.append(_finalise_target(tid, fits, nminima))
+    # stack the per-target tables (astropy.table.vstack equivalent)
+    cols = ['targetid'] + [k for k in rows[0] if k != 'targetid']
+    allzfit = {}
+    for k in cols:
+        allzfit[k] = np.concatenate([r[k] for r in rows], axis=0)
+    for k in list(allzfit):
+        if 'pca' in k.lower():
+            allzfit[k] = allzfit.pop(k)
+    metakeys = sorted(k for k in allresults[allzfit['targetid'][0]]['meta'].keys()
+                      if not k.endswith('_datatype'))
+    for mk in metakeys:
+        dt = allresults[allzfit['targetid'][0]]['meta'].get(mk + '_datatype')
+        allzfit[mk] = np.array([allresults[x]['meta'][mk] for x in allzfit['targetid']], dtype=dt)
+    for tid in targets.all_target_ids:
+        del allresults[tid]['meta']
+    if allzfit['subtype'].dtype != '<U20':
+        ml = max(20, max(len(s) for s in allzfit['subtype']))
+        allzfit['subtype'] = allzfit['subtype'].astype(f'<U{ml}')
+    if allzfit['spectype'].dtype != '<U6':
+        allzfit['spectype'] = allzfit['spectype'].astype('<U6')
+    maxcoeff = np.max([t.template.nbasis for t in templates])
+    co = allzfit['coeff']
+    ntarg, ncoeff = (co.shape[0], 1) if co.ndim == 1 else co.shape
+    if ncoeff != maxcoeff:
+        c = np.zeros((ntarg, maxcoeff), dtype=co.dtype)
+        c[:, 0:ncoeff] = co if co.ndim == 2 else co[:, None]
+        allzfit['coeff'] = c
+    if len(np.unique(allzfit['ncoeff'])) == 1:
+        m = int(np.unique(allzfit['ncoeff'])[0])
+        allzfit['coeff'] = allzfit['coeff'][:, 0:m]
+    return allresults, allzfit

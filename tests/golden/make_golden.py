@@ -31,6 +31,7 @@ def import_redrock():
     sys.modules["astropy.table"].Table = None
     sys.modules["fitsio"].FITS = None
     sys.modules["astropy"].io = sys.modules["astropy.io"]
+    sys.modules["astropy"].table = sys.modules["astropy.table"]
     sys.modules["astropy.io"].fits = sys.modules["astropy.io.fits"]
     sys.path.insert(0, REDROCK_PY)
     import redrock.zscan
@@ -42,7 +43,62 @@ def import_redrock():
     return redrock
 
 
+class _Column(np.ndarray):
+    """Stand-in for astropy.table.Column (array with a name)."""
+
+    def __new__(cls, data, name=None, dtype=None):
+        obj = np.asarray(data, dtype=dtype).view(cls)
+        obj.name = name
+        return obj
+
+
+class _Table(dict):
+    """Minimal stand-in for astropy.table.Table as zfind uses it (dict of
+    columns; the redrock numbers are untouched)."""
+
+    def __init__(self, cols=None):
+        super().__init__()
+        for k, v in (cols or {}).items():
+            self[k] = np.asarray(v)
+
+    @property
+    def colnames(self):
+        return list(self.keys())
+
+    @property
+    def columns(self):
+        return self
+
+    def move_to_end(self, key, last=True):
+        v = self.pop(key)
+        if last:
+            self[key] = v
+        else:
+            items = list(self.items())
+            self.clear()
+            self[key] = v
+            for k, x in items:
+                self[k] = x
+
+    def add_column(self, col):
+        self[col.name] = np.asarray(col)
+
+    def replace_column(self, name, col):
+        self[name] = np.asarray(col)
+
+
+def _vstack(tables):
+    out = _Table()
+    for k in tables[0].keys():
+        out[k] = np.concatenate([np.asarray(t[k]) for t in tables], axis=0)
+    return out
+
+
 rr = import_redrock()
+sys.modules["astropy.table"].Table = _Table
+sys.modules["astropy.table"].vstack = _vstack
+sys.modules["astropy.table"].Column = _Column
+import redrock.zfind  # noqa: E402
 import scipy.sparse  # noqa: E402
 
 
@@ -202,6 +258,23 @@ def main():
     out["singular_zchi2"] = zc
     out["singular_zcoeff"] = co
     out["singular_penalty"] = pe
+    # --- zfind end to end (coarse scan, fitz, finalisation) ------------------
+    ztg = synth.make_targets(5, seed=41, amp=2.0, first_id=5000)
+    out["zfind_targets_sha"] = np.array(synth.targets_checksum(ztg))
+    rz = ref_targets(ztg)
+    dz = rr.targets.DistTargetsCopy(rz)
+    sel = {"GALAXY": 23, "QSO": 31, "STAR:::K": 4, "STAR:::M": 4}
+    zt = []
+    for ts in tmpls:
+        if ts.full_type in sel:
+            tm = ref_template(ts)
+            tm._redshifts = ts.redshifts[::sel[ts.full_type]]
+            zt.append(rr.templates.DistTemplate(tm, dz.wavegrids()))
+    _, zfit = rr.zfind.zfind(dz, zt, mp_procs=1, nminima=3)
+    for k in ("targetid", "z", "zerr", "zwarn", "chi2", "deltachi2", "spectype", "subtype",
+              "ncoeff", "znum", "npixels", "coeff"):
+        out[f"zfind_{k}"] = np.asarray(zfit[k])
+    out["zfind_columns"] = np.array(list(zfit.keys()))
     path = os.path.join(HERE, "redrock_golden.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")

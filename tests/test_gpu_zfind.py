@@ -1,0 +1,41 @@
+"""zfind end to end (fused coarse scan -> batched GPU fitz -> finalisation)
+against redrock's own zfind on the same inputs.
+
+Tolerances: row order, targetid, spectype, subtype, ZWARN, znum, ncoeff and
+npixels identical; redshift |dz| <= 1e-7; chi2 and delta-chi2 |d| <= 1e-3;
+zerr relative 1e-5; coefficients |dc| <= 1e-5 max|c|.
+"""
+import numpy as np
+import pytest
+
+from tests.conftest import cuda_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+from redrock_b200 import synth  # noqa: E402
+
+
+def test_zfind_vs_redrock(golden):
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.zfind import zfind
+    ztg = synth.make_targets(5, seed=41, amp=2.0, first_id=5000)
+    assert synth.targets_checksum(ztg) == str(golden["zfind_targets_sha"])
+    dz = T.DistTargetsCopy(T.from_synth(ztg))
+    sel = {"GALAXY": 23, "QSO": 31, "STAR:::K": 4, "STAR:::M": 4}
+    dts = []
+    for ts in synth.template_set():
+        if ts.full_type in sel:
+            ts.redshifts = ts.redshifts[::sel[ts.full_type]]
+            dts.append(TM.DistTemplate(TM.from_synth(ts), dz.wavegrids()))
+    _, zfit = zfind(dz, dts, nminima=3)
+    assert list(zfit.keys()) == list(golden["zfind_columns"])
+    for k in ("targetid", "spectype", "subtype", "zwarn", "znum", "ncoeff", "npixels"):
+        np.testing.assert_array_equal(zfit[k], golden[f"zfind_{k}"], err_msg=k)
+    np.testing.assert_allclose(zfit["z"], golden["zfind_z"], rtol=0, atol=1e-7)
+    np.testing.assert_allclose(zfit["zerr"], golden["zfind_zerr"], rtol=1e-5)
+    assert np.max(np.abs(zfit["chi2"] - golden["zfind_chi2"])) <= 1e-3
+    assert np.max(np.abs(zfit["deltachi2"] - golden["zfind_deltachi2"])) <= 1e-3
+    g = golden["zfind_coeff"]
+    scale = np.maximum(np.abs(g).max(axis=1, keepdims=True), 1e-300)
+    assert np.all(np.abs(zfit["coeff"] - g) <= 1e-5 * scale)

@@ -107,7 +107,8 @@ def test_installer_rebinds_every_import_site():
     for sub, attr in PATCHES:
         mods.setdefault(sub, types.SimpleNamespace())
         setattr(mods[sub], attr, "original")
-    mods.setdefault("zfind", types.SimpleNamespace(calc_zchi2_targets="original"))
+    mods.setdefault("zfind", types.SimpleNamespace())
+    mods["zfind"].calc_zchi2_targets = "original"
     mods["zscan"].calc_zchi2_targets = "original"
     done = install(modules=mods)
     assert len(done) == len(PATCHES) + 2
@@ -123,3 +124,27 @@ def test_flop_model():
     assert round(bench.flops_per_eval(10, 7958)) == 2785853
     assert round(bench.flops_per_eval(4, 7958)) == 923189
     assert round(bench.flops_per_eval(5, 7958)) == 1193802
+
+
+def test_calc_deltachi2_known_answers():
+    # redrock test_zscan.py:101-111 / test_zfind.py
+    from redrock_b200.zfind import calc_deltachi2
+    chi2 = np.array([1.0, 2.0, 4.0, 8.0])
+    z = np.array([3.0, 3.1, 3.2, 3.3])
+    zwarn = np.array([0, 0, 0, 0])
+    dchi2, _ = calc_deltachi2(chi2, z, zwarn)
+    assert np.all(dchi2 == np.array([1, 2, 4, 0.0]))
+    z = np.array([3.0, 3.0, 4.0, 4.0])
+    dchi2, _ = calc_deltachi2(chi2, z, zwarn)
+    assert np.all(dchi2 == np.array([3, 2, 0.0, 0.0]))
+
+
+def test_find_minima_and_minfit():
+    from redrock_b200.fitz import find_minima, minfit
+    assert list(find_minima([1, 1, 1, 2, 2, 2])) == [0, 1, 2, 4, 5]
+    assert list(find_minima([3, 1, 2, 0, 5])) == [3, 1]
+    x = np.array([0.1, 0.2, 0.3])
+    x0, xerr, y0, zw = minfit(x, 2.0 + ((x - 0.21) / 0.05) ** 2)
+    assert abs(x0 - 0.21) < 1e-12 and abs(xerr - 0.05) < 1e-12 and abs(y0 - 2.0) < 1e-9
+    assert zw == 0
+    assert minfit(x[:2], x[:2])[3] == 2 ** 10
