@@ -32,6 +32,9 @@
  *   rr_pack_rows,
  *   rr_zscan_pairs          fitz.py:133-395 fine-grid refinement (every
  *                           target's own redshifts, batched)
+ *   rr_zscan_pairs_grad     adjoint of the pair scan: dchi2/dz,
+ *                           d2chi2/dz2, dchi2/dflux (Newton refinement in
+ *                           place of fitz.py:255-261's parabola)
  */
 #ifndef REDROCK_B200_H
 #define REDROCK_B200_H
@@ -241,14 +244,38 @@ int rr_pack_rows(const rr_spectrum_desc* specs /* device */, int64_t nspec,
                  const int64_t* target_first /* device, ntarget + 1 */, int64_t ntarget,
                  const double* rdata, const int32_t* roffsets, const double* ivar,
                  const double* flux, const rr_segment_desc* segs /* device */, int nseg,
-                 int64_t npix_row, double* rows, double* fwf, double* wsum, int* status,
-                 rr_stream_t stream);
+                 int64_t npix_row, double* rows, double* sw /* [ntarget][npix_row] sqrt(w),
+                 or NULL */, double* fwf, double* wsum, int* status, rr_stream_t stream);
 
 int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segment* segs /* host, <= 16 */,
                    int nseg, const double* rows, const double* fwf, const double* wsum,
                    int64_t npix_row, const int32_t* pair_target, const double* pair_z,
                    int64_t npairs, double* chi2, double* coeff /* [npairs][nbasis] */,
                    double* penalty /* [npairs] or NULL */, int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Adjoint of the pair scan (differentiation of chi2(z), configuration
+ * "Differentiation" of this engine; redrock refines z with the parabola of
+ * fitz.py:255-261 instead).  For each pair, besides chi2 (as the direct
+ * residual sum), coefficients and penalty:
+ *   dchi2_dz   = -2 sum_p w_p r_p (R dT/dz c)_p      (least-squares
+ *                stationarity: the coefficients' own z dependence drops out)
+ *   d2chi2_dz2 = 2 sum_p w_p (R dT/dz c)_p^2 - 2 (u-v)^T (M+P)^-1 (u-v)
+ *                (envelope curvature without the second derivative of T;
+ *                u = (R dT/dz)^T W r, v = (R T)^T W (R dT/dz c))
+ *   dchi2_dflux[pair][p] = 2 w_p r_p in the packed pixel order (optional;
+ *                needs sw from rr_pack_rows; not with a prior).
+ * dT/dz is exact for the trapezoid rebin (from the bin-edge values of the
+ * redshifted interpolant) and includes the smooth z dependence of the
+ * Inoue14 Lyman-continuum optical depth; on/off switches of IGM lines with z
+ * are steps with no derivative.
+ * ---------------------------------------------------------------------- */
+int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_segment* segs, int nseg,
+                        const double* rows, const double* sw, const double* fwf,
+                        const double* wsum, int64_t npix_row, const int32_t* pair_target,
+                        const double* pair_z, int64_t npairs, double* chi2, double* coeff,
+                        double* penalty, double* dchi2_dz, double* d2chi2_dz2,
+                        double* dchi2_dflux, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Plain per-target path (the structure of redrock's own GPU branch: R.T for

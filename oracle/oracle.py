@@ -362,3 +362,43 @@ def oii_template(wave, flux):
     """Template.OIItemplate (templates.py:172-174)."""
     isOII = (3724 <= wave) & (wave <= 3733)
     return flux[:, isOII]
+
+
+# ---------------------------------------------------------------------------
+# reference gradient (checker for the adjoint kernel)
+# ---------------------------------------------------------------------------
+
+def basis_and_dz(wave, flux, z, dwave, igm_model, h_igm=1e-7):
+    """T(z) per grid (npix, nb) and dT/dz: the trapezoid average of the
+    piecewise-linear template over a bin of width w obeys
+    dT/dz = (T - (e_hi y(e_hi) - e_lo y(e_lo)) / w) / (1+z) with y the
+    redshifted interpolant at the edges; the IGM factor's z derivative is a
+    central difference of transmission_Lyman (step h_igm)."""
+    T = template_basis(wave, flux, np.array([z]), dwave, igm_model)
+    out = {}
+    for k, w in dwave.items():
+        e = centers2edges(w)
+        Tr = trapz_rebin(wave, flux, edges=e, myz=np.array([z]))[0]     # (npix, nb)
+        xs = wave * (1 + z)
+        ye = np.stack([np.interp(e, xs, fb) for fb in flux], axis=1)   # (npix+1, nb)
+        dT = (Tr - (e[1:, None] * ye[1:] - e[:-1, None] * ye[:-1]) / np.diff(e)[:, None]) / (1 + z)
+        tr = transmission_Lyman(np.array([z]), w, model=igm_model, always_return_array=True)[0]
+        tp = transmission_Lyman(np.array([z + h_igm]), w, model=igm_model,
+                                always_return_array=True)[0]
+        tm = transmission_Lyman(np.array([z - h_igm]), w, model=igm_model,
+                                always_return_array=True)[0]
+        dtr = (tp - tm) / (2 * h_igm)
+        out[k] = (T[k][0], dT * tr[:, None] + Tr * dtr[:, None])
+    return out
+
+
+def chi2_grad_z(spectra, wave, flux, z, dwave, igm_model):
+    """(chi2, dchi2/dz) at z from the normal equations and stationarity."""
+    bd = basis_and_dz(wave, flux, z, dwave, igm_model)
+    Tb = np.vstack([s.Rcsr.dot(bd[s.wavehash][0]) for s in spectra])
+    dTb = np.vstack([s.Rcsr.dot(bd[s.wavehash][1]) for s in spectra])
+    w, f, wf = spectral_data(spectra)
+    M = Tb.T.dot(w[:, None] * Tb)
+    c = solve_pca(M, Tb.T.dot(wf))
+    r = f - Tb.dot(c)
+    return np.dot(w * r, r), -2.0 * np.dot(w * r, dTb.dot(c))

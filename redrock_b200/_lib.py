@@ -101,7 +101,11 @@ _SIGNATURES = {
                                c_void_p, c_void_p, c_void_p]),
     "rr_pack_rows": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
                              c_void_p, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_void_p,
-                             c_void_p, c_void_p]),
+                             c_void_p, c_void_p, c_void_p]),
+    "rr_zscan_pairs_grad": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment),
+                                    c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                    c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_zscan_pairs": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment), c_int,
                                c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
                                c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -28,7 +28,7 @@ namespace rr {
 constexpr int kPairThreads = 256;
 constexpr int kPairChunk = kPairThreads - 2 * kHalfBand;  // output pixels per chunk
 constexpr int kPairMaxSeg = 16;
-constexpr int kPairWin = 2048;  // template samples staged per chunk
+constexpr int kPairWin = 1536;  // template samples staged per chunk
 
 struct PairsParams {
   rr_pair_template tm;
@@ -44,6 +44,11 @@ struct PairsParams {
   double* chi2;
   double* coeff;
   double* penalty;
+  // gradient mode (rr_zscan_pairs_grad)
+  double* dchi2_dz;     // [npairs]
+  double* d2chi2_dz2;   // [npairs]
+  double* dchi2_dflux;  // [npairs][npix_row] or NULL
+  const double* sw;     // [ntarget][npix_row] sqrt(w), needed for dchi2_dflux
   int* status;
 };
 
@@ -65,6 +70,7 @@ constexpr int pair_stride() { return (NB & 1) ? NB : NB + 1; }
 template <int NB>
 struct PairSmem {
   double t[kPairThreads * pair_stride<NB>()];  // basis rows of the chunk + halo
+  double dt[kPairThreads * pair_stride<NB>()]; // their z derivatives (gradient mode)
   double xs[kPairWin];                          // staged template wavelengths
   double ys[NB * kPairWin];                     // staged template fluxes
   double red[kPairThreads / 32][NB * (NB + 1) / 2 + NB];
@@ -77,7 +83,7 @@ struct PairSmem {
 // Fill the shared basis rows for output pixels [c0 - 5, c0 + kPairChunk + 5)
 // of segment sg at redshift z.  Returns false if a bin fell outside the
 // template (never for pairs that pass the host-side range check).
-template <int NB>
+template <int NB, bool DZ>
 __device__ bool fill_rows(const PairsParams& p, const rr_pair_segment& sg, int64_t c0, double z,
                           double zp1, bool igm, PairSmem<NB>& sm) {
   constexpr int S = pair_stride<NB>();
@@ -106,52 +112,68 @@ __device__ bool fill_rows(const PairsParams& p, const rr_pair_segment& sg, int64
   bool ok = true;
   const int64_t ip = first + threadIdx.x;
   double* row = sm.t + threadIdx.x * S;
+  double* drow = sm.dt + threadIdx.x * S;
   if (ip < 0 || ip >= sg.npix) {
 #pragma unroll
     for (int b = 0; b < NB; ++b) row[b] = 0.0;
+    if (DZ)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) drow[b] = 0.0;
   } else {
-    double res[NB];
+    double res[kMaxRebinBasis], dres[DZ ? kMaxRebinBasis : 1];
     bool got = false;
     if (win > 0) {
       // rebin on the staged window: the bin must have a sample before and
       // after it inside the window, else fall back to the global arrays
-      double tmp[kMaxRebinBasis];
-      got = rebin_bin_strided(sm.xs, win, sm.ys, kPairWin, NB, zp1, sg.edges[ip], sg.edges[ip + 1],
-                              tmp);
-      if (got) {
-#pragma unroll
-        for (int b = 0; b < NB; ++b) res[b] = tmp[b];
-      }
+      got = rebin_bin_strided<DZ>(sm.xs, win, sm.ys, kPairWin, NB, zp1, sg.edges[ip],
+                                  sg.edges[ip + 1], res, dres);
     }
-    if (!got) {
-      double tmp[kMaxRebinBasis];
-      got = rebin_bin(tm.x, tm.nx, tm.y, NB, zp1, sg.edges[ip], sg.edges[ip + 1], tmp);
-#pragma unroll
-      for (int b = 0; b < NB; ++b) res[b] = tmp[b];
-    }
+    if (!got)
+      got = rebin_bin_strided<DZ>(tm.x, tm.nx, tm.y, tm.nx, NB, zp1, sg.edges[ip],
+                                  sg.edges[ip + 1], res, dres);
     if (!got) {
       ok = false;
 #pragma unroll
       for (int b = 0; b < NB; ++b) res[b] = 0.0;
+      if (DZ)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) dres[b] = 0.0;
     }
     if (igm) {
-      const double tr = transmission(tm.igm_model, z, sg.wave[ip]);
+      double dtr = 0.0;
+      const double tr = DZ ? transmission_dz(tm.igm_model, z, sg.wave[ip], &dtr)
+                           : transmission(tm.igm_model, z, sg.wave[ip]);
+      if (DZ)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) dres[b] = dres[b] * tr + res[b] * dtr;
 #pragma unroll
       for (int b = 0; b < NB; ++b) res[b] = dmul(res[b], tr);
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) row[b] = res[b];
+    if (DZ)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) drow[b] = dres[b];
   }
   __syncthreads();
   return ok;
 }
 
-// Accumulate Gram / y (RESID = false) or the residual sum (RESID = true)
-// over every pixel of the pair's target.
-template <int NB, bool RESID>
-__device__ bool pair_sweep(const PairsParams& p, int64_t t, double z, double (&m)[NB * (NB + 1) / 2],
-                           double (&y)[NB], const double* c, double& acc, PairSmem<NB>& sm) {
+// Sweep modes over every pixel of the pair's target:
+//   kGram:  Gram matrix m and y (forward);
+//   kResid: residual sum (g - Tb'.c)^2 into acc[0];
+//   kGrad:  residual sum, gradient and curvature accumulators with
+//           dTb' = R' dT/dz:  acc[0] = sum res^2, acc[1] = sum res (dTb'.c),
+//           acc[2] = sum (dTb'.c)^2, acc[3..3+NB) = u = dTb'^T res,
+//           acc[3+NB..3+2NB) = v = Tb'^T (dTb'.c); and dchi2/dflux.
+enum SweepMode { kGram = 0, kResid = 1, kGrad = 2 };
+
+template <int NB, int MODE>
+__device__ bool pair_sweep(const PairsParams& p, int64_t pr, int64_t t, double z,
+                           double (&m)[NB * (NB + 1) / 2], double (&y)[NB], const double* c,
+                           double* acc, PairSmem<NB>& sm) {
   constexpr int S = pair_stride<NB>();
+  constexpr bool DZ = MODE == kGrad;
   const double zp1 = dadd(1.0, z);
   bool ok = true;
   for (int s = 0; s < p.nseg; ++s) {
@@ -161,11 +183,11 @@ __device__ bool pair_sweep(const PairsParams& p, int64_t t, double z, double (&m
     // 1 there anyway
     const bool igm = p.tm.igm_model != RR_IGM_NONE && !(ddiv(sg.wave_min, zp1) > kLyA);
     for (int64_t c0 = 0; c0 < sg.npix; c0 += kPairChunk) {
-      ok = fill_rows<NB>(p, sg, c0, z, zp1, igm, sm) && ok;
+      ok = fill_rows<NB, DZ>(p, sg, c0, z, zp1, igm, sm) && ok;
       const int64_t ip = c0 + threadIdx.x;
       if (threadIdx.x < kPairChunk && ip < sg.npix) {
-        const double* rr =
-            p.rows + ((t * p.npix_row) + sg.row_offset + ip) * RR_RW;
+        const int64_t prow = (t * p.npix_row) + sg.row_offset + ip;
+        const double* rr = p.rows + prow * RR_RW;
         double r[kBand];
 #pragma unroll
         for (int k = 0; k < kBand; ++k) r[k] = rr[k];
@@ -179,13 +201,7 @@ __device__ bool pair_sweep(const PairsParams& p, int64_t t, double z, double (&m
 #pragma unroll
           for (int b = 0; b < NB; ++b) tb[b] = fma(r[k], trow[b], tb[b]);
         }
-        if (RESID) {
-          double model = 0.0;
-#pragma unroll
-          for (int b = 0; b < NB; ++b) model = fma(tb[b], c[b], model);
-          const double res = g - model;
-          acc = fma(res, res, acc);
-        } else {
+        if (MODE == kGram) {
 #pragma unroll
           for (int b = 0; b < NB; ++b) y[b] = fma(g, tb[b], y[b]);
 #pragma unroll
@@ -193,6 +209,37 @@ __device__ bool pair_sweep(const PairsParams& p, int64_t t, double z, double (&m
 #pragma unroll
             for (int b = 0; b <= a; ++b)
               m[a * (a + 1) / 2 + b] = fma(tb[a], tb[b], m[a * (a + 1) / 2 + b]);
+        } else {
+          double model = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b) model = fma(tb[b], c[b], model);
+          const double res = g - model;
+          acc[0] = fma(res, res, acc[0]);
+          if (MODE == kGrad) {
+            double db[NB];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) db[b] = 0.0;
+#pragma unroll
+            for (int k = 0; k < kBand; ++k) {
+              const double* drow = sm.dt + (threadIdx.x + k) * S;
+#pragma unroll
+              for (int b = 0; b < NB; ++b) db[b] = fma(r[k], drow[b], db[b]);
+            }
+            double dm = 0.0;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) dm = fma(db[b], c[b], dm);
+            acc[1] = fma(res, dm, acc[1]);
+            acc[2] = fma(dm, dm, acc[2]);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+              acc[3 + b] = fma(db[b], res, acc[3 + b]);
+              acc[3 + NB + b] = fma(tb[b], dm, acc[3 + NB + b]);
+            }
+            // d chi2 / d f_p = 2 w_p r_p = 2 sqrt(w_p) * (sqrt(w_p) r_p)
+            if (p.dchi2_dflux)
+              p.dchi2_dflux[pr * p.npix_row + sg.row_offset + ip] =
+                  2.0 * p.sw[prow] * res;
+          }
         }
       }
       __syncthreads();  // rows of this chunk fully consumed
@@ -222,11 +269,12 @@ __device__ void block_sum(double* v, int n, PairSmem<NB>& sm) {
   __syncthreads();
 }
 
-template <int NB>
+template <int NB, bool GRAD>
 __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __grid_constant__ PairsParams p) {
   extern __shared__ __align__(16) unsigned char pair_smem_raw[];
   PairSmem<NB>& sm = *reinterpret_cast<PairSmem<NB>*>(pair_smem_raw);
   constexpr int kTri = NB * (NB + 1) / 2;
+  constexpr int kAcc = 3 + 2 * NB;
   for (int64_t pr = blockIdx.x; pr < p.npairs; pr += gridDim.x) {
     const int64_t t = p.pair_target[pr];
     const double z = p.pair_z[pr];
@@ -235,23 +283,30 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
     double(&yy)[NB] = *reinterpret_cast<double(*)[NB]>(m + kTri);
 #pragma unroll
     for (int i = 0; i < kTri + NB; ++i) m[i] = 0.0;
-    double acc = 0.0;
-    bool ok = pair_sweep<NB, false>(p, t, z, mm, yy, nullptr, acc, sm);
+    double acc[kAcc];
+#pragma unroll
+    for (int i = 0; i < kAcc; ++i) acc[i] = 0.0;
+    bool ok = pair_sweep<NB, kGram>(p, pr, t, z, mm, yy, nullptr, acc, sm);
     if (!__syncthreads_and(ok)) {
       if (threadIdx.x == 0) {
         set_status(p.status, RR_ERANGE);
         p.chi2[pr] = nan("");
         for (int b = 0; b < NB; ++b) p.coeff[pr * NB + b] = nan("");
         if (p.penalty) p.penalty[pr] = nan("");
+        if (GRAD) {
+          p.dchi2_dz[pr] = nan("");
+          p.d2chi2_dz2[pr] = nan("");
+        }
       }
       continue;
     }
     block_sum<NB>(m, kTri + NB, sm);
+    bool solved = false;
     if (threadIdx.x == 0) {
       double c[NB], chi2 = 0.0, err = 0.0;
-      const bool solved =
-          solve_eval<NB>(p.tm.method, p.tm.prior, mm, yy, p.fwf[t], p.wsum[t], c, chi2, err);
-      sm.fix = solved && err > kChi2FixTol;
+      solved = solve_eval<NB>(p.tm.method, p.tm.prior, mm, yy, p.fwf[t], p.wsum[t], c, chi2, err);
+      sm.fix = (solved && err > kChi2FixTol) ? 1 : 0;
+      sm.bad = solved ? 0 : 1;
       for (int b = 0; b < NB; ++b) sm.c[b] = c[b];
       p.chi2[pr] = chi2;
       for (int b = 0; b < NB; ++b) p.coeff[pr * NB + b] = c[b];
@@ -263,13 +318,47 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
       }
     }
     __syncthreads();
+    if (GRAD) {
+      if (sm.bad) {
+        if (threadIdx.x == 0) {
+          p.dchi2_dz[pr] = 0.0;
+          p.d2chi2_dz2[pr] = 0.0;
+        }
+        __syncthreads();
+        continue;
+      }
+      // residual chi2 (exact), gradient and curvature in one more sweep
+      pair_sweep<NB, kGrad>(p, pr, t, z, mm, yy, sm.c, acc, sm);
+      block_sum<NB>(acc, kAcc, sm);
+      if (threadIdx.x == 0) {
+        // envelope curvature: 2 sum (dTb'.c)^2 - 2 (u - v)^T (M + P)^-1 (u - v)
+        double mp[kTri], uv[NB], x[NB];
+#pragma unroll
+        for (int i = 0; i < kTri; ++i) mp[i] = mm[i];
+        if (p.tm.prior)
+#pragma unroll
+          for (int i = 0; i < NB; ++i)
+#pragma unroll
+            for (int j = 0; j <= i; ++j) mp[i * (i + 1) / 2 + j] += p.tm.prior[i * NB + j];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) uv[b] = acc[3 + b] - acc[3 + NB + b];
+        double q = 0.0;
+        if (ldlt_solve<NB>(mp, uv, x))
+#pragma unroll
+          for (int b = 0; b < NB; ++b) q = fma(uv[b], x[b], q);
+        p.chi2[pr] = acc[0];
+        p.dchi2_dz[pr] = -2.0 * acc[1];
+        p.d2chi2_dz2[pr] = 2.0 * acc[2] - 2.0 * q;
+      }
+      __syncthreads();
+      continue;
+    }
     if (sm.fix) {
       // ill-conditioned: chi2 as the direct residual sum w (f - Tb c)^2
-      acc = 0.0;
-      pair_sweep<NB, true>(p, t, z, mm, yy, sm.c, acc, sm);
-      double v[1] = {acc};
-      block_sum<NB>(v, 1, sm);
-      if (threadIdx.x == 0) p.chi2[pr] = v[0];
+      acc[0] = 0.0;
+      pair_sweep<NB, kResid>(p, pr, t, z, mm, yy, sm.c, acc, sm);
+      block_sum<NB>(acc, 1, sm);
+      if (threadIdx.x == 0) p.chi2[pr] = acc[0];
     }
     __syncthreads();
   }
@@ -281,7 +370,8 @@ __global__ void pack_rows_kernel(const rr_spectrum_desc* __restrict__ specs, int
                                  const double* __restrict__ rdata, const int32_t* __restrict__ roff,
                                  const double* __restrict__ ivar, const double* __restrict__ flux,
                                  const rr_segment_desc* __restrict__ segs, int64_t npix_row,
-                                 double* __restrict__ rows, int* status) {
+                                 double* __restrict__ rows, double* __restrict__ sw_out,
+                                 int* status) {
   const int64_t s = blockIdx.y;
   if (s >= nspec) return;
   const rr_spectrum_desc sd = specs[s];
@@ -309,6 +399,7 @@ __global__ void pack_rows_kernel(const rr_spectrum_desc* __restrict__ specs, int
 #pragma unroll
   for (int k = 0; k < kBand; ++k) o[k] = sw * r[k];
   o[kBand] = sw * flux[sd.pix_offset + i];
+  if (sw_out) sw_out[(t * npix_row) + seg.rw_offset + i] = sw;
 }
 
 // f^T W f and sum w per target (spectra grouped by target, fixed order)
@@ -350,18 +441,18 @@ __global__ void pack_row_sums_kernel(const rr_spectrum_desc* __restrict__ specs,
   }
 }
 
-template <int NB>
+template <int NB, bool GRAD>
 static int launch_pairs(const PairsParams& p, cudaStream_t st) {
   const size_t smem = sizeof(PairSmem<NB>);
-  if (cudaFuncSetAttribute(zscan_pairs_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(zscan_pairs_kernel<NB, GRAD>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return RR_ECUDA;
   int dev = 0, nsm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return RR_ECUDA;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return RR_ECUDA;
   const int64_t grid = p.npairs < (int64_t)nsm * 4 ? p.npairs : (int64_t)nsm * 4;
-  zscan_pairs_kernel<NB><<<(unsigned)grid, kPairThreads, smem, st>>>(p);
+  zscan_pairs_kernel<NB, GRAD><<<(unsigned)grid, kPairThreads, smem, st>>>(p);
   if (cudaGetLastError() != cudaSuccess) return RR_ECUDA;
   return RR_OK;
 }
@@ -374,7 +465,8 @@ extern "C" int rr_pack_rows(const rr_spectrum_desc* specs, int64_t nspec,
                             const int64_t* target_first, int64_t ntarget, const double* rdata,
                             const int32_t* roffsets, const double* ivar, const double* flux,
                             const rr_segment_desc* segs, int nseg, int64_t npix_row, double* rows,
-                            double* fwf, double* wsum, int* status, rr_stream_t stream) {
+                            double* sw, double* fwf, double* wsum, int* status,
+                            rr_stream_t stream) {
   if (nspec < 0 || ntarget < 0 || nseg < 1 || npix_row < 1) return RR_EINVAL;
   if (nspec == 0 || ntarget == 0) return RR_OK;
   if (!specs || !target_first || !rdata || !roffsets || !ivar || !flux || !segs || !rows || !fwf ||
@@ -386,7 +478,7 @@ extern "C" int rr_pack_rows(const rr_spectrum_desc* specs, int64_t nspec,
     dim3 block(128);
     dim3 grid((unsigned)((npix_row + block.x - 1) / block.x), (unsigned)n);
     pack_rows_kernel<<<grid, block, 0, st>>>(specs + s0, n, rdata, roffsets, ivar, flux, segs,
-                                             npix_row, rows, status);
+                                             npix_row, rows, sw, status);
     if (cudaGetLastError() != cudaSuccess) return RR_ECUDA;
   }
   pack_row_sums_kernel<<<(unsigned)ntarget, 256, 0, st>>>(specs, target_first, ntarget, ivar, flux,
@@ -395,20 +487,19 @@ extern "C" int rr_pack_rows(const rr_spectrum_desc* specs, int64_t nspec,
   return RR_OK;
 }
 
-extern "C" int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segment* segs, int nseg,
-                              const double* rows, const double* fwf, const double* wsum,
-                              int64_t npix_row, const int32_t* pair_target, const double* pair_z,
-                              int64_t npairs, double* chi2, double* coeff, double* penalty,
-                              int* status, rr_stream_t stream) {
+static int pairs_params(PairsParams& p, const rr_pair_template* tmpl, const rr_pair_segment* segs,
+                        int nseg, const double* rows, const double* fwf, const double* wsum,
+                        int64_t npix_row, const int32_t* pair_target, const double* pair_z,
+                        int64_t npairs, double* chi2, double* coeff, double* penalty,
+                        int* status) {
   if (!tmpl || !segs || nseg < 1 || nseg > kPairMaxSeg || npix_row < 1 || npairs < 0)
     return RR_EINVAL;
-  if (npairs == 0) return RR_OK;
-  if (!rows || !fwf || !wsum || !pair_target || !pair_z || !chi2 || !coeff) return RR_EINVAL;
+  if (npairs > 0 && (!rows || !fwf || !wsum || !pair_target || !pair_z || !chi2 || !coeff))
+    return RR_EINVAL;
   if (!tmpl->x || !tmpl->y || tmpl->nx < 2 || tmpl->nbasis < 1 || tmpl->nbasis > RR_MAX_NBASIS)
     return RR_EINVAL;
   if (tmpl->igm_model < RR_IGM_NONE || tmpl->igm_model > RR_IGM_INOUE14) return RR_EINVAL;
   if (tmpl->oii && !penalty) return RR_EINVAL;
-  PairsParams p;
   memset(&p, 0, sizeof(p));
   p.tm = *tmpl;
   p.nseg = nseg;
@@ -429,20 +520,56 @@ extern "C" int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segmen
   p.coeff = coeff;
   p.penalty = penalty;
   p.status = status;
-  cudaStream_t st = (cudaStream_t)stream;
+  return RR_OK;
+}
+
+template <bool GRAD>
+static int dispatch_pairs(const PairsParams& p, int nbasis, cudaStream_t st) {
   int rc = upload_igm_tables(st);
   if (rc) return rc;
-  switch (tmpl->nbasis) {
-    case 1: return launch_pairs<1>(p, st);
-    case 2: return launch_pairs<2>(p, st);
-    case 3: return launch_pairs<3>(p, st);
-    case 4: return launch_pairs<4>(p, st);
-    case 5: return launch_pairs<5>(p, st);
-    case 6: return launch_pairs<6>(p, st);
-    case 7: return launch_pairs<7>(p, st);
-    case 8: return launch_pairs<8>(p, st);
-    case 9: return launch_pairs<9>(p, st);
-    case 10: return launch_pairs<10>(p, st);
+  switch (nbasis) {
+    case 1: return launch_pairs<1, GRAD>(p, st);
+    case 2: return launch_pairs<2, GRAD>(p, st);
+    case 3: return launch_pairs<3, GRAD>(p, st);
+    case 4: return launch_pairs<4, GRAD>(p, st);
+    case 5: return launch_pairs<5, GRAD>(p, st);
+    case 6: return launch_pairs<6, GRAD>(p, st);
+    case 7: return launch_pairs<7, GRAD>(p, st);
+    case 8: return launch_pairs<8, GRAD>(p, st);
+    case 9: return launch_pairs<9, GRAD>(p, st);
+    case 10: return launch_pairs<10, GRAD>(p, st);
     default: return RR_EINVAL;
   }
+}
+
+extern "C" int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segment* segs, int nseg,
+                              const double* rows, const double* fwf, const double* wsum,
+                              int64_t npix_row, const int32_t* pair_target, const double* pair_z,
+                              int64_t npairs, double* chi2, double* coeff, double* penalty,
+                              int* status, rr_stream_t stream) {
+  PairsParams p;
+  int rc = pairs_params(p, tmpl, segs, nseg, rows, fwf, wsum, npix_row, pair_target, pair_z,
+                        npairs, chi2, coeff, penalty, status);
+  if (rc || npairs == 0) return rc;
+  return dispatch_pairs<false>(p, tmpl->nbasis, (cudaStream_t)stream);
+}
+
+extern "C" int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_segment* segs,
+                                   int nseg, const double* rows, const double* sw,
+                                   const double* fwf, const double* wsum, int64_t npix_row,
+                                   const int32_t* pair_target, const double* pair_z,
+                                   int64_t npairs, double* chi2, double* coeff, double* penalty,
+                                   double* dchi2_dz, double* d2chi2_dz2, double* dchi2_dflux,
+                                   int* status, rr_stream_t stream) {
+  PairsParams p;
+  int rc = pairs_params(p, tmpl, segs, nseg, rows, fwf, wsum, npix_row, pair_target, pair_z,
+                        npairs, chi2, coeff, penalty, status);
+  if (rc || npairs == 0) return rc;
+  if (!dchi2_dz || !d2chi2_dz2 || (dchi2_dflux && !sw)) return RR_EINVAL;
+  if (tmpl->prior && dchi2_dflux) return RR_ENOTSUP;
+  p.dchi2_dz = dchi2_dz;
+  p.d2chi2_dz2 = d2chi2_dz2;
+  p.dchi2_dflux = dchi2_dflux;
+  p.sw = sw;
+  return dispatch_pairs<true>(p, tmpl->nbasis, (cudaStream_t)stream);
 }

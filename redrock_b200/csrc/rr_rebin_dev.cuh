@@ -158,6 +158,40 @@ static __device__ double transmission_calura_kamble(int model, double z, double 
   return T;
 }
 
+// d/dz of the Inoue14 Lyman-continuum optical depth at fixed observed
+// wavelength (the smooth part of the z dependence; the Lyman-series terms
+// depend on z only through their on/off masks).  Mirrors the branch
+// structure of transmission_inoue14.
+static __device__ double dtau_lc_dz_inoue14(double z, double lobs) {
+  const double zp1 = dadd(1.0, z);
+  if (!(lobs < dmul(kLamL, zp1))) return 0.0;
+  const double r = ddiv(lobs, kLamL);
+  const double r_m03 = pow(r, -3e-1);
+  double d = 0.0;
+  if (z < 2.0) {
+    d += 2.0 * 0.2113 * zp1 - 0.07661 * 2.3 * pow(zp1, 1.3) * r_m03;
+  } else {
+    d += 3.0 * 0.04696 * zp1 * zp1 - 0.01779 * 3.3 * pow(zp1, 2.3) * r_m03;
+  }
+  const double i21 = pow(r, 2.1);
+  if (z < 4.7) {
+    d += 2.545e-2 * 1.6 * pow(zp1, 0.6) * i21;
+  } else if (lobs > dmul(kLamL, dadd(1.0, 4.7)) || lobs < dmul(kLamL, dadd(1.0, 4.7))) {
+    d += 5.221e-4 * 3.4 * pow(zp1, 2.4) * i21;
+  }
+  return d;
+}
+
+__device__ __forceinline__ double transmission(int model, double z, double lobs);
+
+// Transmission and its smooth z derivative at one (z, wavelength).
+// Calura12 / Kamble20 depend on z only through line masks: derivative 0.
+__device__ __forceinline__ double transmission_dz(int model, double z, double lobs, double* dt) {
+  const double t = transmission(model, z, lobs);
+  *dt = (model == RR_IGM_INOUE14) ? -t * dtau_lc_dz_inoue14(z, lobs) : 0.0;
+  return t;
+}
+
 __device__ __forceinline__ double transmission(int model, double z, double lobs) {
   if (model == RR_IGM_INOUE14) return transmission_inoue14(z, lobs);
   if (model == RR_IGM_CALURA12 || model == RR_IGM_KAMBLE20)
@@ -174,10 +208,20 @@ constexpr int kMaxRebinBasis = 16;
 // Returns false (and leaves res untouched) when the bin falls outside the
 // redshifted input range; callers then report an error.
 // y[b * ystride + j] holds basis b at sample j.
+//
+// With DZ, dres[b] also receives dT/dz of the rebinned value.  Writing the
+// bin average as T = ((1+z)/w) * integral of the rest-frame interpolant over
+// [e_lo/(1+z), e_hi/(1+z)] gives
+//   dT/dz = (T - (e_hi y(e_hi) - e_lo y(e_lo)) / w) / (1+z),
+// where y(e) is the redshifted interpolant at the bin edges -- the edge
+// values the trapezoid sum already forms.  (T itself is unchanged, bit for
+// bit, by the extra output.)
+template <bool DZ = false>
 __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, int64_t nx,
                                                   const double* __restrict__ y, int64_t ystride,
                                                   int nb, double zp1, double e_lo, double e_hi,
-                                                  double* res) {
+                                                  double* res, double* dres = nullptr) {
+  double ylo_e[DZ ? kMaxRebinBasis : 1], yhi_e[DZ ? kMaxRebinBasis : 1];
   // first j with x[j] (1+z) > e_lo
   int64_t lo = 0, hi = nx;
   while (lo < hi) {
@@ -195,6 +239,7 @@ __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, 
       const double* yb = y + (int64_t)b * ystride;
       const double yedge = dadd(yb[j - 1], ddiv(dmul(dsub(e_lo, xjm1), dsub(yb[j], yb[j - 1])),
                                                  dsub(xj, xjm1)));
+      if (DZ) ylo_e[b] = yedge;
       res[b] = dadd(res[b], dmul(dmul(0.5, dadd(yb[j], yedge)), dsub(xj, e_lo)));
     }
     // interior samples
@@ -216,6 +261,7 @@ __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, 
       const double* yb = y + (int64_t)b * ystride;
       const double yedge = dadd(yb[j], ddiv(dmul(dsub(e_hi, xj), dsub(yb[j + 1], yb[j])),
                                             dsub(xn, xj)));
+      if (DZ) yhi_e[b] = yedge;
       res[b] = dadd(res[b], dmul(dmul(0.5, dadd(yedge, yb[j])), dsub(e_hi, xj)));
     }
   } else {
@@ -226,11 +272,18 @@ __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, 
       const double dx = dsub(xj, xjm1);
       const double ylo = dadd(yb[j], ddiv(dmul(dsub(e_lo, xj), slope_num), dx));
       const double yhi = dadd(yb[j], ddiv(dmul(dsub(e_hi, xj), slope_num), dx));
+      if (DZ) {
+        ylo_e[b] = ylo;
+        yhi_e[b] = yhi;
+      }
       res[b] = dadd(res[b], dmul(dmul(0.5, dadd(ylo, yhi)), dsub(e_hi, e_lo)));
     }
   }
   const double width = dsub(e_hi, e_lo);
   for (int b = 0; b < nb; ++b) res[b] = ddiv(res[b], width);
+  if (DZ)
+    for (int b = 0; b < nb; ++b)
+      dres[b] = (res[b] - (e_hi * yhi_e[b] - e_lo * ylo_e[b]) / width) / zp1;
   return true;
 }
 

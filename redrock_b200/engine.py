@@ -422,6 +422,7 @@ class RowPack:
         self.ntarget = b.ntarget
         self.npix_row = b.npix_block
         self.rows = torch.zeros((b.ntarget, b.npix_block, _lib.RW), dtype=torch.float64, device=dev)
+        self.sw = torch.zeros((b.ntarget, b.npix_block), dtype=torch.float64, device=dev)
         self.fwf = torch.zeros(max(b.ntarget, 1), dtype=torch.float64, device=dev)
         self.wsum = torch.zeros(max(b.ntarget, 1), dtype=torch.float64, device=dev)
         self._status = status or StatusWord(dev)
@@ -429,8 +430,8 @@ class RowPack:
             rc = L.rr_pack_rows(ptr(dbatch.descs), b.nspec, ptr(dbatch.first), b.ntarget,
                                 ptr(dbatch.rdata), ptr(dbatch.roffs), ptr(dbatch.ivar),
                                 ptr(dbatch.flux), ptr(dbatch.segs), len(b.segs), b.npix_block,
-                                ptr(self.rows), ptr(self.fwf), ptr(self.wsum), self._status.ptr,
-                                stream_handle(stream))
+                                ptr(self.rows), ptr(self.sw), ptr(self.fwf), ptr(self.wsum),
+                                self._status.ptr, stream_handle(stream))
             _lib.check(rc, "rr_pack_rows")
         # pair segments: one per (grid, slot) segment, with its grid arrays
         self.segments = []
@@ -490,6 +491,39 @@ def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
         torch.cuda.current_stream().synchronize()
         st.check("rr_zscan_pairs")
     return chi2, coeff, pen
+
+
+def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=None, status=None):
+    """chi2, coeff, penalty, dchi2/dz, d2chi2/dz2 (and dchi2/dflux
+    [n][npix_row] in the packed pixel order) device tensors for the pairs."""
+    L = _lib.lib()
+    dev = device()
+    n = len(pair_z)
+    nb = src.nbasis
+    chi2 = torch.empty(n, dtype=torch.float64, device=dev)
+    coeff = torch.empty((n, nb), dtype=torch.float64, device=dev)
+    pen = torch.zeros(n, dtype=torch.float64, device=dev)
+    g = torch.empty(n, dtype=torch.float64, device=dev)
+    h = torch.empty(n, dtype=torch.float64, device=dev)
+    df = torch.zeros((n, rowpack.npix_row), dtype=torch.float64, device=dev) if want_dflux else None
+    if n == 0:
+        return chi2, coeff, pen, g, h, df
+    dt = to_device(np.asarray(pair_target, dtype=np.int32), torch.int32)
+    dz = to_device(np.asarray(pair_z, dtype=np.float64))
+    oii = None if src.oii is None else to_device(src.oii)
+    tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0, None,
+                           ptr(oii))
+    segs = (_lib.PairSegment * len(rowpack.segments))(*rowpack.segments)
+    st = status or StatusWord(dev)
+    rc = L.rr_zscan_pairs_grad(ctypes.byref(tm), segs, len(rowpack.segments), ptr(rowpack.rows),
+                               ptr(rowpack.sw), ptr(rowpack.fwf), ptr(rowpack.wsum),
+                               rowpack.npix_row, ptr(dt), ptr(dz), n, ptr(chi2), ptr(coeff),
+                               ptr(pen), ptr(g), ptr(h), ptr(df), st.ptr, stream_handle(stream))
+    _lib.check(rc, "rr_zscan_pairs_grad")
+    if status is None:
+        torch.cuda.current_stream().synchronize()
+        st.check("rr_zscan_pairs_grad")
+    return chi2, coeff, pen, g, h, df
 
 
 # ---------------------------------------------------------------------------

@@ -72,6 +72,15 @@ def minfit(x, y):
     return (x0, xerr, y0, zwarn)
 
 
+class _NewtonCtx:
+    """The pair context refine_newton expects, built from a _Refiner."""
+
+    def __init__(self, ref):
+        self.layout = ref.layout
+        self.rows = ref.rows
+        self.src = ref.src
+
+
 class _Refiner:
     """Device state shared by the pair launches of one fitz_targets call."""
 
@@ -107,9 +116,16 @@ class _Refiner:
 
 def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=None,
                  use_gpu=True, deg_legendre=None, zminfit_npoints=15, per_camera=False,
-                 n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=2):
+                 n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=2,
+                 refine="parabola"):
     """redrock's fitz for many targets of one template; returns a list of
-    per-target result dicts (the same dict-of-arrays fitz returns)."""
+    per-target result dicts (the same dict-of-arrays fitz returns).
+
+    refine="parabola" is redrock's minfit through the three fine-grid points
+    around the best one.  refine="newton" instead runs safeguarded Newton
+    steps on chi2(z) (the adjoint kernel's dchi2/dz and envelope curvature)
+    inside that three-point cell, with zerr = sqrt(2 / d2chi2/dz2); the
+    decisions that follow (ZWARN bits, velocity separation) are the same."""
     if archetype is not None:
         raise NotImplementedError("archetype refinement is not implemented by the GPU engine")
     redshifts = np.asarray(redshifts)
@@ -152,6 +168,31 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             fine[j][imin] = (zz, zzchi2)
             off += nz
 
+    newton_ctx = {}
+
+    def newton_min(j, z3, chi2_mid):
+        # safeguarded Newton in [z3[0], z3[2]] from z3[1]
+        from .adjoint import refine_newton
+        ctx = newton_ctx.get("ctx")
+        if ctx is None:
+            ctx = newton_ctx["ctx"] = _NewtonCtx(ref)
+        z, c2, co, g, h, _ = refine_newton(ctx, np.array([j], dtype=np.int32),
+                                           np.array([z3[1]]), np.array([z3[0]]),
+                                           np.array([z3[2]]))
+        zwarn = 0
+        if h[0] > 0:
+            sigma = np.sqrt(2.0 / h[0])
+        else:
+            sigma = -1.0
+            zwarn |= BAD_MINFIT
+        if not (z3[0] < z[0] < z3[2]):
+            zwarn |= BAD_MINFIT
+        pen = 0.0
+        if has_oii:
+            s_ = float(np.dot(co[0], ref.src.oii))
+            pen = -s_ if s_ < 0 else 0.0
+        return z[0], sigma, c2[0] + pen, zwarn
+
     pending_final = []   # (target, result dict, zmin)
     active = list(range(ntg))
     fetch(active, want)
@@ -171,7 +212,10 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                     continue
                 zz, zzchi2 = fine[j][imin]
                 i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
-                zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])
+                if refine == "newton":
+                    zmin, sigma, chi2min, zwarn = newton_min(j, zz[i - 1:i + 2], zzchi2[i])
+                else:
+                    zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])
                 zbest = zmin
                 zerr = sigma
                 if zbest < zz[0] or zbest > zz[-1]:

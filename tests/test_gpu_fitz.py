@@ -61,3 +61,23 @@ def test_fitz_single_target_signature(golden):
     with pytest.raises(NotImplementedError):
         fitz.fitz(golden["scan_GALAXY_zchi2"][0], ts.redshifts, T.from_synth(tg)[0],
                   TM.from_synth(ts), archetype=object())
+
+
+def test_fitz_newton_refinement(golden):
+    """refine="newton" replaces the parabola: the refined z stays in the
+    same fine cell as the parabola's, and its chi2 is not higher."""
+    from redrock_b200 import fitz, targets as T, templates as TM
+    tg = scan_case()[:4]
+    ts = synth.template_set()[0]
+    ts.redshifts = golden["scan_GALAXY_z"]
+    chi2 = [golden["scan_GALAXY_zchi2"][j] + golden["scan_GALAXY_penalty"][j] for j in range(4)]
+    rtg = T.from_synth(tg)
+    par = fitz.fitz_targets(chi2, ts.redshifts, rtg, TM.from_synth(ts), nminima=3)
+    new = fitz.fitz_targets(chi2, ts.redshifts, rtg, TM.from_synth(ts), nminima=3,
+                            refine="newton")
+    step = np.diff(ts.redshifts).max() * 2 / 14
+    for a, b in zip(par, new):
+        good = (a["zwarn"] == 0)
+        assert np.all(np.abs(a["z"] - b["z"])[good] <= step)
+        assert np.all((b["chi2"] <= a["chi2"] + 1e-3)[good])
+        assert np.all(b["zerr"][good] > 0)
