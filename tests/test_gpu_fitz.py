@@ -64,8 +64,9 @@ def test_fitz_single_target_signature(golden):
 
 
 def test_fitz_newton_refinement(golden):
-    """refine="newton" replaces the parabola: the refined z stays in the
-    same fine cell as the parabola's, and its chi2 is not higher."""
+    """refine="newton" replaces the parabola: the refined z stays within a
+    fine-grid step of the parabola's, and its chi2 (a real evaluation, unlike
+    the parabola's fitted minimum) is not above the best fine-grid point."""
     from redrock_b200 import fitz, targets as T, templates as TM
     tg = scan_case()[:4]
     ts = synth.template_set()[0]
@@ -79,5 +80,6 @@ def test_fitz_newton_refinement(golden):
     for a, b in zip(par, new):
         good = (a["zwarn"] == 0)
         assert np.all(np.abs(a["z"] - b["z"])[good] <= step)
-        assert np.all((b["chi2"] <= a["chi2"] + 1e-3)[good])
+        best_grid = b["zzchi2"].min(axis=1)
+        assert np.all((b["chi2"] <= best_grid + 1e-6)[good])
         assert np.all(b["zerr"][good] > 0)
