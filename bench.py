@@ -19,6 +19,7 @@ scan (oracle/) on the host cores instead.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import subprocess
@@ -232,17 +233,20 @@ def run_ours(args, rank, world, local_rank):
             dts = [TM.DistTemplate(tm, dwave) for tm in tms]
             res = zscan.calc_zchi2_targets(dtg, dts)
             return res
-        for _ in range(max(1, min(args.warmup, 2))):
-            e2e_step()
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(args.steps):
-            e2e_step()
-        b.record()
+        # calc_zchi2_targets prints redrock's progress line; keep stdout for
+        # the one JSON result line
+        with contextlib.redirect_stdout(sys.stderr):
+            for _ in range(max(1, min(args.warmup, 2))):
+                e2e_step()
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(args.steps):
+                e2e_step()
+            b.record()
         torch.cuda.synchronize()
         e2e_ms = a.elapsed_time(b) / args.steps
         if world > 1:

@@ -27,12 +27,13 @@ import torch
 
 from . import _lib
 from .device import to_device, to_numpy
-from .engine import DeviceBasis, GridLayout, IdCache, PlainTarget, TargetPack, run_fused, run_plain
+from .engine import (DeviceBasis, GridLayout, IdCache, PlainTarget, TargetBatch, TargetPack,
+                     run_fused, run_plain)
 from .templates import oii_sums, solve_code
 
 HUGE_CHI2 = 9999999.0
 
-_pack_cache = IdCache(4)
+_pack_cache = IdCache(64)
 _basis_cache = IdCache(32)
 
 
@@ -95,13 +96,10 @@ def _pack(targets, layout):
 # ---------------------------------------------------------------------------
 # fused scan
 # ---------------------------------------------------------------------------
-def scan_device(targets, dtemplates):
-    """Fused scan of every target against every template.
+CHUNK_TARGETS = 128   # targets per pipelined chunk (4 target blocks)
 
-    Returns a list (one entry per template) of device ScanResult objects
-    with zchi2 (T, nz), zcoeff (T, nz, nbasis), penalty (T, nz).
-    """
-    layout = _layout_for(dtemplates[0], targets)
+
+def _bases_for(dtemplates, layout):
     bases = []
     for dt in dtemplates:
         b = _device_basis(dt, layout)
@@ -110,11 +108,55 @@ def scan_device(targets, dtemplates):
             b = DeviceBasis.from_tdata(dt.local.data, layout, redshifts=dt.local.redshifts,
                                        oii=oii_sums(dt.template), method=solve_code(dt.template))
         bases.append(b)
-    pack = _pack(targets, layout)
-    results, st = run_fused(pack, bases)
+    return bases
+
+
+def scan_device(targets, dtemplates, chunk=None):
+    """Fused scan of every target against every template.
+
+    Returns a list (one entry per template) of device ScanResult objects
+    with zchi2 (T, nz), zcoeff (T, nz, nbasis), penalty (T, nz).  Large
+    target lists are processed in chunks: the host packing and upload of
+    chunk k + 1 run while the GPU scans chunk k.
+    """
+    layout = _layout_for(dtemplates[0], targets)
+    bases = _bases_for(dtemplates, layout)
+    chunk = chunk or CHUNK_TARGETS
+    if len(targets) <= 2 * chunk:
+        pack = _pack(targets, layout)
+        results, st = run_fused(pack, bases)
+        torch.cuda.current_stream().synchronize()
+        st.check("rr_zscan_fused")
+        return results
+    from .device import StatusWord
+    st = StatusWord()
+    parts = []
+    keep = []
+    for i0 in range(0, len(targets), chunk):
+        sub = targets[i0:i0 + chunk]
+        pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
+                               lambda: TargetPack(TargetBatch(sub, layout).to_device(),
+                                                  status=st))
+        res, _ = run_fused(pack, bases, status=st)
+        parts.append(res)
+        keep.append(pack)
     torch.cuda.current_stream().synchronize()
     st.check("rr_zscan_fused")
-    return results
+    out = []
+    for it in range(len(bases)):
+        r = parts[0][it]
+        r.zchi2 = torch.cat([p[it].zchi2 for p in parts])
+        r.zcoeff = torch.cat([p[it].zcoeff for p in parts])
+        r.penalty = torch.cat([p[it].penalty for p in parts])
+        out.append(r)
+    return out
+
+
+def _to_host(t):
+    """Device tensor -> numpy through a pinned buffer."""
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t, non_blocking=True)
+    return h
 
 
 def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False):
@@ -125,9 +167,9 @@ def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False)
     if ntargets == 0:
         return np.zeros((0, nz)), np.zeros((0, nz, nbasis)), np.zeros((0, nz))
     res = scan_device(list(target_data), [dtemplate])[0]
-    zchi2 = res.zchi2.cpu().numpy()
-    zcoeff = res.zcoeff.cpu().numpy()
-    pen = res.penalty.cpu().numpy()
+    zchi2, zcoeff, pen = _to_host(res.zchi2), _to_host(res.zcoeff), _to_host(res.penalty)
+    torch.cuda.current_stream().synchronize()
+    zchi2, zcoeff, pen = zchi2.numpy(), zcoeff.numpy(), pen.numpy()
     if dtemplate.comm is None and progress is not None:
         for _ in range(ntargets):
             progress.put(1)
@@ -154,11 +196,11 @@ def calc_zchi2_targets(targets, templates, mp_procs=1, use_gpu=True):
     if len(tids) == 0:
         return results
     out = scan_device(data, list(templates))
-    for t, r in zip(templates, out):
+    host = [(_to_host(r.zchi2), _to_host(r.zcoeff), _to_host(r.penalty)) for r in out]
+    torch.cuda.current_stream().synchronize()
+    for t, (zc, co, pe) in zip(templates, host):
         ft = t.template.full_type
-        zc = r.zchi2.cpu().numpy()
-        co = r.zcoeff.cpu().numpy()
-        pe = r.penalty.cpu().numpy()
+        zc, co, pe = zc.numpy(), co.numpy(), pe.numpy()
         for i, tid in enumerate(tids):
             results.setdefault(tid, {})[ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
                                     zcoeff=co[i])

@@ -297,3 +297,24 @@ def test_best_z_recovers_truth_high_snr(rr):
     zbest = gal.redshifts[np.argmin(zc, axis=1)]
     ztrue = np.array([t.ztrue for t in tg])
     assert np.all(np.abs(np.log1p(zbest) - np.log1p(ztrue)) <= 3e-4)
+
+
+def test_chunked_pipeline_bit_identical(rr):
+    """Pipelined target chunks give bit-identical results to one launch
+    (each lane's sums do not depend on the block it sits in)."""
+    from redrock_b200 import zscan
+    tg = synth.make_targets(70, seed=71, mask_range=(0.0, 0.4), drop_camera_frac=0.1)
+    T, TM = rr["targets"], rr["templates"]
+    rtg = T.from_synth(tg)
+    dwave = T.DistTargetsCopy(rtg).wavegrids()
+    dts = [TM.DistTemplate(TM.from_synth(ts), dwave) for ts in synth.template_set(zsub=151)]
+    a = zscan.scan_device(rtg, dts, chunk=1000)
+    b = zscan.scan_device(rtg, dts, chunk=16)
+    for x, y in zip(a, b):
+        assert torch_equal(x.zchi2, y.zchi2) and torch_equal(x.zcoeff, y.zcoeff)
+        assert torch_equal(x.penalty, y.penalty)
+
+
+def torch_equal(a, b):
+    import torch
+    return bool(torch.equal(a, b))
