@@ -78,11 +78,15 @@ enum rr_solve_method { /* zscan.py:1107-1203 solve_matrices */
 #define RR_HALF_BAND 5           /* resolution offsets handled: -5..5 */
 #define RR_LANES 32              /* targets per target block */
 #define RR_RW 12                 /* doubles per (pixel, lane): 11 band + 1 */
-#define RR_CHUNK 16              /* pixels per scan stage */
+#ifndef RR_CHUNK
+#define RR_CHUNK 24              /* pixels per scan stage */
+#endif
 #define RR_MAX_TEMPLATES 16
 #define RR_MAX_NBASIS 10
 
 int rr_version(void);
+/* pixels per scan stage of this build: every npix_pad must be a multiple */
+int rr_scan_chunk(void);
 const char* rr_status_string(int status);
 /* last cudaError_t seen by a call of this library on this thread */
 int rr_last_cuda_error(void);

@@ -19,7 +19,7 @@ RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED = 0, 1
 HALF_BAND = 5
 LANES = 32
 RW = 12
-CHUNK = 16
+CHUNK = 24   # default; chunk() returns the loaded library's value
 MAX_TEMPLATES = 16
 MAX_NBASIS = 10
 
@@ -84,6 +84,7 @@ _lib = None
 
 _SIGNATURES = {
     "rr_version": (c_int, []),
+    "rr_scan_chunk": (c_int, []),
     "rr_status_string": (ctypes.c_char_p, [c_int]),
     "rr_last_cuda_error": (c_int, []),
     "rr_trapz_rebin": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
@@ -144,6 +145,11 @@ def lib():
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def chunk():
+    """Pixels per scan stage of the loaded library (npix_pad granularity)."""
+    return int(lib().rr_scan_chunk())
 
 
 def status_string(code):

@@ -51,10 +51,16 @@ namespace rr {
 #define RR_SCAN_STAGES 2
 #endif
 
+#ifndef RR_PIX
+#define RR_PIX 3
+#endif
+
 constexpr int kQUnroll = RR_Q_UNROLL;
+constexpr int kPix = RR_PIX;  // pixels per step of the pixel loop
 constexpr int kWarps = RR_SCAN_WARPS;  // redshifts per tile (one per warp)
 constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = RR_CHUNK;
+static_assert(kChunk % kPix == 0, "chunk must hold whole pixel steps");
 constexpr int kWin = kChunk + 2 * kHalfBand;  // basis rows per chunk window
 constexpr int kStages = RR_SCAN_STAGES;      // copy pipeline depth
 constexpr int kRwChunkDoubles = kChunk * RR_RW * RR_LANES;
@@ -173,55 +179,58 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     if (active && ok) {
       const double* rws = sb.rw(s) + lane;
       const double* ts = sb.t(s) + warp * kWin * stride;
-      // two pixels per step: basis row q + k serves pixel q (band index k)
-      // and pixel q + 1 (band index k - 1), so each row is read once
+      // kPix pixels per step: basis row q + k serves pixel q + i with band
+      // index k - i, so each row is read once for all kPix pixels
 #pragma unroll kQUnroll
-      for (int q = 0; q < kChunk; q += 2) {
-        double ta[NB], tb[NB];
+      for (int q = 0; q < kChunk; q += kPix) {
+        double tp[kPix][NB];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) { ta[b] = 0.0; tb[b] = 0.0; }
+        for (int i = 0; i < kPix; ++i)
 #pragma unroll
-        for (int k = 0; k <= kBand; ++k) {
+          for (int b = 0; b < NB; ++b) tp[i][b] = 0.0;
+#pragma unroll
+        for (int k = 0; k < kBand + kPix - 1; ++k) {
           const double* trow = ts + (q + k) * stride;
-          const double ra = k < kBand ? rws[(q * RR_RW + k) * RR_LANES] : 0.0;
-          const double rb = k > 0 ? rws[((q + 1) * RR_RW + k - 1) * RR_LANES] : 0.0;
+          double rk[kPix];
+#pragma unroll
+          for (int i = 0; i < kPix; ++i)
+            rk[i] = (k - i >= 0 && k - i < kBand) ? rws[((q + i) * RR_RW + k - i) * RR_LANES] : 0.0;
 #pragma unroll
           for (int b = 0; b + 1 < NB; b += 2) {
             const double2 tv = *reinterpret_cast<const double2*>(trow + b);
-            if (k < kBand) { ta[b] = fma(ra, tv.x, ta[b]); ta[b + 1] = fma(ra, tv.y, ta[b + 1]); }
-            if (k > 0) { tb[b] = fma(rb, tv.x, tb[b]); tb[b + 1] = fma(rb, tv.y, tb[b + 1]); }
+#pragma unroll
+            for (int i = 0; i < kPix; ++i) {
+              if (k - i >= 0 && k - i < kBand) {
+                tp[i][b] = fma(rk[i], tv.x, tp[i][b]);
+                tp[i][b + 1] = fma(rk[i], tv.y, tp[i][b + 1]);
+              }
+            }
           }
           if (NB & 1) {
             const double tv = trow[NB - 1];
-            if (k < kBand) ta[NB - 1] = fma(ra, tv, ta[NB - 1]);
-            if (k > 0) tb[NB - 1] = fma(rb, tv, tb[NB - 1]);
+#pragma unroll
+            for (int i = 0; i < kPix; ++i)
+              if (k - i >= 0 && k - i < kBand) tp[i][NB - 1] = fma(rk[i], tv, tp[i][NB - 1]);
           }
         }
-        const double ga = rws[(q * RR_RW + kBand) * RR_LANES];
-        const double gb = rws[((q + 1) * RR_RW + kBand) * RR_LANES];
-        if (RESID) {
-          double ma = 0.0, mb = 0.0;
 #pragma unroll
-          for (int b = 0; b < NB; ++b) { ma = fma(ta[b], c[b], ma); mb = fma(tb[b], c[b], mb); }
-          const double resa = ga - ma;
-          const double resb = gb - mb;
-          acc = fma(resa, resa, acc);
-          acc = fma(resb, resb, acc);
-        } else {
+        for (int i = 0; i < kPix; ++i) {
+          const double gi = rws[((q + i) * RR_RW + kBand) * RR_LANES];
+          if (RESID) {
+            double mi = 0.0;
 #pragma unroll
-          for (int b = 0; b < NB; ++b) y[b] = fma(ga, ta[b], y[b]);
+            for (int b = 0; b < NB; ++b) mi = fma(tp[i][b], c[b], mi);
+            const double res = gi - mi;
+            acc = fma(res, res, acc);
+          } else {
 #pragma unroll
-          for (int a = 0; a < NB; ++a)
+            for (int b = 0; b < NB; ++b) y[b] = fma(gi, tp[i][b], y[b]);
 #pragma unroll
-            for (int b = 0; b <= a; ++b)
-              m[a * (a + 1) / 2 + b] = fma(ta[a], ta[b], m[a * (a + 1) / 2 + b]);
+            for (int a = 0; a < NB; ++a)
 #pragma unroll
-          for (int b = 0; b < NB; ++b) y[b] = fma(gb, tb[b], y[b]);
-#pragma unroll
-          for (int a = 0; a < NB; ++a)
-#pragma unroll
-            for (int b = 0; b <= a; ++b)
-              m[a * (a + 1) / 2 + b] = fma(tb[a], tb[b], m[a * (a + 1) / 2 + b]);
+              for (int b = 0; b <= a; ++b)
+                m[a * (a + 1) / 2 + b] = fma(tp[i][a], tp[i][b], m[a * (a + 1) / 2 + b]);
+          }
         }
       }
     }
@@ -591,6 +600,8 @@ static thread_local int g_last_cuda_error = 0;
 extern "C" int rr_last_cuda_error(void) { return g_last_cuda_error; }
 
 extern "C" int rr_version(void) { return 1; }
+
+extern "C" int rr_scan_chunk(void) { return kChunk; }
 
 extern "C" const char* rr_status_string(int status) {
   switch (status) {

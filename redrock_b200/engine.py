@@ -59,7 +59,7 @@ class GridLayout:
         start = 0
         for key, npix, wave in grids:
             npix = int(npix)
-            npad = round_up(npix, _lib.CHUNK)
+            npad = round_up(npix, _lib.chunk())
             self.keys.append(key)
             self.npix.append(npix)
             self.npix_pad.append(npad)
