@@ -100,11 +100,33 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def make_workload(ntarget, seed, zsub=None):
+WORKLOADS = {
+    # the 500-target DESI-like batch (the headline)
+    "desi500": dict(ntarget=500),
+    # uneven batching: 0-40 % of pixels masked per target, 10 % of targets
+    # with one camera dropped, resolution width varying per camera
+    "uneven5000": dict(ntarget=5000, mask_range=(0.0, 0.4), drop_camera_frac=0.1),
+    # precision stress: 60 % QSO-like targets at z up to 6 rendered with
+    # Inoue14 IGM attenuation, S/N (amplitude) log-uniform 0.5-50
+    "stress20000": dict(ntarget=20000, qso_frac=0.6, snr_range=(0.5, 50.0)),
+}
+
+
+def make_workload(ntarget, seed, zsub=None, workload="desi500"):
     from redrock_b200 import synth
     from redrock_b200 import targets as T
     from redrock_b200 import templates as TM
-    tg = synth.make_targets(ntarget, seed=seed)
+    spec = dict(WORKLOADS[workload])
+    n = ntarget or spec.pop("ntarget")
+    spec.pop("ntarget", None)
+    if "qso_frac" in spec:
+        from redrock_b200.igm import transmission_Lyman
+
+        def tr(z, w):
+            return transmission_Lyman(np.array([z]), w, model="Inoue14")[0]
+        tg = synth.make_population(n, seed=seed, transmission=tr, **spec)
+    else:
+        tg = synth.make_targets(n, seed=seed, **spec)
     tset = synth.template_set(zsub=zsub)
     rtg = T.from_synth(tg)
     tms = [TM.from_synth(ts) for ts in tset]
@@ -171,7 +193,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     L = _lib.lib()
     tg, rtg, tset, tms = make_workload(args.ntargets, seed=args.seed + 7919 * rank,
-                                       zsub=args.zsub)
+                                       zsub=args.zsub, workload=args.workload)
     evals, flops = evals_and_flops(rtg, tms)
     layout = GridLayout.from_dwave(synth.camera_grids())
     srcs = [TemplateSource.from_template(tm) for tm in tms]
@@ -196,6 +218,16 @@ def run_ours(args, rank, world, local_rank):
         step(False)
     torch.cuda.synchronize()
     st.check("warm-up")
+    graph = None
+    if args.graph:
+        # the whole step (21 basis launches, packing, the fused scan) as one
+        # CUDA graph, replayed per step
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            step(False)
+        graph.replay()
+        torch.cuda.synchronize()
+        st.check("graph replay")
     launches_per_step = sum(len(layout.keys) for _ in srcs) + 2 + 1
 
     clocks = ClockSampler(torch.cuda.current_device())
@@ -207,7 +239,10 @@ def run_ours(args, rank, world, local_rank):
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
     for _ in range(args.steps):
-        step(True)
+        if graph is not None:
+            graph.replay()
+        else:
+            step(True)
     t1.record()
     torch.cuda.synchronize()
     if world > 1:
@@ -215,7 +250,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     st.check("timed steps")
     ms = t0.elapsed_time(t1) / args.steps
-    fused_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_fused]))
+    fused_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_fused])) if ev_fused else ms
     if world > 1:
         v = torch.tensor([ms, fused_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
@@ -297,13 +332,16 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded DESI-like targets and "
         "templates, redrock_b200/synth.py)",
-        "config": {"workload": WORKLOAD if args.ntargets == 500 and not args.zsub else
-                   f"reduced: {args.ntargets} targets, zsub={args.zsub}",
-                   "targets_per_gpu": args.ntargets,
+        "config": {"workload": (WORKLOAD if args.workload == "desi500" else args.workload)
+                   if not args.ntargets and not args.zsub else
+                   f"reduced {args.workload}: {len(rtg)} targets, zsub={args.zsub}",
+                   "targets_per_gpu": len(rtg),
                    "templates": [tm.full_type for tm in tms],
-                   "evals_per_step_per_gpu": evals, "pixels_per_target": 7958,
+                   "evals_per_step_per_gpu": evals,
+                   "pixels_per_target": "7958 (fewer with a dropped camera)",
                    "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
-                   "parallelism": f"targets sharded {world}-way, no collective"},
+                   "parallelism": f"targets sharded {world}-way, no collective",
+                   "cuda_graph": bool(args.graph)},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(),
                      "kernel": "zscan_fused_kernel",
@@ -377,7 +415,7 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded DESI-like targets and templates)",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": WORKLOAD if args.workload == "desi500" else args.workload},
         "cpu_baseline": {"value": value, "unit": "chi2 evals/s", "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "chi2 evals/s", "h2d_bytes_per_step": 0,
@@ -391,13 +429,17 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ntargets", type=int, default=500)
+    ap.add_argument("--workload", default="desi500", choices=sorted(WORKLOADS))
+    ap.add_argument("--ntargets", type=int, default=None,
+                    help="override the workload's number of targets")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--zsub", type=int, default=None,
                     help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--graph", action="store_true",
+                    help="capture the device step as a CUDA graph and replay it")
     ap.add_argument("--plain-targets", type=int, default=8)
     ap.add_argument("--ref-zsub", type=int, default=5)
     ap.add_argument("--ref-targets", type=int, default=4)

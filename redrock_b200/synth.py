@@ -281,13 +281,15 @@ def centers_to_edges(c):
 def make_targets(ntarget, seed=0, template=None, zrange=(0.0, 1.5), amp=1.0,
                  snr_range=None, mask_frac=0.05, mask_range=None,
                  drop_camera_frac=0.0, sigma_r=(0.8, 1.2), cameras=CAMERAS,
-                 first_id=1000):
+                 first_id=1000, transmission=None):
     """Seeded synthetic targets.
 
     Flux = R . rebin(template(z_true) . c) + N(0, sigma) with random
     coefficients c ~ N(0, 1) * amp (or amp drawn log-uniform from
     ``snr_range`` when given), sigma ~ U(0.5, 2), a random fraction of masked
     pixels, optionally one camera dropped for a fraction of targets.
+    ``transmission(z, wave) -> T`` (e.g. an IGM model) multiplies the
+    rendered template before the resolution is applied.
     """
     rng = np.random.default_rng(seed)
     if template is None:
@@ -318,10 +320,28 @@ def make_targets(ntarget, seed=0, template=None, zrange=(0.0, 1.5), amp=1.0,
             if ic == drop:
                 continue
             m = trapz_rebin_np(twave * (1 + z), model_rest, edges[name])
+            if transmission is not None:
+                m = m * np.asarray(transmission(z, wave), dtype=np.float64)
             flux = dia_matvec(rdata, roff, m) + rng.normal(size=npix) * noise
             tg.spectra.append(SpectrumSpec(name, wave, flux, ivar, rdata, roff))
         out.append(tg)
     return out
+
+
+def make_population(ntarget, seed=0, qso_frac=0.0, snr_range=None, mask_range=None,
+                    drop_camera_frac=0.0, transmission=None, first_id=1000):
+    """Mixed GALAXY / QSO-like targets, shuffled: a fraction qso_frac drawn
+    from the QSO basis at z ~ U(0.05, 6) (rendered with ``transmission``,
+    e.g. an IGM model), the rest GALAXY at z ~ U(0, 1.5)."""
+    rng = np.random.default_rng(seed)
+    nq = int(round(qso_frac * ntarget))
+    kw = dict(snr_range=snr_range, mask_range=mask_range, drop_camera_frac=drop_camera_frac)
+    gal = make_targets(ntarget - nq, seed=seed + 1, first_id=first_id, **kw)
+    qso = make_targets(nq, seed=seed + 2, template=qso_basis(), zrange=(0.05, 6.0),
+                       first_id=first_id + ntarget - nq, transmission=transmission, **kw)
+    out = gal + qso
+    order = rng.permutation(len(out))
+    return [out[i] for i in order]
 
 
 def checksum(arrays):
