@@ -250,6 +250,7 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     st.check("timed steps")
     ms = t0.elapsed_time(t1) / args.steps
+    resweeps = int(run_fused.last_counter[2].item()) if hasattr(run_fused, "last_counter") else None
     fused_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_fused])) if ev_fused else ms
     if world > 1:
         v = torch.tensor([ms, fused_ms], dtype=torch.float64, device="cuda")
@@ -346,6 +347,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peak, "traffic": traffic_from_profile(),
                      "kernel": "zscan_fused_kernel",
                      "kernel_ms": fused_ms, "flops_per_launch": fused_flops,
+                     "resweep_tiles_per_launch": resweeps,
                      "peak_source": "measured FP64 FMA peak (rr_fma_peak) on this GPU"},
         "e2e": e2e,
         "plain": plain,

@@ -205,9 +205,11 @@ typedef struct {
   int64_t npix_block;
 } rr_scan_targets;
 
-/* tile_counter: two device ints of scratch (reset by the call).  Templates
- * with nbasis 4, 5 or 10 run in one persistent launch, any others in a
- * second one. */
+/* tile_counter: three device ints of scratch (reset by the call); on
+ * return tile_counter[2] counts the tiles that were swept a second time to
+ * sum chi2 as the direct residual (ill-conditioned fits).  Templates with
+ * nbasis 4, 5 or 10 run in one persistent launch, any others in a second
+ * one. */
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                    int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
 

@@ -75,6 +75,7 @@ struct FusedParams {
   int64_t chunks_total;  // pixel chunks per block (over all segments)
   int max_stride;        // largest basis_stride
   int* tile_counter;
+  int* resweep_counter;  // tiles swept a second time for the direct residual
   int* status;
 };
 
@@ -286,6 +287,7 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   // sum w (f - Tb c)^2 (redrock's own formula, zscan.py:777-780), which does
   // not suffer the cancellation of f^T W f - c^T y
   if (__syncthreads_or(fix)) {
+    if (threadIdx.x == 0 && p.resweep_counter) atomicAdd(p.resweep_counter, 1);
     acc = 0.0;
     if (!sweep<NB, true>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
       failed = true;
@@ -638,7 +640,7 @@ static size_t fused_smem_bytes(int max_stride) {
 // by `pick` (indices into templates), using counter as its tile counter.
 template <bool COMMON>
 static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
-                        const int* pick, int npick, int* counter, int* status,
+                        const int* pick, int npick, int* counter, int* resweep, int* status,
                         cudaStream_t stream) {
   FusedParams p;
   memset(&p, 0, sizeof(p));
@@ -662,6 +664,7 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   }
   p.max_stride = max_stride;
   p.tile_counter = counter;
+  p.resweep_counter = resweep;
   p.status = status;
   const int64_t ntiles = p.tile_start[npick];
   if (ntiles == 0) return RR_OK;
@@ -715,12 +718,15 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     if (in_common_set(tm.nbasis)) common[nc++] = t; else other[no++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
+  RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, sizeof(int), st));
   if (nc) {
-    int rc = launch_fused<true>(targets, templates, common, nc, tile_counter, status, st);
+    int rc = launch_fused<true>(targets, templates, common, nc, tile_counter, tile_counter + 2,
+                                status, st);
     if (rc) return rc;
   }
   if (no) {
-    int rc = launch_fused<false>(targets, templates, other, no, tile_counter + 1, status, st);
+    int rc = launch_fused<false>(targets, templates, other, no, tile_counter + 1,
+                                 tile_counter + 2, status, st);
     if (rc) return rc;
   }
   return RR_OK;

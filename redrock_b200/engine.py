@@ -110,6 +110,7 @@ class TemplateSource:
         self.y = to_device(flux)
         self.z = to_device(self.zhost)
         self.oii = oii
+        self.oii_dev = None if oii is None else to_device(np.asarray(oii, dtype=np.float64))
         self.method = method
         self.x_first = float(wave[0])
         self.x_last = float(wave[-1])
@@ -154,7 +155,7 @@ class DeviceBasis:
         stride = round_up(nb, 2)
         z = src.zhost
         basis = torch.empty((len(z), layout.pix_stride, stride), dtype=torch.float64, device=dev)
-        kw.setdefault("oii", src.oii)
+        kw.setdefault("oii", src.oii_dev)
         kw.setdefault("method", src.method)
         if len(z) == 0:
             return cls(basis, layout, nb, z, **kw)
@@ -387,7 +388,7 @@ def run_fused(pack, bases, stream=None, status=None):
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
     tgs = pack.scan_targets_struct()
-    counter = torch.zeros(2, dtype=torch.int32, device=dev)
+    counter = torch.zeros(3, dtype=torch.int32, device=dev)
     st = status or StatusWord(dev)
     for i0 in range(0, len(bases), _lib.MAX_TEMPLATES):
         chunk = list(range(i0, min(len(bases), i0 + _lib.MAX_TEMPLATES)))
@@ -404,6 +405,7 @@ def run_fused(pack, bases, stream=None, status=None):
         rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
                               stream_handle(stream))
         _lib.check(rc, "rr_zscan_fused")
+    run_fused.last_counter = counter
     return results, st
 
 
@@ -477,7 +479,7 @@ def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
         return chi2, coeff, pen
     dt = to_device(np.asarray(pair_target, dtype=np.int32), torch.int32)
     dz = to_device(np.asarray(pair_z, dtype=np.float64))
-    oii = None if src.oii is None else to_device(src.oii)
+    oii = src.oii_dev
     prior = None if getattr(src, "prior", None) is None else to_device(src.prior)
     tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0,
                            ptr(prior), ptr(oii))
@@ -510,7 +512,7 @@ def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=N
         return chi2, coeff, pen, g, h, df
     dt = to_device(np.asarray(pair_target, dtype=np.int32), torch.int32)
     dz = to_device(np.asarray(pair_z, dtype=np.float64))
-    oii = None if src.oii is None else to_device(src.oii)
+    oii = src.oii_dev
     tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0, None,
                            ptr(oii))
     segs = (_lib.PairSegment * len(rowpack.segments))(*rowpack.segments)
