@@ -201,18 +201,18 @@ def run_ours(args, rank, world, local_rank):
     st = StatusWord()
     ev_fused = []
 
-    def step(record):
+    def step(record, ygemm=args.ygemm, sink=ev_fused):
         bases = [DeviceBasis.build(s, layout, status=st) for s in srcs]
         pack = TargetPack(dbatch, status=st)
         if record:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        res, _ = run_fused(pack, bases, status=st)
+        res, _ = run_fused(pack, bases, status=st, ygemm=ygemm)
         if record:
             e1.record()
-            ev_fused.append((e0, e1))
-        return res
+            sink.append((e0, e1))
+        return res, pack
 
     for _ in range(args.warmup):
         step(False)
@@ -228,7 +228,11 @@ def run_ours(args, rank, world, local_rank):
         graph.replay()
         torch.cuda.synchronize()
         st.check("graph replay")
+    # basis builds, target packing (2), the fused scan; with a tensor-core y:
+    # rr_pack_g, one rr_ygemm per template (+ column scales for int8x7)
     launches_per_step = sum(len(layout.keys) for _ in srcs) + 2 + 1
+    if args.ygemm != "fp64":
+        launches_per_step += 1 + len(srcs) * (2 if args.ygemm == "int8x7" else 1)
 
     clocks = ClockSampler(torch.cuda.current_device())
     if world > 1:
@@ -257,6 +261,8 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
         ms, fused_ms = float(v[0]), float(v[1])
     value = world * evals / (ms / 1e3)
+
+    study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
 
     # ---- end to end through the public API, host buffers ------------------
     e2e = None
@@ -342,7 +348,8 @@ def run_ours(args, rank, world, local_rank):
                    "pixels_per_target": "7958 (fewer with a dropped camera)",
                    "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
                    "parallelism": f"targets sharded {world}-way, no collective",
-                   "cuda_graph": bool(args.graph)},
+                   "cuda_graph": bool(args.graph),
+                   "y_term": args.ygemm},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(),
                      "kernel": "zscan_fused_kernel",
@@ -354,6 +361,52 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk,
     }
+    if study is not None:
+        out["ygemm_study"] = study
+    return out
+
+
+def ygemm_study(args, step, torch, evals):
+    """Throughput and zchi2/zcoeff error of each y variant (FP64 in the
+    scan, or the tensor-core GEMM in bf16x3 / tf32x3 / int8x7), errors
+    against the FP64 path on the same workload."""
+    huge = 9999999.0
+    out = {}
+    ref = None
+    fwf = None
+    for v in ["fp64", "bf16x3", "tf32x3", "int8x7"]:
+        step(False, ygemm=v)
+        torch.cuda.synchronize()
+        ev = []
+        res, pack = step(True, ygemm=v, sink=ev)
+        torch.cuda.synchronize()
+        ms = ev[0][0].elapsed_time(ev[0][1])
+        ent = {"value": evals / (ms / 1e3), "unit": "chi2 evals/s", "scan_ms": ms}
+        if v == "fp64":
+            ref = res
+            rows = pack.rows.long()
+            lane_fwf = pack.fwf
+            fwf = torch.zeros(int(rows.max()) + 1, dtype=torch.float64, device=lane_fwf.device)
+            ok = rows >= 0
+            fwf[rows[ok]] = lane_fwf[ok]
+        else:
+            dmax, drel, agree, n, cmax = 0.0, 0.0, 0, 0, 0.0
+            for a, b in zip(res, ref):
+                good = b.zchi2 < huge
+                d = (a.zchi2 - b.zchi2).abs().where(good, torch.zeros_like(b.zchi2))
+                dmax = max(dmax, float(d.max()))
+                drel = max(drel, float((d / fwf[:, None].clamp_min(1e-300)).max()))
+                agree += int((a.zchi2.argmin(dim=1) == b.zchi2.argmin(dim=1)).sum())
+                n += a.zchi2.shape[0]
+                sc = b.zcoeff.abs().amax(dim=-1, keepdim=True).clamp_min(1e-300)
+                cmax = max(cmax, float(((a.zcoeff - b.zcoeff).abs() / sc).max()))
+            ent.update({"max_abs_dchi2": dmax, "max_dchi2_over_fTWf": drel,
+                        "best_z_index_agreement": agree / n, "max_rel_dcoeff": cmax,
+                        "meets_dchi2_1e-3": dmax <= 1e-3})
+        out[v] = ent
+        del res
+    out["reference"] = ("errors against this engine's FP64 scan on the same workload "
+                        "(itself within |dchi2| <= 2e-5 of the oracle in tests/)")
     return out
 
 
@@ -438,6 +491,10 @@ def main():
     ap.add_argument("--zsub", type=int, default=None,
                     help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ygemm", default="fp64", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
+                    help="y = Tb^T W f in the FP64 scan (default) or as a tensor-core GEMM")
+    ap.add_argument("--ygemm-study", action="store_true",
+                    help="also time every y variant once and report its chi2/coeff error")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--graph", action="store_true",

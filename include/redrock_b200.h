@@ -35,6 +35,8 @@
  *   rr_zscan_pairs_grad     adjoint of the pair scan: dchi2/dz,
  *                           d2chi2/dz2, dchi2/dflux (Newton refinement in
  *                           place of fitz.py:255-261's parabola)
+ *   rr_pack_g, rr_ygemm     zscan.py:741-748 (y = Tb^T W f) for every
+ *                           (target, z) as one tensor-core GEMM per template
  */
 #ifndef REDROCK_B200_H
 #define REDROCK_B200_H
@@ -192,6 +194,9 @@ typedef struct {
   double* zchi2;        /* [nrows][nz] */
   double* zcoeff;       /* [nrows][nz][nbasis] */
   double* penalty;      /* [nrows][nz] (written only when oii != NULL) */
+  const double* y_ext;  /* NULL: y = Tb^T W f is summed in the scan itself;
+                           else [nblock * 32][nz][nbasis] from rr_ygemm
+                           (row = block * 32 + lane) */
 } rr_scan_template;
 
 typedef struct {
@@ -329,6 +334,45 @@ int rr_zchi2_batch_plain_noalloc(const double* band, const double* w, const doub
 /* penalty[z] = max(0, -sum_b coeff[z][b] oii[b])  (zscan.py:783-800) */
 int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const double* oii,
                       double* penalty, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Tensor-core y (zscan.py:741-748, y = Tb^T W f) for the fused scan.
+ * y_i(t, z) = sum_q G[q][t] T_z[q][i] with G[., t] = R^T W f of target t
+ * (independent of z), so y of a whole template is one GEMM
+ * (targets x pixels) . (pixels x (z, basis)) run on tcgen05:
+ *   RR_YGEMM_BF16X3  three bf16 slices, six products, FP32 accumulation
+ *   RR_YGEMM_TF32X3  two tf32 slices, three products, FP32 accumulation
+ *   RR_YGEMM_INT8X7  Ozaki scheme: power-of-two scaled, seven 7-bit integer
+ *                    slices, 28 products accumulated exactly in int32,
+ *                    combined in FP64 (needs row_exp and col_exp)
+ * Flow: rr_pack_targets -> rr_pack_g (G, row_exp) -> per template
+ * [rr_basis_col_exp] + rr_ygemm (Y) -> rr_zscan_fused with y_ext = Y.
+ * ---------------------------------------------------------------------- */
+enum rr_ygemm_variant {
+  RR_YGEMM_NONE = 0,   /* y summed in FP64 inside the scan (default) */
+  RR_YGEMM_BF16X3 = 1,
+  RR_YGEMM_TF32X3 = 2,
+  RR_YGEMM_INT8X7 = 3
+};
+
+/* padded pixel count (rows of G) for a basis of pix_stride rows */
+int64_t rr_ygemm_kpad(int64_t pix_stride);
+
+/* G[kpad][npos] (row q = padded basis pixel, column = block * 32 + lane)
+ * and row_exp[npos] (biased power-of-two exponents of each column's max,
+ * or NULL).  npos: a multiple of 128, >= nblock * 32.  The call zeroes G
+ * and row_exp first. */
+int rr_pack_g(const rr_scan_targets* targets, int64_t pix_stride, int64_t kpad, int64_t npos,
+              double* g, int* row_exp, int* status, rr_stream_t stream);
+
+/* col_exp[nz * nbasis]: biased exponent of max_q |basis[z][q][i]| */
+int rr_basis_col_exp(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
+                     int basis_stride, int* col_exp, rr_stream_t stream);
+
+/* y[npos][nz][nbasis] = G^T . basis for one template (rr_ygemm_variant) */
+int rr_ygemm(int variant, const double* g, const int* row_exp, int64_t npos, int64_t kpad,
+             const double* basis, int64_t nz, int64_t pix_stride, int nbasis, int basis_stride,
+             const int* col_exp, double* y, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * FMA throughput probe (no counterpart in redrock): the roofline

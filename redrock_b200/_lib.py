@@ -16,6 +16,9 @@ LIBPATH = os.path.join(HERE, "librr_b200.so")
 RR_OK, RR_EINVAL, RR_ERANGE, RR_ECUDA, RR_ETIMEOUT, RR_ENOTSUP, RR_ESCRATCH = range(7)
 RR_IGM_NONE, RR_IGM_CALURA12, RR_IGM_KAMBLE20, RR_IGM_INOUE14 = range(4)
 RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED = 0, 1
+RR_YGEMM_NONE, RR_YGEMM_BF16X3, RR_YGEMM_TF32X3, RR_YGEMM_INT8X7 = range(4)
+YGEMM_VARIANTS = {"fp64": RR_YGEMM_NONE, "bf16x3": RR_YGEMM_BF16X3, "tf32x3": RR_YGEMM_TF32X3,
+                  "int8x7": RR_YGEMM_INT8X7}
 HALF_BAND = 5
 LANES = 32
 RW = 12
@@ -54,7 +57,7 @@ class ScanTemplate(ctypes.Structure):
     _fields_ = [("basis", c_void_p), ("pix_stride", c_int64), ("nz", c_int32),
                 ("nbasis", c_int32), ("basis_stride", c_int32), ("method", c_int32),
                 ("prior", c_void_p), ("oii", c_void_p), ("zchi2", c_void_p),
-                ("zcoeff", c_void_p), ("penalty", c_void_p)]
+                ("zcoeff", c_void_p), ("penalty", c_void_p), ("y_ext", c_void_p)]
 
 
 class ScanTargets(ctypes.Structure):
@@ -123,6 +126,12 @@ _SIGNATURES = {
                                              c_void_p, c_void_p]),
     "rr_negoii_penalty": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
     "rr_fma_peak": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p]),
+    "rr_ygemm_kpad": (c_int64, [c_int64]),
+    "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
+                          c_void_p, c_void_p, c_void_p]),
+    "rr_basis_col_exp": (c_int, [c_void_p, c_int64, c_int64, c_int, c_int, c_void_p, c_void_p]),
+    "rr_ygemm": (c_int, [c_int, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64,
+                         c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 

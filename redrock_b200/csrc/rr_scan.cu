@@ -157,7 +157,7 @@ __device__ __forceinline__ void write_eval(const rr_scan_template& tm, int64_t r
 // RESID = true:  accumulate the direct residual sum (g - Tb'.c)^2 into acc
 //                (only lanes with do_lane set do the arithmetic).
 // Returns false (uniformly across the CTA) if a copy wait timed out.
-template <int NB, bool RESID>
+template <int NB, bool RESID, bool EXTY>
 __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_template& tm, int block,
                                       int z0, int nzt, bool active, StageBufs& sb,
                                       Uses& uses, double (&m)[NB * (NB + 1) / 2],
@@ -216,7 +216,7 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
         }
 #pragma unroll
         for (int i = 0; i < kPix; ++i) {
-          const double gi = rws[((q + i) * RR_RW + kBand) * RR_LANES];
+          const double gi = (RESID || !EXTY) ? rws[((q + i) * RR_RW + kBand) * RR_LANES] : 0.0;
           if (RESID) {
             double mi = 0.0;
 #pragma unroll
@@ -224,8 +224,9 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
             const double res = gi - mi;
             acc = fma(res, res, acc);
           } else {
+            if (!EXTY)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) y[b] = fma(gi, tp[i][b], y[b]);
+              for (int b = 0; b < NB; ++b) y[b] = fma(gi, tp[i][b], y[b]);
 #pragma unroll
             for (int a = 0; a < NB; ++a)
 #pragma unroll
@@ -252,7 +253,8 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
   return true;
 }
 
-template <int NB>
+// EXTY: y comes from tm.y_ext (rr_ygemm) instead of the pixel sweep.
+template <int NB, bool EXTY>
 __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
                           StageBufs& sb, Uses& uses, bool& failed) {
   const int warp = threadIdx.x >> 5;
@@ -269,7 +271,7 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   for (int i = 0; i < NB; ++i) y[i] = 0.0;
   const bool inz = warp < nzt;
   const int32_t row = p.tg.rows[block * RR_LANES + lane];
-  if (!sweep<NB, false>(p, tm, block, z0, nzt, inz, sb, uses, m, y, c, acc)) {
+  if (!sweep<NB, false, EXTY>(p, tm, block, z0, nzt, inz, sb, uses, m, y, c, acc)) {
     failed = true;
     return;
   }
@@ -279,6 +281,11 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   if (valid) {
     const double fwf = p.tg.fwf[block * RR_LANES + lane];
     wsum = p.tg.wsum[block * RR_LANES + lane];
+    if (EXTY) {
+      const double* ye = tm.y_ext + ((int64_t)(block * RR_LANES + lane) * tm.nz + z0 + warp) * NB;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) y[b] = ye[b];
+    }
     const bool ok = solve_eval<NB>(tm.method, tm.prior, m, y, fwf, wsum, c, chi2, err);
     fix = ok && err > kChi2FixTol;
     write_eval<NB>(tm, row, z0 + warp, c, chi2, wsum);
@@ -289,7 +296,7 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   if (__syncthreads_or(fix)) {
     if (threadIdx.x == 0 && p.resweep_counter) atomicAdd(p.resweep_counter, 1);
     acc = 0.0;
-    if (!sweep<NB, true>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
+    if (!sweep<NB, true, EXTY>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
       failed = true;
       return;
     }
@@ -304,7 +311,9 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
 // allocator spill on every path).
 __host__ __device__ constexpr bool in_common_set(int nb) { return nb == 4 || nb == 5 || nb == 10; }
 
-template <bool COMMON>
+// EXTY: every template of the launch has y_ext set (rr_ygemm), and the
+// pixel sweep skips y.
+template <bool COMMON, bool EXTY>
 __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ int64_t s_tile;
@@ -334,7 +343,7 @@ __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_k
 #define RR_TILE_CASE(N)                                                   \
   case N:                                                                 \
     if constexpr (in_common_set(N) == COMMON) {                           \
-      scan_tile<N>(p, tm, block, z0, sb, uses, failed);                   \
+      scan_tile<N, EXTY>(p, tm, block, z0, sb, uses, failed);             \
     } else {                                                              \
       set_status(p.status, RR_EINVAL);                                    \
       failed = true;                                                      \
@@ -638,7 +647,7 @@ static size_t fused_smem_bytes(int max_stride) {
 
 // Launch one instantiation of the fused kernel over the templates selected
 // by `pick` (indices into templates), using counter as its tile counter.
-template <bool COMMON>
+template <bool COMMON, bool EXTY>
 static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                         const int* pick, int npick, int* counter, int* resweep, int* status,
                         cudaStream_t stream) {
@@ -669,19 +678,19 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   const int64_t ntiles = p.tile_start[npick];
   if (ntiles == 0) return RR_OK;
   const size_t smem = fused_smem_bytes(max_stride);
-  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<COMMON>,
+  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<COMMON, EXTY>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 0;
   RR_CUDA_TRY(cudaGetDevice(&dev));
   RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
   int per_sm = 1;
-  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<COMMON>,
+  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<COMMON, EXTY>,
                                                             kThreads, smem));
   if (per_sm < 1) per_sm = 1;
   const int64_t slots = (int64_t)nsm * per_sm;
   const int64_t grid = ntiles < slots ? ntiles : slots;
-  zscan_fused_kernel<COMMON><<<(unsigned)grid, kThreads, smem, stream>>>(p);
+  zscan_fused_kernel<COMMON, EXTY><<<(unsigned)grid, kThreads, smem, stream>>>(p);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
@@ -703,8 +712,9 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     rw_end = sd.rw_offset + sd.npix_pad > rw_end ? sd.rw_offset + sd.npix_pad : rw_end;
   }
   if (rw_end > targets->npix_block) return RR_EINVAL;
-  int common[RR_MAX_TEMPLATES], other[RR_MAX_TEMPLATES];
-  int nc = 0, no = 0;
+  // launch groups: (common nbasis, y_ext) -> one persistent launch each
+  int group[4][RR_MAX_TEMPLATES];
+  int ng[4] = {0, 0, 0, 0};
   for (int t = 0; t < ntemplate; ++t) {
     const rr_scan_template& tm = templates[t];
     if (tm.nbasis < 1 || tm.nbasis > RR_MAX_NBASIS || tm.nz < 0) return RR_EINVAL;
@@ -715,21 +725,21 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     for (int s = 0; s < targets->nseg; ++s)
       if (targets->segs[s].basis_offset + targets->segs[s].npix_pad + kHalfBand > tm.pix_stride)
         return RR_EINVAL;
-    if (in_common_set(tm.nbasis)) common[nc++] = t; else other[no++] = t;
+    if (tm.y_ext && (reinterpret_cast<uintptr_t>(tm.y_ext) & 7) != 0) return RR_EINVAL;
+    const int gi = (in_common_set(tm.nbasis) ? 0 : 1) + (tm.y_ext ? 2 : 0);
+    group[gi][ng[gi]++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
   RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, sizeof(int), st));
-  if (nc) {
-    int rc = launch_fused<true>(targets, templates, common, nc, tile_counter, tile_counter + 2,
-                                status, st);
-    if (rc) return rc;
-  }
-  if (no) {
-    int rc = launch_fused<false>(targets, templates, other, no, tile_counter + 1,
-                                 tile_counter + 2, status, st);
-    if (rc) return rc;
-  }
-  return RR_OK;
+  // each launch resets its counter first (stream order), so common-set
+  // launches share tile_counter[0] and the others tile_counter[1]
+  int* resweep = tile_counter + 2;
+  int rc = RR_OK;
+  if (!rc && ng[0]) rc = launch_fused<true, false>(targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
+  if (!rc && ng[1]) rc = launch_fused<false, false>(targets, templates, group[1], ng[1], tile_counter + 1, resweep, status, st);
+  if (!rc && ng[2]) rc = launch_fused<true, true>(targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
+  if (!rc && ng[3]) rc = launch_fused<false, true>(targets, templates, group[3], ng[3], tile_counter + 1, resweep, status, st);
+  return rc;
 }
 
 extern "C" int rr_pack_targets(const rr_spectrum_desc* specs, int64_t nspec,

@@ -80,7 +80,7 @@ __device__ __forceinline__ bool ldlt_solve(const double (&m)[NB * (NB + 1) / 2],
 // ulp; calibrated against redrock's direct residual), and the chi2 error
 // above which a (target, z) is re-evaluated by the direct residual.
 constexpr double kSumEps = 1e-14;
-constexpr double kChi2FixTol = 1e-6;
+constexpr double kChi2FixTol = 1e-5;
 
 // Solve and chi2 for one (target, z) from its normal equations.
 // chi2 = f^T W f - c^T y - c^T P c.  Also returns an upper estimate of that

@@ -1,0 +1,602 @@
+// Tensor-core form of the y = Tb^T W f term of the redshift scan.
+//
+// With rw[p][k] = sqrt(w_p) R[p, p+k-5] and g_p = sqrt(w_p) f_p (the packed
+// rows of rr_pack_targets), redrock's y (zscan.py:741-748, Tb^T (w f)) is
+//   y_i(t, z) = sum_p g_p sum_k rw[p][k] T_z[p+k-5][i] = sum_q G[q][t] T_z[q][i]
+// with G[., t] = R^T W f of target t, which does not depend on z.  So y for
+// every (target, z, basis) of a template is one GEMM:
+//   Y[t][(z, i)] = sum_q G[q][t] T[z][q][i]   (M = targets, N = (z, i),
+//                                              K = padded basis pixel index).
+// rr_pack_g builds G (and, for the integer variant, a power-of-two scale per
+// target); rr_ygemm runs the GEMM on the tcgen05 tensor cores; the fused scan
+// then reads Y instead of accumulating y itself (rr_scan_template.y_ext).
+//
+// Operands are FP64 in HBM.  Each CTA stages a 128-target x 32/64-pixel tile
+// of G and an N x 32/64-pixel tile of the basis into shared memory, splitting
+// every value into slices on the way (the canonical K-major, no-swizzle UMMA
+// layout: 8-row x 16-byte core matrices), and one thread issues the slice
+// products as tcgen05.mma into TMEM accumulators.  Two stages alternate; a
+// stage is refilled once the tcgen05.commit of its previous MMAs arrives on
+// its mbarrier.  Variants (rr_ygemm_variant):
+//   BF16X3  three bf16 slices per value (hi + mid + lo), the six products of
+//           slice order <= 2, one FP32 accumulator (kind::f16).
+//   TF32X3  two tf32 slices, hi*hi + hi*lo + lo*hi, FP32 (kind::tf32).
+//   INT8X7  Ozaki scheme: G rows and basis columns scaled by powers of two,
+//           split into seven 7-bit signed integer slices; the 28 products of
+//           slices (i, j) with i + j <= 6 accumulate EXACTLY in int32
+//           accumulator i + j (kind::i8), and the seven accumulators are
+//           combined in FP64.  Error ~ 2^-49 of max|G| max|T| per term.
+#include <cuda_bf16.h>
+#include <climits>
+#include <cmath>
+
+#include "rr_common.cuh"
+
+namespace rr {
+namespace yg {
+
+constexpr int kTileM = 128;  // targets per tile (MMA M)
+constexpr int kThreads = 256;
+constexpr int kStages = 2;
+constexpr int kKpadAlign = 64;  // G rows padded to a multiple of the largest stage depth
+constexpr int kExpBias = 4096;  // stored exponents are biased; 0 = all-zero row/column
+
+template <int V>
+struct Var;
+template <>
+struct Var<RR_YGEMM_BF16X3> {
+  static constexpr int kEsz = 2, kSlices = 3, kKInst = 16, kNAcc = 1, kNMax = 256, kKt = 32;
+  static constexpr uint32_t kFmt = (1u << 4) | (1u << 7) | (1u << 10);  // D f32, A/B bf16
+};
+template <>
+struct Var<RR_YGEMM_TF32X3> {
+  static constexpr int kEsz = 4, kSlices = 2, kKInst = 8, kNAcc = 1, kNMax = 256, kKt = 32;
+  static constexpr uint32_t kFmt = (1u << 4) | (2u << 7) | (2u << 10);  // D f32, A/B tf32
+};
+template <>
+struct Var<RR_YGEMM_INT8X7> {
+  static constexpr int kEsz = 1, kSlices = 7, kKInst = 32, kNAcc = 7, kNMax = 64, kKt = 64;
+  static constexpr uint32_t kFmt = (2u << 4) | (1u << 7) | (1u << 10);  // D s32, A/B s8
+};
+
+template <int V>
+struct Geo {
+  using P = Var<V>;
+  static constexpr int kE = 16 / P::kEsz;          // elements per 16-byte core-matrix row
+  static constexpr int kNkg = P::kKt / kE;         // core matrices along K per stage
+  static constexpr int kSteps = P::kKt / P::kKInst;  // MMA instructions along K per stage
+  static constexpr int kSbo = kNkg * 128;          // bytes between 8-row groups
+  static constexpr int kASlice = kTileM * P::kKt * P::kEsz;
+  static constexpr int kTmemCols = P::kNAcc * P::kNMax <= 256 ? 256 : 512;
+  static __host__ __device__ constexpr int b_slice(int n) { return n * P::kKt * P::kEsz; }
+  static __host__ __device__ constexpr int stage_bytes(int n) {
+    return P::kSlices * (kASlice + b_slice(n));
+  }
+};
+
+struct YParams {
+  const double* g;      // [kpad][npos]
+  const int* row_exp;   // [npos] biased exponents (INT8X7)
+  const double* basis;  // [nz][pix_stride][basis_stride]
+  const int* col_exp;   // [nz * nbasis] biased exponents (INT8X7)
+  double* y;            // [npos][nz][nbasis]
+  int64_t npos, kpad, pix_stride;
+  int nz, nbasis, basis_stride;
+  int zt;    // redshifts per tile
+  int n;     // MMA N (zt * nbasis rounded up to 16)
+  int* status;
+};
+
+// ---------------------------------------------------------------------------
+// tcgen05 / descriptor helpers
+// ---------------------------------------------------------------------------
+// Shared-memory matrix descriptor: K-major, no swizzle; LBO = 128 B between
+// the two core matrices along K of one instruction, SBO between 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
+  return d;                // base offset 0, layout type 0 = SWIZZLE_NONE
+}
+
+template <int V>
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                    uint32_t accumulate) {
+  if constexpr (V == RR_YGEMM_BF16X3) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+  } else if constexpr (V == RR_YGEMM_TF32X3) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+  }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// 8 consecutive 32-bit TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// slicing: one 16-byte core-matrix row (kE consecutive K elements) per call
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t bf16_bits(double x, double& rest) {
+  const __nv_bfloat16 h = __double2bfloat16(x);
+  rest = x - (double)__bfloat162float(h);
+  return (uint32_t)__bfloat16_as_ushort(h);
+}
+__device__ __forceinline__ uint32_t tf32_bits(double x, double& rest) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(__double2float_rn(x)));
+  rest = x - (double)__uint_as_float(r);
+  return r;
+}
+
+// Write the slices of v[0..kE) (scaled by 2^-exp for INT8X7) to
+// dst + s * slice_bytes, s = 0..kSlices-1.
+template <int V>
+__device__ __forceinline__ void store_slices(const double (&v)[Geo<V>::kE], int exp,
+                                             unsigned char* dst, int slice_bytes) {
+  constexpr int kE = Geo<V>::kE;
+  if constexpr (V == RR_YGEMM_BF16X3) {
+    uint32_t w[3][4];
+#pragma unroll
+    for (int j = 0; j < kE; j += 2) {
+      double r0 = v[j], r1 = v[j + 1];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const uint32_t lo = bf16_bits(r0, r0);
+        const uint32_t hi = bf16_bits(r1, r1);
+        w[s][j / 2] = lo | (hi << 16);
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 3; ++s)
+      *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+  } else if constexpr (V == RR_YGEMM_TF32X3) {
+    uint32_t w[2][4];
+#pragma unroll
+    for (int j = 0; j < kE; ++j) {
+      double r = v[j];
+      w[0][j] = tf32_bits(r, r);
+      w[1][j] = tf32_bits(r, r);
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+      *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+  } else {
+    // |v| 2^-exp <= 1: slice 0 = rint(2^6 x), then 7 more bits per slice;
+    // every step is exact in FP64
+    uint32_t w[7][4];
+#pragma unroll
+    for (int s = 0; s < 7; ++s)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[s][j] = 0;
+#pragma unroll
+    for (int j = 0; j < kE; ++j) {
+      double r = ldexp(v[j], 6 - exp);
+#pragma unroll
+      for (int s = 0; s < 7; ++s) {
+        const double a = rint(r);
+        r = (r - a) * 128.0;
+        w[s][j >> 2] |= ((uint32_t)(int)a & 0xFFu) << (8 * (j & 3));
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 7; ++s)
+      *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+  }
+}
+
+__device__ __forceinline__ int unbias(int e) { return e > 0 ? e - kExpBias : 0; }
+
+// Stage K-chunk c (pixels q0 .. q0 + kKt) of the tile into shared memory.
+// Unit u of a slice tile is the 16-byte core-matrix row at byte u * 16:
+// row r = (u & 7) + 8 * (u / (8 kNkg)), K group kg = (u >> 3) % kNkg.
+template <int V>
+__device__ __forceinline__ void stage_tile(const YParams& p, unsigned char* st, int64_t t0, int z0,
+                                           int nzt, int64_t q0, const int* s_rexp,
+                                           const int* s_cexp) {
+  using G = Geo<V>;
+  using P = Var<V>;
+  constexpr int kE = G::kE;
+  // A: G[q][t0 + r]
+  for (int u = threadIdx.x; u < kTileM * G::kNkg; u += kThreads) {
+    const int r = (u & 7) + 8 * (u / (8 * G::kNkg));
+    const int kg = (u >> 3) % G::kNkg;
+    const double* src = p.g + (q0 + kg * kE) * p.npos + t0 + r;
+    double v[kE];
+#pragma unroll
+    for (int j = 0; j < kE; ++j) v[j] = __ldg(src + (int64_t)j * p.npos);
+    store_slices<V>(v, V == RR_YGEMM_INT8X7 ? s_rexp[r] : 0, st + u * 16, G::kASlice);
+  }
+  // B: row n = (zl, i) of the basis, T[z0 + zl][q][i]
+  unsigned char* sb = st + P::kSlices * G::kASlice;
+  const int nused = nzt * p.nbasis;
+  for (int u = threadIdx.x; u < p.n * G::kNkg; u += kThreads) {
+    const int r = (u & 7) + 8 * (u / (8 * G::kNkg));
+    const int kg = (u >> 3) % G::kNkg;
+    double v[kE];
+    int e = 0;
+    if (r < nused) {
+      const int zl = r / p.nbasis;
+      const int i = r - zl * p.nbasis;
+      const int64_t q = q0 + kg * kE;
+      const double* src = p.basis + ((int64_t)(z0 + zl) * p.pix_stride + q) * p.basis_stride + i;
+#pragma unroll
+      for (int j = 0; j < kE; ++j)
+        v[j] = (q + j < p.pix_stride) ? __ldg(src + (int64_t)j * p.basis_stride) : 0.0;
+      if (V == RR_YGEMM_INT8X7) e = s_cexp[r];
+    } else {
+#pragma unroll
+      for (int j = 0; j < kE; ++j) v[j] = 0.0;
+    }
+    store_slices<V>(v, e, sb + u * 16, G::b_slice(p.n));
+  }
+}
+
+template <int V>
+__global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constant__ YParams p) {
+  using G = Geo<V>;
+  using P = Var<V>;
+  extern __shared__ __align__(1024) unsigned char ysm[];
+  __shared__ __align__(8) uint64_t done[kStages];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_rexp[kTileM];
+  __shared__ int s_cexp[Var<V>::kNMax];
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t t0 = (int64_t)blockIdx.x * kTileM;
+  const int z0 = blockIdx.y * p.zt;
+  const int nzt = min(p.zt, p.nz - z0);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"((uint32_t)G::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&done[s], 1);
+    fence_mbar_init();
+  }
+  if (V == RR_YGEMM_INT8X7) {
+    for (int r = threadIdx.x; r < kTileM; r += kThreads) s_rexp[r] = unbias(p.row_exp[t0 + r]);
+    for (int r = threadIdx.x; r < p.n; r += kThreads) {
+      const int zl = r / p.nbasis;
+      s_cexp[r] = (zl < nzt) ? unbias(p.col_exp[(int64_t)(z0 + zl) * p.nbasis + r - zl * p.nbasis])
+                             : 0;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  const uint32_t idesc = P::kFmt | ((uint32_t)(p.n >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+  const int stage_bytes = G::stage_bytes(p.n);
+  const int64_t nchunk = p.kpad / P::kKt;
+  bool ok = true;
+  for (int64_t c = 0; c < nchunk; ++c) {
+    const int s = (int)(c & 1);
+    unsigned char* st = ysm + s * stage_bytes;
+    // the MMAs of chunk c - 2 read this stage: wait for their commit
+    if (c >= 2) {
+      const bool w = mbar_wait(&done[s], (uint32_t)(((c >> 1) - 1) & 1), p.status);
+      if (__syncthreads_or(!w)) {
+        ok = false;
+        break;
+      }
+    }
+    stage_tile<V>(p, st, t0, z0, nzt, c * P::kKt, s_rexp, s_cexp);
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(st);
+      const uint32_t b0 = a0 + P::kSlices * G::kASlice;
+#pragma unroll 1
+      for (int ks = 0; ks < G::kSteps; ++ks) {
+        const uint32_t koff = ks * 256;
+        if constexpr (V == RR_YGEMM_INT8X7) {
+          // products (i, j), i + j = d <= 6, into accumulator d
+#pragma unroll 1
+          for (int d = 0; d < 7; ++d)
+#pragma unroll 1
+            for (int i = 0; i <= d; ++i) {
+              const uint64_t da = smem_desc(a0 + i * G::kASlice + koff, G::kSbo);
+              const uint64_t db = smem_desc(b0 + (d - i) * G::b_slice(p.n) + koff, G::kSbo);
+              const uint32_t acc = (c > 0 || ks > 0 || i > 0) ? 1u : 0u;
+              mma<V>(tmem + d * P::kNMax, da, db, idesc, acc);
+            }
+        } else {
+          // all slice products of order <= kSlices - 1, smallest first
+#pragma unroll 1
+          for (int d = P::kSlices - 1; d >= 0; --d)
+#pragma unroll 1
+            for (int i = 0; i <= d; ++i) {
+              const uint64_t da = smem_desc(a0 + i * G::kASlice + koff, G::kSbo);
+              const uint64_t db = smem_desc(b0 + (d - i) * G::b_slice(p.n) + koff, G::kSbo);
+              const uint32_t acc = (c > 0 || ks > 0 || d != P::kSlices - 1 || i > 0) ? 1u : 0u;
+              mma<V>(tmem, da, db, idesc, acc);
+            }
+        }
+      }
+      mma_commit(&done[s]);
+    }
+  }
+  // all MMAs done: the last commit covers every earlier one
+  if (ok && nchunk > 0) {
+    const int64_t last = nchunk - 1;
+    ok = mbar_wait(&done[last & 1], (uint32_t)((last >> 1) & 1), p.status);
+  }
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    tc_fence_after();
+    const int lg = warp & 3;           // TMEM lanes 32 lg .. 32 lg + 31
+    const int half = warp >> 2;        // column half
+    const int64_t pos = t0 + 32 * lg + lane;
+    const int ncol = p.n / 2;
+    const int nused = nzt * p.nbasis;
+    double* yrow = p.y + (pos * p.nz + z0) * p.nbasis;
+    const bool row_ok = pos < p.npos;
+    const uint32_t tl = tmem + ((uint32_t)(32 * lg) << 16);
+    for (int c0 = half * ncol; c0 < (half + 1) * ncol; c0 += 8) {
+      double out[8];
+      if constexpr (V == RR_YGEMM_INT8X7) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[j] = 0.0;
+        // smallest terms first
+#pragma unroll 1
+        for (int d = 6; d >= 0; --d) {
+          uint32_t v[8];
+          tmem_ld8(tl + d * P::kNMax + c0, v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 8; ++j) out[j] += ldexp((double)(int)v[j], -12 - 7 * d);
+        }
+        const int re = s_rexp[32 * lg + lane];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[j] = ldexp(out[j], re + s_cexp[c0 + j]);
+      } else {
+        uint32_t v[8];
+        tmem_ld8(tl + c0, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[j] = (double)__uint_as_float(v[j]);
+      }
+      if (row_ok)
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (c0 + j < nused) yrow[c0 + j] = out[j];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"((uint32_t)G::kTmemCols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// G = R^T W f per target, pixel-major, and the per-target exponent
+// ---------------------------------------------------------------------------
+struct GParams {
+  const double* rw;
+  int64_t npix_block;
+  rr_segment_desc segs[16];
+  int nseg;
+  int64_t pix_stride, kpad, npos;
+  double* g;
+  int* row_exp;
+};
+
+// block (32 lanes, 8 pixels); grid (kpad / 8, nblock)
+__global__ void __launch_bounds__(256) pack_g_kernel(const __grid_constant__ GParams p) {
+  __shared__ int s_e[8][32];
+  const int lane = threadIdx.x;
+  const int64_t q = (int64_t)blockIdx.x * 8 + threadIdx.y;
+  const int64_t b = blockIdx.y;
+  double acc = 0.0;
+  if (q < p.pix_stride) {
+    for (int s = 0; s < p.nseg; ++s) {
+      const rr_segment_desc& sd = p.segs[s];
+      const int64_t base = q - sd.basis_offset + kHalfBand;
+      for (int k = 0; k < kBand; ++k) {
+        const int64_t px = base - k;
+        if (px < 0 || px >= sd.npix_pad) continue;
+        const double* row = p.rw + ((b * p.npix_block + sd.rw_offset + px) * RR_RW) * RR_LANES + lane;
+        acc = fma(row[k * RR_LANES], row[kBand * RR_LANES], acc);
+      }
+    }
+  }
+  if (q < p.kpad) p.g[q * p.npos + b * RR_LANES + lane] = acc;
+  if (p.row_exp) {
+    int e = 0;
+    if (acc != 0.0) {
+      frexp(acc, &e);
+      e += kExpBias;
+    }
+    s_e[threadIdx.y][lane] = e;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+      int m = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) m = max(m, s_e[j][lane]);
+      if (m > 0) atomicMax(p.row_exp + b * RR_LANES + lane, m);
+    }
+  }
+}
+
+// biased exponent of max_q |T[z][q][i]| per (z, i); one block per z
+__global__ void __launch_bounds__(256) col_exp_kernel(const double* __restrict__ basis,
+                                                      int64_t pix_stride, int nbasis,
+                                                      int basis_stride, int* col_exp) {
+  __shared__ double s_m[256];
+  const int64_t z = blockIdx.x;
+  const double* tz = basis + z * pix_stride * basis_stride;
+  for (int i = 0; i < nbasis; ++i) {
+    double m = 0.0;
+    for (int64_t q = threadIdx.x; q < pix_stride; q += blockDim.x)
+      m = fmax(m, fabs(tz[q * basis_stride + i]));
+    s_m[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) s_m[threadIdx.x] = fmax(s_m[threadIdx.x], s_m[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      int e = 0;
+      if (s_m[0] > 0.0) {
+        frexp(s_m[0], &e);
+        e += kExpBias;
+      }
+      col_exp[z * nbasis + i] = e;
+    }
+    __syncthreads();
+  }
+}
+
+template <int V>
+static int launch_ygemm(YParams p, cudaStream_t stream) {
+  using P = Var<V>;
+  if (p.kpad % P::kKt) return RR_EINVAL;
+  if (V == RR_YGEMM_INT8X7 && (!p.row_exp || !p.col_exp)) return RR_EINVAL;
+  // exact int32 accumulation: |slice| <= 64, at most 7 products per
+  // accumulator and pixel
+  if (V == RR_YGEMM_INT8X7 && p.kpad > 65536) return RR_ENOTSUP;
+  int zt = P::kNMax / p.nbasis;
+  if (zt > p.nz) zt = p.nz;
+  p.zt = zt;
+  p.n = ((zt * p.nbasis + 15) / 16) * 16;
+  if (p.n > P::kNMax) return RR_EINVAL;
+  const size_t smem = (size_t)kStages * Geo<V>::stage_bytes(p.n);
+  RR_CUDA_TRY(cudaFuncSetAttribute(ygemm_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  dim3 grid((unsigned)(p.npos / kTileM), (unsigned)((p.nz + zt - 1) / zt));
+  ygemm_kernel<V><<<grid, kThreads, smem, stream>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+}  // namespace yg
+}  // namespace rr
+
+using namespace rr;
+
+extern "C" int64_t rr_ygemm_kpad(int64_t pix_stride) {
+  return ((pix_stride + yg::kKpadAlign - 1) / yg::kKpadAlign) * yg::kKpadAlign;
+}
+
+extern "C" int rr_pack_g(const rr_scan_targets* targets, int64_t pix_stride, int64_t kpad,
+                         int64_t npos, double* g, int* row_exp, int* status,
+                         rr_stream_t stream) {
+  (void)status;
+  if (!targets || !g || pix_stride < 1 || kpad < pix_stride || kpad % yg::kKpadAlign) return RR_EINVAL;
+  if (targets->nseg < 1 || targets->nseg > 16 || !targets->segs) return RR_EINVAL;
+  if (npos % yg::kTileM || npos < (int64_t)targets->nblock * RR_LANES) return RR_EINVAL;
+  yg::GParams p;
+  p.rw = targets->rw;
+  p.npix_block = targets->npix_block;
+  p.nseg = targets->nseg;
+  if (!targets->rw || targets->nblock < 0) return RR_EINVAL;
+  for (int s = 0; s < p.nseg; ++s) {
+    p.segs[s] = targets->segs[s];
+    const rr_segment_desc& sd = p.segs[s];
+    if (sd.npix_pad < 0 || sd.rw_offset < 0 || sd.rw_offset + sd.npix_pad > p.npix_block ||
+        sd.basis_offset < kHalfBand || sd.basis_offset + sd.npix_pad + kHalfBand > pix_stride)
+      return RR_EINVAL;
+  }
+  p.pix_stride = pix_stride;
+  p.kpad = kpad;
+  p.npos = npos;
+  p.g = g;
+  p.row_exp = row_exp;
+  cudaStream_t st = (cudaStream_t)stream;
+  // positions past the last block stay zero
+  RR_CUDA_TRY(cudaMemsetAsync(g, 0, (size_t)kpad * npos * sizeof(double), st));
+  if (row_exp) RR_CUDA_TRY(cudaMemsetAsync(row_exp, 0, (size_t)npos * sizeof(int), st));
+  if (targets->nblock < 1) return RR_OK;
+  dim3 grid((unsigned)(kpad / 8), (unsigned)targets->nblock);
+  yg::pack_g_kernel<<<grid, dim3(32, 8), 0, st>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_basis_col_exp(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
+                                int basis_stride, int* col_exp, rr_stream_t stream) {
+  if (!basis || !col_exp || nz < 0 || pix_stride < 1 || nbasis < 1 || basis_stride < nbasis)
+    return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  yg::col_exp_kernel<<<(unsigned)nz, 256, 0, (cudaStream_t)stream>>>(basis, pix_stride, nbasis,
+                                                                      basis_stride, col_exp);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_ygemm(int variant, const double* g, const int* row_exp, int64_t npos,
+                        int64_t kpad, const double* basis, int64_t nz, int64_t pix_stride,
+                        int nbasis, int basis_stride, const int* col_exp, double* y, int* status,
+                        rr_stream_t stream) {
+  if (!g || !basis || !y || npos < yg::kTileM || npos % yg::kTileM) return RR_EINVAL;
+  if (nz < 0 || nz > INT_MAX || nbasis < 1 || nbasis > RR_MAX_NBASIS || basis_stride < nbasis)
+    return RR_EINVAL;
+  if (kpad < pix_stride || kpad % yg::kKpadAlign || pix_stride < 1) return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  yg::YParams p;
+  p.g = g;
+  p.row_exp = row_exp;
+  p.basis = basis;
+  p.col_exp = col_exp;
+  p.y = y;
+  p.npos = npos;
+  p.kpad = kpad;
+  p.pix_stride = pix_stride;
+  p.nz = (int)nz;
+  p.nbasis = nbasis;
+  p.basis_stride = basis_stride;
+  p.status = status;
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (variant) {
+    case RR_YGEMM_BF16X3: return yg::launch_ygemm<RR_YGEMM_BF16X3>(p, st);
+    case RR_YGEMM_TF32X3: return yg::launch_ygemm<RR_YGEMM_TF32X3>(p, st);
+    case RR_YGEMM_INT8X7: return yg::launch_ygemm<RR_YGEMM_INT8X7>(p, st);
+    default: return RR_EINVAL;
+  }
+}

@@ -201,6 +201,19 @@ class DeviceBasis:
         z = np.zeros(nz) if redshifts is None else redshifts
         return cls(basis, layout, nb, z, **kw)
 
+    def col_exp(self, stream=None):
+        """Power-of-two exponents of each (z, basis) column's max |value|
+        (the integer tensor-core y variant's column scales), cached."""
+        if getattr(self, "_col_exp", None) is None:
+            L = _lib.lib()
+            ce = torch.empty(max(self.nz * self.nbasis, 1), dtype=torch.int32,
+                             device=self.basis.device)
+            rc = L.rr_basis_col_exp(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
+                                    self.stride, ptr(ce), stream_handle(stream))
+            _lib.check(rc, "rr_basis_col_exp")
+            self._col_exp = ce
+        return self._col_exp
+
     def data_dict(self, as_numpy=True):
         """redrock's DistTemplate.local.data view: dict[wavehash] -> (nz, npix, nb)."""
         out = {}
@@ -382,14 +395,52 @@ class ScanResult:
         self.penalty = torch.zeros((ntarget, basis.nz), dtype=torch.float64, device=dev)
 
 
-def run_fused(pack, bases, stream=None, status=None):
-    """One persistent launch over every (target, template, z)."""
+class YGemm:
+    """y = Tb^T W f of every (target, z) on the tensor cores: G = R^T W f of
+    a target pack (rr_pack_g) and, per template, Y = G^T . basis
+    (rr_ygemm).  variant: "bf16x3", "tf32x3" or "int8x7"."""
+
+    def __init__(self, pack, variant, stream=None, status=None):
+        L = _lib.lib()
+        dev = device()
+        if variant not in _lib.YGEMM_VARIANTS or variant == "fp64":
+            raise ValueError(f"unknown tensor-core y variant {variant!r}")
+        self.variant = _lib.YGEMM_VARIANTS[variant]
+        self.layout = pack.layout
+        self.npos = round_up(pack.nblock * _lib.LANES, 128)
+        self.kpad = int(L.rr_ygemm_kpad(pack.layout.pix_stride))
+        self.g = torch.empty((self.kpad, self.npos), dtype=torch.float64, device=dev)
+        self.row_exp = (torch.empty(self.npos, dtype=torch.int32, device=dev)
+                        if self.variant == _lib.RR_YGEMM_INT8X7 else None)
+        self._status = status or StatusWord(dev)
+        tgs = pack.scan_targets_struct()
+        rc = L.rr_pack_g(ctypes.byref(tgs), pack.layout.pix_stride, self.kpad, self.npos,
+                         ptr(self.g), ptr(self.row_exp), self._status.ptr, stream_handle(stream))
+        _lib.check(rc, "rr_pack_g")
+
+    def y(self, basis, stream=None):
+        """[npos][nz][nbasis] y of every packed target against one basis."""
+        L = _lib.lib()
+        y = torch.empty((self.npos, basis.nz, basis.nbasis), dtype=torch.float64,
+                        device=self.g.device)
+        col = basis.col_exp(stream) if self.variant == _lib.RR_YGEMM_INT8X7 else None
+        rc = L.rr_ygemm(self.variant, ptr(self.g), ptr(self.row_exp), self.npos, self.kpad,
+                        ptr(basis.basis), basis.nz, basis.layout.pix_stride, basis.nbasis,
+                        basis.stride, ptr(col), ptr(y), self._status.ptr, stream_handle(stream))
+        _lib.check(rc, "rr_ygemm")
+        return y
+
+
+def run_fused(pack, bases, stream=None, status=None, ygemm="fp64"):
+    """One persistent launch over every (target, template, z).  ygemm other
+    than "fp64" computes y on the tensor cores first (YGemm)."""
     L = _lib.lib()
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
     tgs = pack.scan_targets_struct()
     counter = torch.zeros(3, dtype=torch.int32, device=dev)
     st = status or StatusWord(dev)
+    yg = None if ygemm == "fp64" else YGemm(pack, ygemm, stream=stream, status=st)
     for i0 in range(0, len(bases), _lib.MAX_TEMPLATES):
         chunk = list(range(i0, min(len(bases), i0 + _lib.MAX_TEMPLATES)))
         tms = []
@@ -397,10 +448,14 @@ def run_fused(pack, bases, stream=None, status=None):
             b, r = bases[i], results[i]
             if b.layout.signature != pack.layout.signature:
                 raise ValueError("template basis and targets use different wavelength grids")
+            if yg is not None:
+                # kept with the result so it outlives the launch
+                r.y_ext = yg.y(b, stream=stream)
             tms.append(_lib.ScanTemplate(ptr(b.basis), b.layout.pix_stride, b.nz, b.nbasis,
                                          b.stride, b.method, ptr(b.prior), ptr(b.oii),
                                          ptr(r.zchi2), ptr(r.zcoeff),
-                                         ptr(r.penalty) if b.oii is not None else None))
+                                         ptr(r.penalty) if b.oii is not None else None,
+                                         ptr(r.y_ext) if yg is not None else None))
         arr = (_lib.ScanTemplate * len(tms))(*tms)
         rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
                               stream_handle(stream))

@@ -6,7 +6,7 @@ Tolerances (FP64 everywhere on the GPU):
   * IGM transmission: relative 1e-13 (CUDA pow/exp vs libm, <= 2 ulp each);
   * chi2: |dchi2| <= 1e-3 absolute (the acceptance bar) and also 2e-5
     absolute, the fused kernel's own error budget (normal-equation chi2 is
-    kept only when its rounding-error bound is below 1e-6, else the direct
+    kept only when its rounding-error bound is below 1e-5, else the direct
     residual is summed); identical argmin per target;
   * coefficients: |dc| <= 1e-5 * max|c| per (target, z).
 """
