@@ -134,15 +134,18 @@ def make_workload(ntarget, seed, zsub=None, workload="desi500"):
 
 
 def evals_and_flops(rtg, tms):
+    """(evals, algorithmic FLOPs F(n, P) summed, the y part 2 P n of them)"""
     ev = 0
     fl = 0.0
+    yfl = 0.0
     for t in rtg:
         npix = sum(len(s.wave) for s in t.spectra)
         for tm in tms:
             nz = len(tm.redshifts)
             ev += nz
             fl += nz * flops_per_eval(tm.nbasis, npix)
-    return ev, fl
+            yfl += nz * 2.0 * npix * tm.nbasis
+    return ev, fl, yfl
 
 
 def measure_fp64_peak(L, torch):
@@ -194,12 +197,14 @@ def run_ours(args, rank, world, local_rank):
     L = _lib.lib()
     tg, rtg, tset, tms = make_workload(args.ntargets, seed=args.seed + 7919 * rank,
                                        zsub=args.zsub, workload=args.workload)
-    evals, flops = evals_and_flops(rtg, tms)
+    evals, flops, y_flops = evals_and_flops(rtg, tms)
     layout = GridLayout.from_dwave(synth.camera_grids())
     srcs = [TemplateSource.from_template(tm) for tm in tms]
     dbatch = TargetBatch(rtg, layout).to_device()
     st = StatusWord()
     ev_fused = []
+
+    ev_kernel = []
 
     def step(record, ygemm=args.ygemm, sink=ev_fused):
         bases = [DeviceBasis.build(s, layout, status=st) for s in srcs]
@@ -208,7 +213,8 @@ def run_ours(args, rank, world, local_rank):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        res, _ = run_fused(pack, bases, status=st, ygemm=ygemm)
+        res, _ = run_fused(pack, bases, status=st, ygemm=ygemm,
+                           kernel_events=ev_kernel if (record and sink is ev_fused) else None)
         if record:
             e1.record()
             sink.append((e0, e1))
@@ -228,11 +234,15 @@ def run_ours(args, rank, world, local_rank):
         graph.replay()
         torch.cuda.synchronize()
         st.check("graph replay")
-    # basis builds, target packing (2), the fused scan; with a tensor-core y:
-    # rr_pack_g, one rr_ygemm per template (+ column scales for int8x7)
+    # basis builds, target packing (2), the fused scan; with a tensor-core y
+    # also the G packing, slicing and one GEMM per template
     launches_per_step = sum(len(layout.keys) for _ in srcs) + 2 + 1
-    if args.ygemm != "fp64":
-        launches_per_step += 1 + len(srcs) * (2 if args.ygemm == "int8x7" else 1)
+    if args.ygemm == "int8x7":
+        # rr_pack_g, rr_slice_g_i8; per template rr_basis_col_exp,
+        # rr_slice_basis_i8, rr_ygemm_i8
+        launches_per_step += 2 + 3 * len(srcs)
+    elif args.ygemm != "fp64":
+        launches_per_step += 1 + len(srcs)
 
     clocks = ClockSampler(torch.cuda.current_device())
     if world > 1:
@@ -254,12 +264,18 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     st.check("timed steps")
     ms = t0.elapsed_time(t1) / args.steps
-    resweeps = int(run_fused.last_counter[2].item()) if hasattr(run_fused, "last_counter") else None
+    resweeps = resweep_lanes = None
+    if hasattr(run_fused, "last_counter"):
+        resweeps = int(run_fused.last_counter[2].item())
+        resweep_lanes = int(run_fused.last_counter[3].item())
+    # scan stage (y GEMM + fused kernel) and the fused kernel alone
     fused_ms = float(np.mean([a.elapsed_time(b) for a, b in ev_fused])) if ev_fused else ms
+    kernel_ms = (float(np.mean([a.elapsed_time(b) for a, b in ev_kernel])) * len(ev_kernel)
+                 / max(len(ev_fused), 1)) if ev_kernel else fused_ms
     if world > 1:
-        v = torch.tensor([ms, fused_ms], dtype=torch.float64, device="cuda")
+        v = torch.tensor([ms, fused_ms, kernel_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(v, op=dist.ReduceOp.MAX)
-        ms, fused_ms = float(v[0]), float(v[1])
+        ms, fused_ms, kernel_ms = float(v[0]), float(v[1]), float(v[2])
     value = world * evals / (ms / 1e3)
 
     study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
@@ -331,8 +347,11 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return None
     peak = measure_fp64_peak(L, torch)
-    fused_flops = flops
-    achieved = fused_flops / (fused_ms / 1e3) / 1e12
+    # FP64 work of the fused kernel: all of F(n, P), less y when the tensor
+    # cores compute it
+    y_on_tc = args.ygemm != "fp64"
+    fused_flops = flops - (y_flops if y_on_tc else 0.0)
+    achieved = fused_flops / (kernel_ms / 1e3) / 1e12
     out = {
         "metric": "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3",
         "value": value, "unit": "chi2 evals/s", "n_gpus": world, "steps": args.steps,
@@ -353,8 +372,13 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(),
                      "kernel": "zscan_fused_kernel",
-                     "kernel_ms": fused_ms, "flops_per_launch": fused_flops,
+                     "kernel_ms": kernel_ms, "flops_per_launch": fused_flops,
+                     "flops_note": ("FP64 FLOPs of F(n,P) done by this kernel"
+                                    + ("; y (2 P n per eval) on the tensor cores" if y_on_tc
+                                       else "")),
+                     "scan_stage_ms": fused_ms,
                      "resweep_tiles_per_launch": resweeps,
+                     "resweep_evals_per_launch": resweep_lanes,
                      "peak_source": "measured FP64 FMA peak (rr_fma_peak) on this GPU"},
         "e2e": e2e,
         "plain": plain,
@@ -491,8 +515,9 @@ def main():
     ap.add_argument("--zsub", type=int, default=None,
                     help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--ygemm", default="fp64", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
-                    help="y = Tb^T W f in the FP64 scan (default) or as a tensor-core GEMM")
+    ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
+                    help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
+                         "summed in the FP64 scan (fp64)")
     ap.add_argument("--ygemm-study", action="store_true",
                     help="also time every y variant once and report its chi2/coeff error")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -35,8 +35,8 @@
  *   rr_zscan_pairs_grad     adjoint of the pair scan: dchi2/dz,
  *                           d2chi2/dz2, dchi2/dflux (Newton refinement in
  *                           place of fitz.py:255-261's parabola)
- *   rr_pack_g, rr_ygemm     zscan.py:741-748 (y = Tb^T W f) for every
- *                           (target, z) as one tensor-core GEMM per template
+ *   rr_pack_g, rr_ygemm,    zscan.py:741-748 (y = Tb^T W f) for every
+ *   rr_ygemm_i8 (+ slicing) (target, z) as one tensor-core GEMM per template
  */
 #ifndef REDROCK_B200_H
 #define REDROCK_B200_H
@@ -210,9 +210,10 @@ typedef struct {
   int64_t npix_block;
 } rr_scan_targets;
 
-/* tile_counter: three device ints of scratch (reset by the call); on
+/* tile_counter: four device ints of scratch (reset by the call); on
  * return tile_counter[2] counts the tiles that were swept a second time to
- * sum chi2 as the direct residual (ill-conditioned fits).  Templates with
+ * sum chi2 as the direct residual (ill-conditioned fits) and
+ * tile_counter[3] the (target, z) pairs re-evaluated that way.  Templates with
  * nbasis 4, 5 or 10 run in one persistent launch, any others in a second
  * one. */
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
@@ -342,11 +343,16 @@ int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const dou
  * (targets x pixels) . (pixels x (z, basis)) run on tcgen05:
  *   RR_YGEMM_BF16X3  three bf16 slices, six products, FP32 accumulation
  *   RR_YGEMM_TF32X3  two tf32 slices, three products, FP32 accumulation
- *   RR_YGEMM_INT8X7  Ozaki scheme: power-of-two scaled, seven 7-bit integer
- *                    slices, 28 products accumulated exactly in int32,
- *                    combined in FP64 (needs row_exp and col_exp)
+ *   RR_YGEMM_INT8X7  Ozaki scheme: each G column / basis column scaled by a
+ *                    power of two and rounded to a 49-bit integer of seven
+ *                    base-128 digits; the 28 digit products of order <= 6
+ *                    accumulate exactly in int32 and combine in FP64
+ *                    (error <= K 2^-45 2^(e_t + e_n) per output)
  * Flow: rr_pack_targets -> rr_pack_g (G, row_exp) -> per template
- * [rr_basis_col_exp] + rr_ygemm (Y) -> rr_zscan_fused with y_ext = Y.
+ *   BF16X3 / TF32X3: rr_ygemm
+ *   INT8X7: rr_slice_g_i8 (once per target pack), rr_basis_col_exp +
+ *           rr_slice_basis_i8 (once per basis), rr_ygemm_i8
+ * -> rr_zscan_fused with y_ext = Y.
  * ---------------------------------------------------------------------- */
 enum rr_ygemm_variant {
   RR_YGEMM_NONE = 0,   /* y summed in FP64 inside the scan (default) */
@@ -369,10 +375,25 @@ int rr_pack_g(const rr_scan_targets* targets, int64_t pix_stride, int64_t kpad, 
 int rr_basis_col_exp(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
                      int basis_stride, int* col_exp, rr_stream_t stream);
 
-/* y[npos][nz][nbasis] = G^T . basis for one template (rr_ygemm_variant) */
-int rr_ygemm(int variant, const double* g, const int* row_exp, int64_t npos, int64_t kpad,
-             const double* basis, int64_t nz, int64_t pix_stride, int nbasis, int basis_stride,
-             const int* col_exp, double* y, int* status, rr_stream_t stream);
+/* y[npos][nz][nbasis] = G^T . basis, variant RR_YGEMM_BF16X3 or _TF32X3 */
+int rr_ygemm(int variant, const double* g, int64_t npos, int64_t kpad, const double* basis,
+             int64_t nz, int64_t pix_stride, int nbasis, int basis_stride, double* y,
+             int* status, rr_stream_t stream);
+
+/* RR_YGEMM_INT8X7: digit planes of G and of a basis, laid out as the
+ * GEMM's shared-memory tiles (16-byte aligned buffers of the sizes
+ * returned by the _bytes queries, -1 for invalid arguments) */
+int64_t rr_ygemm_i8_g_bytes(int64_t npos, int64_t kpad);
+int64_t rr_ygemm_i8_basis_bytes(int64_t nz, int nbasis, int64_t kpad);
+int rr_slice_g_i8(const double* g, const int* row_exp, int64_t npos, int64_t kpad,
+                  void* g_digits, rr_stream_t stream);
+int rr_slice_basis_i8(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
+                      int basis_stride, int64_t kpad, const int* col_exp, void* basis_digits,
+                      rr_stream_t stream);
+/* y[npos][nz][nbasis]; RR_ENOTSUP when kpad > 65536 (int32 headroom) */
+int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t kpad,
+                const void* basis_digits, const int* col_exp, int64_t nz, int nbasis,
+                double* y, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * FMA throughput probe (no counterpart in redrock): the roofline

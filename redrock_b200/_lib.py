@@ -130,8 +130,15 @@ _SIGNATURES = {
     "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
                           c_void_p, c_void_p, c_void_p]),
     "rr_basis_col_exp": (c_int, [c_void_p, c_int64, c_int64, c_int, c_int, c_void_p, c_void_p]),
-    "rr_ygemm": (c_int, [c_int, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64,
-                         c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "rr_ygemm": (c_int, [c_int, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64, c_int,
+                         c_int, c_void_p, c_void_p, c_void_p]),
+    "rr_ygemm_i8_g_bytes": (c_int64, [c_int64, c_int64]),
+    "rr_ygemm_i8_basis_bytes": (c_int64, [c_int64, c_int, c_int64]),
+    "rr_slice_g_i8": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
+    "rr_slice_basis_i8": (c_int, [c_void_p, c_int64, c_int64, c_int, c_int, c_int64, c_void_p,
+                                  c_void_p, c_void_p]),
+    "rr_ygemm_i8": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64,
+                            c_int, c_void_p, c_void_p, c_void_p]),
 }
 
 

@@ -75,7 +75,8 @@ struct FusedParams {
   int64_t chunks_total;  // pixel chunks per block (over all segments)
   int max_stride;        // largest basis_stride
   int* tile_counter;
-  int* resweep_counter;  // tiles swept a second time for the direct residual
+  int* resweep_counter;  // [0] tiles swept a second time for the direct residual,
+                         // [1] (target, z) lanes re-evaluated there
   int* status;
 };
 
@@ -295,6 +296,8 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   // not suffer the cancellation of f^T W f - c^T y
   if (__syncthreads_or(fix)) {
     if (threadIdx.x == 0 && p.resweep_counter) atomicAdd(p.resweep_counter, 1);
+    const unsigned lanes = __ballot_sync(0xffffffffu, fix);
+    if (lane == 0 && lanes && p.resweep_counter) atomicAdd(p.resweep_counter + 1, __popc(lanes));
     acc = 0.0;
     if (!sweep<NB, true, EXTY>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
       failed = true;
@@ -730,7 +733,7 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     group[gi][ng[gi]++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, sizeof(int), st));
+  RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, 2 * sizeof(int), st));
   // each launch resets its counter first (stream order), so common-set
   // launches share tile_counter[0] and the others tile_counter[1]
   int* resweep = tile_counter + 2;

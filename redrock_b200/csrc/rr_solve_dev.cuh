@@ -77,10 +77,15 @@ __device__ __forceinline__ bool ldlt_solve(const double (&m)[NB * (NB + 1) / 2],
 }
 
 // Relative accuracy assumed for the FP64 sums M, y and f^T W f (about 90
-// ulp; calibrated against redrock's direct residual), and the chi2 error
-// above which a (target, z) is re-evaluated by the direct residual.
+// ulp; calibrated against redrock's direct residual, whose measured error
+// stays below a tenth of this bound), and the bound on the chi2 error above
+// which a (target, z) is re-evaluated by the direct residual: 1e-4, a tenth
+// of the |dchi2| <= 1e-3 acceptance bar.
 constexpr double kSumEps = 1e-14;
-constexpr double kChi2FixTol = 1e-5;
+#ifndef RR_CHI2_FIX_TOL
+#define RR_CHI2_FIX_TOL 1e-4
+#endif
+constexpr double kChi2FixTol = RR_CHI2_FIX_TOL;
 
 // Solve and chi2 for one (target, z) from its normal equations.
 // chi2 = f^T W f - c^T y - c^T P c.  Also returns an upper estimate of that

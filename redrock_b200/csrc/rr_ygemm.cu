@@ -7,25 +7,30 @@
 // every (target, z, basis) of a template is one GEMM:
 //   Y[t][(z, i)] = sum_q G[q][t] T[z][q][i]   (M = targets, N = (z, i),
 //                                              K = padded basis pixel index).
-// rr_pack_g builds G (and, for the integer variant, a power-of-two scale per
-// target); rr_ygemm runs the GEMM on the tcgen05 tensor cores; the fused scan
-// then reads Y instead of accumulating y itself (rr_scan_template.y_ext).
+// rr_pack_g builds G (and a power-of-two scale per target); the GEMM runs on
+// the tcgen05 tensor cores; the fused scan then reads Y instead of summing y
+// itself (rr_scan_template.y_ext).
 //
-// Operands are FP64 in HBM.  Each CTA stages a 128-target x 32/64-pixel tile
-// of G and an N x 32/64-pixel tile of the basis into shared memory, splitting
-// every value into slices on the way (the canonical K-major, no-swizzle UMMA
-// layout: 8-row x 16-byte core matrices), and one thread issues the slice
-// products as tcgen05.mma into TMEM accumulators.  Two stages alternate; a
-// stage is refilled once the tcgen05.commit of its previous MMAs arrives on
-// its mbarrier.  Variants (rr_ygemm_variant):
-//   BF16X3  three bf16 slices per value (hi + mid + lo), the six products of
-//           slice order <= 2, one FP32 accumulator (kind::f16).
-//   TF32X3  two tf32 slices, hi*hi + hi*lo + lo*hi, FP32 (kind::tf32).
-//   INT8X7  Ozaki scheme: G rows and basis columns scaled by powers of two,
-//           split into seven 7-bit signed integer slices; the 28 products of
-//           slices (i, j) with i + j <= 6 accumulate EXACTLY in int32
-//           accumulator i + j (kind::i8), and the seven accumulators are
-//           combined in FP64.  Error ~ 2^-49 of max|G| max|T| per term.
+// Operand tiles sit in shared memory in the canonical K-major, no-swizzle
+// UMMA layout (8-row x 16-byte core matrices; unit u of a tile is the
+// 16-byte core-matrix row at byte 16 u) and one thread issues the
+// tcgen05.mma into TMEM accumulators.  Variants (rr_ygemm_variant):
+//   BF16X3  (rr_ygemm) three bf16 slices per value (hi + mid + lo), the six
+//           products of slice order <= 2, one FP32 accumulator (kind::f16).
+//           Slicing happens while a tile is staged.
+//   TF32X3  (rr_ygemm) two tf32 slices, hi*hi + hi*lo + lo*hi, FP32
+//           accumulation (kind::tf32).
+//   INT8X7  (rr_slice_g_i8 + rr_slice_basis_i8 + rr_ygemm_i8) Ozaki scheme:
+//           each G column and basis column is scaled by a power of two and
+//           rounded to a 49-bit integer X = sum_k a_k 128^(6-k) with seven
+//           base-128 digits |a_k| <= 64 (kind::i8 operands).  The 28 digit
+//           products of order i + j <= 6 accumulate EXACTLY in the int32
+//           accumulator i + j and the seven accumulators combine in FP64.
+//           The digits are written once per operand, already in the
+//           shared-memory tile layout, and the GEMM streams them with 1-D
+//           bulk copies (warp-specialised: one producer thread, one MMA
+//           thread, four stages).  Error <= K 2^-45 2^(e_t + e_n) per
+//           output for columns bounded by 2^e_t and 2^e_n.
 #include <cuda_bf16.h>
 #include <climits>
 #include <cmath>
@@ -37,55 +42,8 @@ namespace yg {
 
 constexpr int kTileM = 128;  // targets per tile (MMA M)
 constexpr int kThreads = 256;
-constexpr int kStages = 2;
-constexpr int kKpadAlign = 64;  // G rows padded to a multiple of the largest stage depth
+constexpr int kKpadAlign = 64;  // G rows padded to a multiple of every stage depth
 constexpr int kExpBias = 4096;  // stored exponents are biased; 0 = all-zero row/column
-
-template <int V>
-struct Var;
-template <>
-struct Var<RR_YGEMM_BF16X3> {
-  static constexpr int kEsz = 2, kSlices = 3, kKInst = 16, kNAcc = 1, kNMax = 256, kKt = 32;
-  static constexpr uint32_t kFmt = (1u << 4) | (1u << 7) | (1u << 10);  // D f32, A/B bf16
-};
-template <>
-struct Var<RR_YGEMM_TF32X3> {
-  static constexpr int kEsz = 4, kSlices = 2, kKInst = 8, kNAcc = 1, kNMax = 256, kKt = 32;
-  static constexpr uint32_t kFmt = (1u << 4) | (2u << 7) | (2u << 10);  // D f32, A/B tf32
-};
-template <>
-struct Var<RR_YGEMM_INT8X7> {
-  static constexpr int kEsz = 1, kSlices = 7, kKInst = 32, kNAcc = 7, kNMax = 64, kKt = 64;
-  static constexpr uint32_t kFmt = (2u << 4) | (1u << 7) | (1u << 10);  // D s32, A/B s8
-};
-
-template <int V>
-struct Geo {
-  using P = Var<V>;
-  static constexpr int kE = 16 / P::kEsz;          // elements per 16-byte core-matrix row
-  static constexpr int kNkg = P::kKt / kE;         // core matrices along K per stage
-  static constexpr int kSteps = P::kKt / P::kKInst;  // MMA instructions along K per stage
-  static constexpr int kSbo = kNkg * 128;          // bytes between 8-row groups
-  static constexpr int kASlice = kTileM * P::kKt * P::kEsz;
-  static constexpr int kTmemCols = P::kNAcc * P::kNMax <= 256 ? 256 : 512;
-  static __host__ __device__ constexpr int b_slice(int n) { return n * P::kKt * P::kEsz; }
-  static __host__ __device__ constexpr int stage_bytes(int n) {
-    return P::kSlices * (kASlice + b_slice(n));
-  }
-};
-
-struct YParams {
-  const double* g;      // [kpad][npos]
-  const int* row_exp;   // [npos] biased exponents (INT8X7)
-  const double* basis;  // [nz][pix_stride][basis_stride]
-  const int* col_exp;   // [nz * nbasis] biased exponents (INT8X7)
-  double* y;            // [npos][nz][nbasis]
-  int64_t npos, kpad, pix_stride;
-  int nz, nbasis, basis_stride;
-  int zt;    // redshifts per tile
-  int n;     // MMA N (zt * nbasis rounded up to 16)
-  int* status;
-};
 
 // ---------------------------------------------------------------------------
 // tcgen05 / descriptor helpers
@@ -101,15 +59,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo) {
   return d;                // base offset 0, layout type 0 = SWIZZLE_NONE
 }
 
-template <int V>
+// instruction descriptor: D format / A,B formats (fmt), K-major A and B, N, M
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt, int n, int m) {
+  return fmt | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+enum Kind { kF16, kTF32, kI8 };
+
+template <Kind K>
 __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
                                     uint32_t accumulate) {
-  if constexpr (V == RR_YGEMM_BF16X3) {
+  if constexpr (K == kF16) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-  } else if constexpr (V == RR_YGEMM_TF32X3) {
+  } else if constexpr (K == kTF32) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
@@ -136,6 +101,17 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
 // 8 consecutive 32-bit TMEM columns of this thread's lane
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
   asm volatile(
@@ -148,9 +124,59 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// ---------------------------------------------------------------------------
-// slicing: one 16-byte core-matrix row (kE consecutive K elements) per call
-// ---------------------------------------------------------------------------
+__device__ __forceinline__ int unbias(int e) { return e > 0 ? e - kExpBias : 0; }
+
+// unit u of a tile with nkg core matrices along K: row and K group
+__device__ __forceinline__ void unit_rc(int u, int nkg, int& r, int& kg) {
+  r = (u & 7) + 8 * (u / (8 * nkg));
+  kg = (u >> 3) % nkg;
+}
+
+// ===========================================================================
+// BF16X3 / TF32X3: slices made while staging, FP32 accumulation
+// ===========================================================================
+template <int V>
+struct Var;
+template <>
+struct Var<RR_YGEMM_BF16X3> {
+  static constexpr int kEsz = 2, kSlices = 3, kKInst = 16, kNMax = 256, kKt = 32;
+  static constexpr Kind kKind = kF16;
+  static constexpr uint32_t kFmt = (1u << 4) | (1u << 7) | (1u << 10);  // D f32, A/B bf16
+};
+template <>
+struct Var<RR_YGEMM_TF32X3> {
+  static constexpr int kEsz = 4, kSlices = 2, kKInst = 8, kNMax = 256, kKt = 32;
+  static constexpr Kind kKind = kTF32;
+  static constexpr uint32_t kFmt = (1u << 4) | (2u << 7) | (2u << 10);  // D f32, A/B tf32
+};
+
+template <int V>
+struct Geo {
+  using P = Var<V>;
+  static constexpr int kE = 16 / P::kEsz;            // elements per 16-byte core-matrix row
+  static constexpr int kNkg = P::kKt / kE;           // core matrices along K per stage
+  static constexpr int kSteps = P::kKt / P::kKInst;  // MMA instructions along K per stage
+  static constexpr int kSbo = kNkg * 128;            // bytes between 8-row groups
+  static constexpr int kASlice = kTileM * P::kKt * P::kEsz;
+  static constexpr int kTmemCols = 256;
+  static constexpr int kStages = 2;
+  static __host__ __device__ constexpr int b_slice(int n) { return n * P::kKt * P::kEsz; }
+  static __host__ __device__ constexpr int stage_bytes(int n) {
+    return P::kSlices * (kASlice + b_slice(n));
+  }
+};
+
+struct YParams {
+  const double* g;      // [kpad][npos]
+  const double* basis;  // [nz][pix_stride][basis_stride]
+  double* y;            // [npos][nz][nbasis]
+  int64_t npos, kpad, pix_stride;
+  int nz, nbasis, basis_stride;
+  int zt;    // redshifts per tile
+  int n;     // MMA N (zt * nbasis rounded up to 16)
+  int* status;
+};
+
 __device__ __forceinline__ uint32_t bf16_bits(double x, double& rest) {
   const __nv_bfloat16 h = __double2bfloat16(x);
   rest = x - (double)__bfloat162float(h);
@@ -163,11 +189,10 @@ __device__ __forceinline__ uint32_t tf32_bits(double x, double& rest) {
   return r;
 }
 
-// Write the slices of v[0..kE) (scaled by 2^-exp for INT8X7) to
-// dst + s * slice_bytes, s = 0..kSlices-1.
+// Write the slices of v[0..kE) to dst + s * slice_bytes, s < kSlices.
 template <int V>
-__device__ __forceinline__ void store_slices(const double (&v)[Geo<V>::kE], int exp,
-                                             unsigned char* dst, int slice_bytes) {
+__device__ __forceinline__ void store_slices(const double (&v)[Geo<V>::kE], unsigned char* dst,
+                                             int slice_bytes) {
   constexpr int kE = Geo<V>::kE;
   if constexpr (V == RR_YGEMM_BF16X3) {
     uint32_t w[3][4];
@@ -184,7 +209,7 @@ __device__ __forceinline__ void store_slices(const double (&v)[Geo<V>::kE], int 
 #pragma unroll
     for (int s = 0; s < 3; ++s)
       *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
-  } else if constexpr (V == RR_YGEMM_TF32X3) {
+  } else {
     uint32_t w[2][4];
 #pragma unroll
     for (int j = 0; j < kE; ++j) {
@@ -195,60 +220,33 @@ __device__ __forceinline__ void store_slices(const double (&v)[Geo<V>::kE], int 
 #pragma unroll
     for (int s = 0; s < 2; ++s)
       *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
-  } else {
-    // |v| 2^-exp <= 1: slice 0 = rint(2^6 x), then 7 more bits per slice;
-    // every step is exact in FP64
-    uint32_t w[7][4];
-#pragma unroll
-    for (int s = 0; s < 7; ++s)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) w[s][j] = 0;
-#pragma unroll
-    for (int j = 0; j < kE; ++j) {
-      double r = ldexp(v[j], 6 - exp);
-#pragma unroll
-      for (int s = 0; s < 7; ++s) {
-        const double a = rint(r);
-        r = (r - a) * 128.0;
-        w[s][j >> 2] |= ((uint32_t)(int)a & 0xFFu) << (8 * (j & 3));
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < 7; ++s)
-      *reinterpret_cast<uint4*>(dst + s * slice_bytes) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
   }
 }
 
-__device__ __forceinline__ int unbias(int e) { return e > 0 ? e - kExpBias : 0; }
-
-// Stage K-chunk c (pixels q0 .. q0 + kKt) of the tile into shared memory.
-// Unit u of a slice tile is the 16-byte core-matrix row at byte u * 16:
-// row r = (u & 7) + 8 * (u / (8 kNkg)), K group kg = (u >> 3) % kNkg.
+// Stage K-chunk (pixels q0 .. q0 + kKt) of the tile into shared memory.
 template <int V>
 __device__ __forceinline__ void stage_tile(const YParams& p, unsigned char* st, int64_t t0, int z0,
-                                           int nzt, int64_t q0, const int* s_rexp,
-                                           const int* s_cexp) {
+                                           int nzt, int64_t q0) {
   using G = Geo<V>;
   using P = Var<V>;
   constexpr int kE = G::kE;
   // A: G[q][t0 + r]
   for (int u = threadIdx.x; u < kTileM * G::kNkg; u += kThreads) {
-    const int r = (u & 7) + 8 * (u / (8 * G::kNkg));
-    const int kg = (u >> 3) % G::kNkg;
+    int r, kg;
+    unit_rc(u, G::kNkg, r, kg);
     const double* src = p.g + (q0 + kg * kE) * p.npos + t0 + r;
     double v[kE];
 #pragma unroll
     for (int j = 0; j < kE; ++j) v[j] = __ldg(src + (int64_t)j * p.npos);
-    store_slices<V>(v, V == RR_YGEMM_INT8X7 ? s_rexp[r] : 0, st + u * 16, G::kASlice);
+    store_slices<V>(v, st + u * 16, G::kASlice);
   }
   // B: row n = (zl, i) of the basis, T[z0 + zl][q][i]
   unsigned char* sb = st + P::kSlices * G::kASlice;
   const int nused = nzt * p.nbasis;
   for (int u = threadIdx.x; u < p.n * G::kNkg; u += kThreads) {
-    const int r = (u & 7) + 8 * (u / (8 * G::kNkg));
-    const int kg = (u >> 3) % G::kNkg;
+    int r, kg;
+    unit_rc(u, G::kNkg, r, kg);
     double v[kE];
-    int e = 0;
     if (r < nused) {
       const int zl = r / p.nbasis;
       const int i = r - zl * p.nbasis;
@@ -257,12 +255,11 @@ __device__ __forceinline__ void stage_tile(const YParams& p, unsigned char* st, 
 #pragma unroll
       for (int j = 0; j < kE; ++j)
         v[j] = (q + j < p.pix_stride) ? __ldg(src + (int64_t)j * p.basis_stride) : 0.0;
-      if (V == RR_YGEMM_INT8X7) e = s_cexp[r];
     } else {
 #pragma unroll
       for (int j = 0; j < kE; ++j) v[j] = 0.0;
     }
-    store_slices<V>(v, e, sb + u * 16, G::b_slice(p.n));
+    store_slices<V>(v, sb + u * 16, G::b_slice(p.n));
   }
 }
 
@@ -270,11 +267,10 @@ template <int V>
 __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constant__ YParams p) {
   using G = Geo<V>;
   using P = Var<V>;
+  constexpr int kStages = G::kStages;
   extern __shared__ __align__(1024) unsigned char ysm[];
   __shared__ __align__(8) uint64_t done[kStages];
   __shared__ uint32_t s_tmem;
-  __shared__ int s_rexp[kTileM];
-  __shared__ int s_cexp[Var<V>::kNMax];
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -282,31 +278,17 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
   const int z0 = blockIdx.y * p.zt;
   const int nzt = min(p.zt, p.nz - z0);
 
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(&s_tmem)),
-                 "r"((uint32_t)G::kTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
+  if (warp == 0) tmem_alloc(&s_tmem, G::kTmemCols);
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&done[s], 1);
     fence_mbar_init();
-  }
-  if (V == RR_YGEMM_INT8X7) {
-    for (int r = threadIdx.x; r < kTileM; r += kThreads) s_rexp[r] = unbias(p.row_exp[t0 + r]);
-    for (int r = threadIdx.x; r < p.n; r += kThreads) {
-      const int zl = r / p.nbasis;
-      s_cexp[r] = (zl < nzt) ? unbias(p.col_exp[(int64_t)(z0 + zl) * p.nbasis + r - zl * p.nbasis])
-                             : 0;
-    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
 
-  const uint32_t idesc = P::kFmt | ((uint32_t)(p.n >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
+  const uint32_t idesc = instr_desc(P::kFmt, p.n, kTileM);
   const int stage_bytes = G::stage_bytes(p.n);
   const int64_t nchunk = p.kpad / P::kKt;
   bool ok = true;
@@ -321,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
         break;
       }
     }
-    stage_tile<V>(p, st, t0, z0, nzt, c * P::kKt, s_rexp, s_cexp);
+    stage_tile<V>(p, st, t0, z0, nzt, c * P::kKt);
     fence_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -331,29 +313,16 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
 #pragma unroll 1
       for (int ks = 0; ks < G::kSteps; ++ks) {
         const uint32_t koff = ks * 256;
-        if constexpr (V == RR_YGEMM_INT8X7) {
-          // products (i, j), i + j = d <= 6, into accumulator d
+        // all slice products of order <= kSlices - 1, smallest first
 #pragma unroll 1
-          for (int d = 0; d < 7; ++d)
+        for (int d = P::kSlices - 1; d >= 0; --d)
 #pragma unroll 1
-            for (int i = 0; i <= d; ++i) {
-              const uint64_t da = smem_desc(a0 + i * G::kASlice + koff, G::kSbo);
-              const uint64_t db = smem_desc(b0 + (d - i) * G::b_slice(p.n) + koff, G::kSbo);
-              const uint32_t acc = (c > 0 || ks > 0 || i > 0) ? 1u : 0u;
-              mma<V>(tmem + d * P::kNMax, da, db, idesc, acc);
-            }
-        } else {
-          // all slice products of order <= kSlices - 1, smallest first
-#pragma unroll 1
-          for (int d = P::kSlices - 1; d >= 0; --d)
-#pragma unroll 1
-            for (int i = 0; i <= d; ++i) {
-              const uint64_t da = smem_desc(a0 + i * G::kASlice + koff, G::kSbo);
-              const uint64_t db = smem_desc(b0 + (d - i) * G::b_slice(p.n) + koff, G::kSbo);
-              const uint32_t acc = (c > 0 || ks > 0 || d != P::kSlices - 1 || i > 0) ? 1u : 0u;
-              mma<V>(tmem, da, db, idesc, acc);
-            }
-        }
+          for (int i = 0; i <= d; ++i) {
+            const uint64_t da = smem_desc(a0 + i * G::kASlice + koff, G::kSbo);
+            const uint64_t db = smem_desc(b0 + (d - i) * G::b_slice(p.n) + koff, G::kSbo);
+            const uint32_t acc = (c > 0 || ks > 0 || d != P::kSlices - 1 || i > 0) ? 1u : 0u;
+            mma<P::kKind>(tmem, da, db, idesc, acc);
+          }
       }
       mma_commit(&done[s]);
     }
@@ -366,53 +335,276 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
   ok = __syncthreads_and(ok);
   if (ok) {
     tc_fence_after();
-    const int lg = warp & 3;           // TMEM lanes 32 lg .. 32 lg + 31
-    const int half = warp >> 2;        // column half
+    const int lg = warp & 3;     // TMEM lanes 32 lg .. 32 lg + 31
+    const int half = warp >> 2;  // column half
     const int64_t pos = t0 + 32 * lg + lane;
     const int ncol = p.n / 2;
     const int nused = nzt * p.nbasis;
     double* yrow = p.y + (pos * p.nz + z0) * p.nbasis;
-    const bool row_ok = pos < p.npos;
     const uint32_t tl = tmem + ((uint32_t)(32 * lg) << 16);
     for (int c0 = half * ncol; c0 < (half + 1) * ncol; c0 += 8) {
-      double out[8];
-      if constexpr (V == RR_YGEMM_INT8X7) {
+      uint32_t v[8];
+      tmem_ld8(tl + c0, v);
+      tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) out[j] = 0.0;
-        // smallest terms first
-#pragma unroll 1
-        for (int d = 6; d >= 0; --d) {
-          uint32_t v[8];
-          tmem_ld8(tl + d * P::kNMax + c0, v);
-          tmem_wait_ld();
-#pragma unroll
-          for (int j = 0; j < 8; ++j) out[j] += ldexp((double)(int)v[j], -12 - 7 * d);
-        }
-        const int re = s_rexp[32 * lg + lane];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) out[j] = ldexp(out[j], re + s_cexp[c0 + j]);
-      } else {
-        uint32_t v[8];
-        tmem_ld8(tl + c0, v);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 8; ++j) out[j] = (double)__uint_as_float(v[j]);
-      }
-      if (row_ok)
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (c0 + j < nused) yrow[c0 + j] = out[j];
+      for (int j = 0; j < 8; ++j)
+        if (pos < p.npos && c0 + j < nused) yrow[c0 + j] = (double)__uint_as_float(v[j]);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"((uint32_t)G::kTmemCols)
-                 : "memory");
+    tmem_dealloc(tmem, G::kTmemCols);
   }
 }
+
+template <int V>
+static int launch_ygemm(YParams p, cudaStream_t stream) {
+  using P = Var<V>;
+  if (p.kpad % P::kKt) return RR_EINVAL;
+  int zt = P::kNMax / p.nbasis;
+  if (zt > p.nz) zt = p.nz;
+  p.zt = zt;
+  p.n = ((zt * p.nbasis + 15) / 16) * 16;
+  if (p.n > P::kNMax) return RR_EINVAL;
+  const size_t smem = (size_t)Geo<V>::kStages * Geo<V>::stage_bytes(p.n);
+  RR_CUDA_TRY(cudaFuncSetAttribute(ygemm_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  dim3 grid((unsigned)(p.npos / kTileM), (unsigned)((p.nz + zt - 1) / zt));
+  ygemm_kernel<V><<<grid, kThreads, smem, stream>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+// ===========================================================================
+// INT8X7: pre-sliced operands, exact integer accumulation
+// ===========================================================================
+namespace i8 {
+constexpr int kDigits = 7;
+constexpr int kKt = 32;                    // pixels per stage = one MMA K step
+constexpr int kNkg = kKt / 16;             // 2 core matrices along K
+constexpr int kSbo = kNkg * 128;           // 256 B between 8-row groups
+constexpr int kN = 64;                     // MMA N: 7 accumulators x 64 columns <= 512
+constexpr int kStages = 4;
+constexpr int kASlice = kTileM * kKt;      // bytes of one digit plane of a G block
+constexpr int kBSlice = kN * kKt;
+constexpr int kABlock = kDigits * kASlice;  // 28672 B per (target tile, chunk)
+constexpr int kBBlock = kDigits * kBSlice;  // 14336 B per (z tile, chunk)
+constexpr int kStageBytes = kABlock + kBBlock;
+constexpr uint32_t kFmt = (2u << 4) | (1u << 7) | (1u << 10);  // D s32, A/B signed 8-bit
+
+__host__ __device__ constexpr int zt_of(int nbasis) { return kN / nbasis; }
+
+// Base-128 digits of X = rint(x 2^(48 - e)), |x| < 2^e, so |X| < 2^48 and
+// X = sum_k a_k 128^(6 - k): six balanced low digits in [-64, 63] and a
+// leading digit |a_0| <= 64.  One FP64 -> int64 conversion; the digits are
+// integer shifts and masks.  Digit k of element j goes to byte j of plane k.
+__device__ __forceinline__ void digits16(const double (&v)[16], int e, unsigned char* dst,
+                                         int plane_bytes) {
+  // 2^(48 - e) as two factors so that neither overflows for tiny columns
+  const int sh = 48 - e;
+  const double f1 = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
+  uint32_t w[kDigits][4];
+#pragma unroll
+  for (int k = 0; k < kDigits; ++k)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[k][j] = 0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    long long x = __double2ll_rn((v[j] * f1) * f2);
+#pragma unroll
+    for (int k = kDigits - 1; k >= 1; --k) {
+      const long long a = ((x + 64) & 127) - 64;  // in [-64, 63]
+      x = (x - a) >> 7;                           // exact: x - a is a multiple of 128
+      w[k][j >> 2] |= ((uint32_t)a & 0xFFu) << (8 * (j & 3));
+    }
+    // the rest is the leading digit: |X| < 2^48 and the six lower digits sum
+    // to within (-0.504, 0.496) 128^6, so |x| <= 64 (no wrap here, which
+    // would drop a carry)
+    w[0][j >> 2] |= ((uint32_t)x & 0xFFu) << (8 * (j & 3));
+  }
+#pragma unroll
+  for (int k = 0; k < kDigits; ++k)
+    *reinterpret_cast<uint4*>(dst + k * plane_bytes) = make_uint4(w[k][0], w[k][1], w[k][2], w[k][3]);
+}
+
+// G digits: one block per (target tile, chunk), one thread per unit
+__global__ void __launch_bounds__(256) slice_g_kernel(const double* __restrict__ g,
+                                                      const int* __restrict__ row_exp,
+                                                      int64_t npos, int64_t nchunk,
+                                                      unsigned char* __restrict__ out) {
+  const int64_t tile = blockIdx.x;
+  const int64_t c = blockIdx.y;
+  const int u = threadIdx.x;  // < kTileM * kNkg
+  int r, kg;
+  unit_rc(u, kNkg, r, kg);
+  const int64_t t = tile * kTileM + r;
+  const double* src = g + (c * kKt + kg * 16) * npos + t;
+  double v[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __ldg(src + (int64_t)j * npos);
+  digits16(v, unbias(row_exp[t]), out + (tile * nchunk + c) * kABlock + u * 16, kASlice);
+}
+
+// basis digits: one block per (z tile, chunk), one thread per unit
+__global__ void __launch_bounds__(128) slice_basis_kernel(
+    const double* __restrict__ basis, int nz, int64_t pix_stride, int nbasis, int basis_stride,
+    const int* __restrict__ col_exp, int64_t nchunk, unsigned char* __restrict__ out) {
+  const int zt = zt_of(nbasis);
+  const int64_t tile = blockIdx.x;
+  const int64_t c = blockIdx.y;
+  const int u = threadIdx.x;  // < kN * kNkg
+  int r, kg;
+  unit_rc(u, kNkg, r, kg);
+  const int z0 = (int)tile * zt;
+  const int nused = min(zt, nz - z0) * nbasis;
+  double v[16];
+  int e = 0;
+  if (r < nused) {
+    const int zl = r / nbasis;
+    const int i = r - zl * nbasis;
+    const int64_t q = c * kKt + kg * 16;
+    const double* src = basis + ((int64_t)(z0 + zl) * pix_stride + q) * basis_stride + i;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      v[j] = (q + j < pix_stride) ? __ldg(src + (int64_t)j * basis_stride) : 0.0;
+    e = unbias(col_exp[(int64_t)(z0 + zl) * nbasis + i]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = 0.0;
+  }
+  digits16(v, e, out + (tile * nchunk + c) * kBBlock + u * 16, kBSlice);
+}
+
+struct Params {
+  const unsigned char* ga;  // G digits, [npos / 128][nchunk] blocks
+  const unsigned char* tb;  // basis digits, [ztiles][nchunk] blocks
+  const int* row_exp;
+  const int* col_exp;
+  double* y;  // [npos][nz][nbasis]
+  int64_t npos, nchunk;
+  int nz, nbasis, zt;
+  int* status;
+};
+
+// grid (npos / 128, ztiles), 256 threads: thread 0 streams the digit blocks
+// (1-D bulk copies), thread 32 issues the MMAs, all eight warps read TMEM.
+__global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constant__ Params p) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ __align__(8) uint64_t acc_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_fail;
+  __shared__ int s_rexp[kTileM];
+  __shared__ int s_cexp[kN];
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t mt = blockIdx.x;
+  const int64_t ztile = blockIdx.y;
+  const int z0 = (int)ztile * p.zt;
+  const int nused = min(p.zt, p.nz - z0) * p.nbasis;
+
+  if (warp == 0) tmem_alloc(&s_tmem, 512);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&acc_done, 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  for (int r = threadIdx.x; r < kTileM; r += kThreads) s_rexp[r] = unbias(p.row_exp[mt * kTileM + r]);
+  for (int r = threadIdx.x; r < kN; r += kThreads) {
+    const int zl = r / p.nbasis;
+    s_cexp[r] = r < nused ? unbias(p.col_exp[(int64_t)(z0 + zl) * p.nbasis + r - zl * p.nbasis]) : 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  if (threadIdx.x == 0) {
+    // producer
+    for (int64_t c = 0; c < p.nchunk; ++c) {
+      const int s = (int)(c % kStages);
+      const uint32_t use = (uint32_t)(c / kStages);
+      if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, p.status)) {
+        s_fail = 1;
+        break;
+      }
+      unsigned char* st = sm + s * kStageBytes;
+      mbar_arrive_expect_tx(&full[s], kStageBytes);
+      bulk_g2s(st, p.ga + (mt * p.nchunk + c) * kABlock, kABlock, &full[s]);
+      bulk_g2s(st + kABlock, p.tb + (ztile * p.nchunk + c) * kBBlock, kBBlock, &full[s]);
+    }
+  } else if (threadIdx.x == 32) {
+    // MMA issuer: digit products (i, j), i + j = d <= 6, into accumulator d
+    const uint32_t idesc = instr_desc(kFmt, kN, kTileM);
+    for (int64_t c = 0; c < p.nchunk; ++c) {
+      const int s = (int)(c % kStages);
+      const uint32_t use = (uint32_t)(c / kStages);
+      if (!mbar_wait(&full[s], use & 1, p.status)) {
+        s_fail = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(sm + s * kStageBytes);
+      const uint32_t b0 = a0 + kABlock;
+#pragma unroll 1
+      for (int d = 0; d < kDigits; ++d)
+#pragma unroll 1
+        for (int i = 0; i <= d; ++i) {
+          const uint64_t da = smem_desc(a0 + i * kASlice, kSbo);
+          const uint64_t db = smem_desc(b0 + (d - i) * kBSlice, kSbo);
+          mma<kI8>(tmem + d * kN, da, db, idesc, (c > 0 || i > 0) ? 1u : 0u);
+        }
+      mma_commit(&empty[s]);
+    }
+    mma_commit(&acc_done);
+  }
+  __syncthreads();
+  bool ok = s_fail == 0;
+  if (ok) ok = mbar_wait(&acc_done, 0, p.status);
+  ok = __syncthreads_and(ok);
+  if (ok) {
+    tc_fence_after();
+    const int lg = warp & 3;     // TMEM lanes 32 lg .. 32 lg + 31
+    const int half = warp >> 2;  // column half
+    const int row = 32 * lg + lane;
+    const int64_t pos = mt * kTileM + row;
+    double* yrow = p.y + (pos * p.nz + z0) * p.nbasis;
+    const uint32_t tl = tmem + ((uint32_t)(32 * lg) << 16);
+    for (int c0 = half * (kN / 2); c0 < (half + 1) * (kN / 2); c0 += 8) {
+      double out[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) out[j] = 0.0;
+      // X_t X_n = sum_d D_d 128^(12 - d) (d <= 6 kept); smallest terms first
+#pragma unroll 1
+      for (int d = kDigits - 1; d >= 0; --d) {
+        uint32_t v[8];
+        tmem_ld8(tl + d * kN + c0, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) out[j] += ldexp((double)(int)v[j], -7 * d);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (c0 + j < nused) yrow[c0 + j] = ldexp(out[j], s_rexp[row] + s_cexp[c0 + j] - 12);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+}  // namespace i8
 
 // ---------------------------------------------------------------------------
 // G = R^T W f per target, pixel-major, and the per-target exponent
@@ -493,28 +685,6 @@ __global__ void __launch_bounds__(256) col_exp_kernel(const double* __restrict__
   }
 }
 
-template <int V>
-static int launch_ygemm(YParams p, cudaStream_t stream) {
-  using P = Var<V>;
-  if (p.kpad % P::kKt) return RR_EINVAL;
-  if (V == RR_YGEMM_INT8X7 && (!p.row_exp || !p.col_exp)) return RR_EINVAL;
-  // exact int32 accumulation: |slice| <= 64, at most 7 products per
-  // accumulator and pixel
-  if (V == RR_YGEMM_INT8X7 && p.kpad > 65536) return RR_ENOTSUP;
-  int zt = P::kNMax / p.nbasis;
-  if (zt > p.nz) zt = p.nz;
-  p.zt = zt;
-  p.n = ((zt * p.nbasis + 15) / 16) * 16;
-  if (p.n > P::kNMax) return RR_EINVAL;
-  const size_t smem = (size_t)kStages * Geo<V>::stage_bytes(p.n);
-  RR_CUDA_TRY(cudaFuncSetAttribute(ygemm_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-  dim3 grid((unsigned)(p.npos / kTileM), (unsigned)((p.nz + zt - 1) / zt));
-  ygemm_kernel<V><<<grid, kThreads, smem, stream>>>(p);
-  RR_CHECK_LAUNCH();
-  return RR_OK;
-}
-
 }  // namespace yg
 }  // namespace rr
 
@@ -531,11 +701,11 @@ extern "C" int rr_pack_g(const rr_scan_targets* targets, int64_t pix_stride, int
   if (!targets || !g || pix_stride < 1 || kpad < pix_stride || kpad % yg::kKpadAlign) return RR_EINVAL;
   if (targets->nseg < 1 || targets->nseg > 16 || !targets->segs) return RR_EINVAL;
   if (npos % yg::kTileM || npos < (int64_t)targets->nblock * RR_LANES) return RR_EINVAL;
+  if (!targets->rw || targets->nblock < 0) return RR_EINVAL;
   yg::GParams p;
   p.rw = targets->rw;
   p.npix_block = targets->npix_block;
   p.nseg = targets->nseg;
-  if (!targets->rw || targets->nblock < 0) return RR_EINVAL;
   for (int s = 0; s < p.nseg; ++s) {
     p.segs[s] = targets->segs[s];
     const rr_segment_desc& sd = p.segs[s];
@@ -570,10 +740,9 @@ extern "C" int rr_basis_col_exp(const double* basis, int64_t nz, int64_t pix_str
   return RR_OK;
 }
 
-extern "C" int rr_ygemm(int variant, const double* g, const int* row_exp, int64_t npos,
-                        int64_t kpad, const double* basis, int64_t nz, int64_t pix_stride,
-                        int nbasis, int basis_stride, const int* col_exp, double* y, int* status,
-                        rr_stream_t stream) {
+extern "C" int rr_ygemm(int variant, const double* g, int64_t npos, int64_t kpad,
+                        const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
+                        int basis_stride, double* y, int* status, rr_stream_t stream) {
   if (!g || !basis || !y || npos < yg::kTileM || npos % yg::kTileM) return RR_EINVAL;
   if (nz < 0 || nz > INT_MAX || nbasis < 1 || nbasis > RR_MAX_NBASIS || basis_stride < nbasis)
     return RR_EINVAL;
@@ -581,9 +750,7 @@ extern "C" int rr_ygemm(int variant, const double* g, const int* row_exp, int64_
   if (nz == 0) return RR_OK;
   yg::YParams p;
   p.g = g;
-  p.row_exp = row_exp;
   p.basis = basis;
-  p.col_exp = col_exp;
   p.y = y;
   p.npos = npos;
   p.kpad = kpad;
@@ -596,7 +763,83 @@ extern "C" int rr_ygemm(int variant, const double* g, const int* row_exp, int64_
   switch (variant) {
     case RR_YGEMM_BF16X3: return yg::launch_ygemm<RR_YGEMM_BF16X3>(p, st);
     case RR_YGEMM_TF32X3: return yg::launch_ygemm<RR_YGEMM_TF32X3>(p, st);
-    case RR_YGEMM_INT8X7: return yg::launch_ygemm<RR_YGEMM_INT8X7>(p, st);
-    default: return RR_EINVAL;
+    default: return RR_EINVAL;  // RR_YGEMM_INT8X7 runs through rr_ygemm_i8
   }
+}
+
+extern "C" int64_t rr_ygemm_i8_g_bytes(int64_t npos, int64_t kpad) {
+  if (npos < 0 || kpad < 0 || npos % yg::kTileM || kpad % yg::i8::kKt) return -1;
+  return (npos / yg::kTileM) * (kpad / yg::i8::kKt) * (int64_t)yg::i8::kABlock;
+}
+
+extern "C" int64_t rr_ygemm_i8_basis_bytes(int64_t nz, int nbasis, int64_t kpad) {
+  if (nz < 0 || nbasis < 1 || nbasis > RR_MAX_NBASIS || kpad < 0 || kpad % yg::i8::kKt) return -1;
+  const int zt = yg::i8::zt_of(nbasis);
+  return ((nz + zt - 1) / zt) * (kpad / yg::i8::kKt) * (int64_t)yg::i8::kBBlock;
+}
+
+extern "C" int rr_slice_g_i8(const double* g, const int* row_exp, int64_t npos, int64_t kpad,
+                             void* g_digits, rr_stream_t stream) {
+  if (!g || !row_exp || !g_digits || npos < yg::kTileM || npos % yg::kTileM) return RR_EINVAL;
+  if (kpad < yg::kKpadAlign || kpad % yg::kKpadAlign || kpad / yg::i8::kKt > 65535) return RR_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(g_digits) & 15) != 0) return RR_EINVAL;
+  const int64_t nchunk = kpad / yg::i8::kKt;
+  dim3 grid((unsigned)(npos / yg::kTileM), (unsigned)nchunk);
+  yg::i8::slice_g_kernel<<<grid, yg::kTileM * yg::i8::kNkg, 0, (cudaStream_t)stream>>>(
+      g, row_exp, npos, nchunk, (unsigned char*)g_digits);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_slice_basis_i8(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
+                                 int basis_stride, int64_t kpad, const int* col_exp,
+                                 void* basis_digits, rr_stream_t stream) {
+  if (!basis || !col_exp || !basis_digits || nz < 0 || nz > INT_MAX || pix_stride < 1)
+    return RR_EINVAL;
+  if (nbasis < 1 || nbasis > RR_MAX_NBASIS || basis_stride < nbasis) return RR_EINVAL;
+  if (kpad < pix_stride || kpad % yg::kKpadAlign || kpad / yg::i8::kKt > 65535) return RR_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(basis_digits) & 15) != 0) return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  const int zt = yg::i8::zt_of(nbasis);
+  const int64_t nchunk = kpad / yg::i8::kKt;
+  dim3 grid((unsigned)((nz + zt - 1) / zt), (unsigned)nchunk);
+  yg::i8::slice_basis_kernel<<<grid, yg::i8::kN * yg::i8::kNkg, 0, (cudaStream_t)stream>>>(
+      basis, (int)nz, pix_stride, nbasis, basis_stride, col_exp, nchunk,
+      (unsigned char*)basis_digits);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+
+extern "C" int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t kpad,
+                           const void* basis_digits, const int* col_exp, int64_t nz, int nbasis,
+                           double* y, int* status, rr_stream_t stream) {
+  if (!g_digits || !row_exp || !basis_digits || !col_exp || !y) return RR_EINVAL;
+  if (npos < yg::kTileM || npos % yg::kTileM || nz < 0 || nz > INT_MAX) return RR_EINVAL;
+  if (nbasis < 1 || nbasis > RR_MAX_NBASIS) return RR_EINVAL;
+  if (kpad < yg::kKpadAlign || kpad % yg::kKpadAlign) return RR_EINVAL;
+  // exact int32 accumulation: |digit| <= 64, at most 7 products per
+  // accumulator and pixel
+  if (kpad > 65536) return RR_ENOTSUP;
+  if (((reinterpret_cast<uintptr_t>(g_digits) | reinterpret_cast<uintptr_t>(basis_digits)) & 15) != 0)
+    return RR_EINVAL;
+  if (nz == 0) return RR_OK;
+  yg::i8::Params p;
+  p.ga = (const unsigned char*)g_digits;
+  p.tb = (const unsigned char*)basis_digits;
+  p.row_exp = row_exp;
+  p.col_exp = col_exp;
+  p.y = y;
+  p.npos = npos;
+  p.nchunk = kpad / yg::i8::kKt;
+  p.nz = (int)nz;
+  p.nbasis = nbasis;
+  p.zt = yg::i8::zt_of(nbasis);
+  p.status = status;
+  const size_t smem = (size_t)yg::i8::kStages * yg::i8::kStageBytes;
+  RR_CUDA_TRY(cudaFuncSetAttribute(yg::i8::ygemm_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((unsigned)(npos / yg::kTileM), (unsigned)((nz + p.zt - 1) / p.zt));
+  yg::i8::ygemm_kernel<<<grid, yg::kThreads, smem, (cudaStream_t)stream>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
 }

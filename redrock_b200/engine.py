@@ -201,18 +201,26 @@ class DeviceBasis:
         z = np.zeros(nz) if redshifts is None else redshifts
         return cls(basis, layout, nb, z, **kw)
 
-    def col_exp(self, stream=None):
-        """Power-of-two exponents of each (z, basis) column's max |value|
-        (the integer tensor-core y variant's column scales), cached."""
-        if getattr(self, "_col_exp", None) is None:
-            L = _lib.lib()
-            ce = torch.empty(max(self.nz * self.nbasis, 1), dtype=torch.int32,
-                             device=self.basis.device)
-            rc = L.rr_basis_col_exp(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
-                                    self.stride, ptr(ce), stream_handle(stream))
-            _lib.check(rc, "rr_basis_col_exp")
-            self._col_exp = ce
-        return self._col_exp
+    def i8_digits(self, kpad, stream=None):
+        """(digit planes, column exponents) of this basis for the exact
+        tensor-core y (rr_basis_col_exp + rr_slice_basis_i8), cached."""
+        cached = getattr(self, "_i8", None)
+        if cached is not None and cached[0] == kpad:
+            return cached[1], cached[2]
+        L = _lib.lib()
+        sh = stream_handle(stream)
+        dev = self.basis.device
+        ce = torch.empty(max(self.nz * self.nbasis, 1), dtype=torch.int32, device=dev)
+        rc = L.rr_basis_col_exp(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
+                                self.stride, ptr(ce), sh)
+        _lib.check(rc, "rr_basis_col_exp")
+        nbytes = int(L.rr_ygemm_i8_basis_bytes(self.nz, self.nbasis, kpad))
+        digits = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
+        rc = L.rr_slice_basis_i8(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
+                                 self.stride, kpad, ptr(ce), ptr(digits), sh)
+        _lib.check(rc, "rr_slice_basis_i8")
+        self._i8 = (kpad, digits, ce)
+        return digits, ce
 
     def data_dict(self, as_numpy=True):
         """redrock's DistTemplate.local.data view: dict[wavehash] -> (nz, npix, nb)."""
@@ -304,10 +312,16 @@ class TargetBatch:
         self.first = np.asarray(first, dtype=np.int64)
         self.rows = np.full(self.nblock * _lib.LANES, -1, dtype=np.int32)
         self.rows[:self.ntarget] = np.arange(self.ntarget, dtype=np.int32)
-        self.rdata = _concat([np.asarray(d, dtype=np.float64).ravel() for d in rdata], np.float64)
+        # the large arrays are gathered straight into pinned host memory (when
+        # a GPU is present), so their upload needs no second staging copy
+        self._pinned = {}
+        self.rdata = _concat([np.asarray(d, dtype=np.float64).ravel() for d in rdata], np.float64,
+                             self._pinned, "rdata")
         self.roffs = _concat([np.asarray(o, dtype=np.int32) for o in roffs], np.int32)
-        self.ivar = _concat([np.asarray(v, dtype=np.float64) for v in ivar], np.float64)
-        self.flux = _concat([np.asarray(v, dtype=np.float64) for v in flux], np.float64)
+        self.ivar = _concat([np.asarray(v, dtype=np.float64) for v in ivar], np.float64,
+                            self._pinned, "ivar")
+        self.flux = _concat([np.asarray(v, dtype=np.float64) for v in flux], np.float64,
+                            self._pinned, "flux")
 
     def host_arrays(self):
         return (self.descs, self.segs_bytes, self.first, self.rows, self.rdata, self.roffs,
@@ -321,9 +335,19 @@ class TargetBatch:
         return DeviceTargetBatch(self)
 
 
-def _concat(parts, dtype):
+def _concat(parts, dtype, pinned=None, name=None):
+    """Concatenate 1-D arrays; into a pinned host tensor (kept in
+    pinned[name]) when pinned is given, the result is >= 1 MB and a GPU is
+    present."""
     n = sum(p.size for p in parts)
-    out = np.empty(n, dtype=dtype)
+    if (pinned is not None and n * np.dtype(dtype).itemsize >= (1 << 20)
+            and torch.cuda.is_available()):
+        t = torch.empty(n, dtype=torch.from_numpy(np.empty(0, dtype=dtype)).dtype,
+                        pin_memory=True)
+        pinned[name] = t
+        out = t.numpy()
+    else:
+        out = np.empty(n, dtype=dtype)
     i = 0
     for p in parts:
         out[i:i + p.size] = p
@@ -340,10 +364,16 @@ class DeviceTargetBatch:
         self.segs = to_device(batch.segs_bytes, torch.uint8)
         self.first = to_device(batch.first, torch.int64)
         self.rows = to_device(batch.rows, torch.int32)
-        self.rdata = to_device(batch.rdata)
+        pinned = getattr(batch, "_pinned", {})
+        dev = device()
+
+        def up(name, arr, dtype=torch.float64):
+            t = pinned.get(name)
+            return t.to(dev, non_blocking=True) if t is not None else to_device(arr, dtype)
+        self.rdata = up("rdata", batch.rdata)
         self.roffs = to_device(batch.roffs, torch.int32)
-        self.ivar = to_device(batch.ivar)
-        self.flux = to_device(batch.flux)
+        self.ivar = up("ivar", batch.ivar)
+        self.flux = up("flux", batch.flux)
 
 
 class TargetPack:
@@ -380,8 +410,11 @@ class TargetPack:
         self._status.check("rr_pack_targets")
 
     def scan_targets_struct(self):
-        arr = (_lib.SegmentDesc * len(self.segs))(*self.segs)
-        self._segarr = arr
+        # one segment array per pack: every struct handed out points at it,
+        # so it must outlive all of them
+        if getattr(self, "_segarr", None) is None:
+            self._segarr = (_lib.SegmentDesc * len(self.segs))(*self.segs)
+        arr = self._segarr
         return _lib.ScanTargets(ptr(self.rw), ptr(self.fwf), ptr(self.wsum), ptr(self.rows),
                                 ctypes.cast(arr, ctypes.c_void_p).value, self.nblock,
                                 len(self.segs), self.npix_block)
@@ -397,8 +430,10 @@ class ScanResult:
 
 class YGemm:
     """y = Tb^T W f of every (target, z) on the tensor cores: G = R^T W f of
-    a target pack (rr_pack_g) and, per template, Y = G^T . basis
-    (rr_ygemm).  variant: "bf16x3", "tf32x3" or "int8x7"."""
+    a target pack (rr_pack_g) and, per template, Y = G^T . basis.
+    variant: "int8x7" (exact Ozaki scheme; rr_slice_g_i8 once here, the
+    basis digits cached on the DeviceBasis, rr_ygemm_i8), or the FP32-
+    accumulated "bf16x3" / "tf32x3" (rr_ygemm)."""
 
     def __init__(self, pack, variant, stream=None, status=None):
         L = _lib.lib()
@@ -410,36 +445,79 @@ class YGemm:
         self.npos = round_up(pack.nblock * _lib.LANES, 128)
         self.kpad = int(L.rr_ygemm_kpad(pack.layout.pix_stride))
         self.g = torch.empty((self.kpad, self.npos), dtype=torch.float64, device=dev)
-        self.row_exp = (torch.empty(self.npos, dtype=torch.int32, device=dev)
-                        if self.variant == _lib.RR_YGEMM_INT8X7 else None)
+        exact = self.variant == _lib.RR_YGEMM_INT8X7
+        self.row_exp = torch.empty(self.npos, dtype=torch.int32, device=dev) if exact else None
         self._status = status or StatusWord(dev)
         tgs = pack.scan_targets_struct()
+        sh = stream_handle(stream)
         rc = L.rr_pack_g(ctypes.byref(tgs), pack.layout.pix_stride, self.kpad, self.npos,
-                         ptr(self.g), ptr(self.row_exp), self._status.ptr, stream_handle(stream))
+                         ptr(self.g), ptr(self.row_exp), self._status.ptr, sh)
         _lib.check(rc, "rr_pack_g")
+        self.g_digits = None
+        if exact:
+            nbytes = int(L.rr_ygemm_i8_g_bytes(self.npos, self.kpad))
+            self.g_digits = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            rc = L.rr_slice_g_i8(ptr(self.g), ptr(self.row_exp), self.npos, self.kpad,
+                                 ptr(self.g_digits), sh)
+            _lib.check(rc, "rr_slice_g_i8")
 
     def y(self, basis, stream=None):
         """[npos][nz][nbasis] y of every packed target against one basis."""
         L = _lib.lib()
+        sh = stream_handle(stream)
         y = torch.empty((self.npos, basis.nz, basis.nbasis), dtype=torch.float64,
                         device=self.g.device)
-        col = basis.col_exp(stream) if self.variant == _lib.RR_YGEMM_INT8X7 else None
-        rc = L.rr_ygemm(self.variant, ptr(self.g), ptr(self.row_exp), self.npos, self.kpad,
-                        ptr(basis.basis), basis.nz, basis.layout.pix_stride, basis.nbasis,
-                        basis.stride, ptr(col), ptr(y), self._status.ptr, stream_handle(stream))
-        _lib.check(rc, "rr_ygemm")
+        if self.variant == _lib.RR_YGEMM_INT8X7:
+            digits, col = basis.i8_digits(self.kpad, stream)
+            rc = L.rr_ygemm_i8(ptr(self.g_digits), ptr(self.row_exp), self.npos, self.kpad,
+                               ptr(digits), ptr(col), basis.nz, basis.nbasis, ptr(y),
+                               self._status.ptr, sh)
+            _lib.check(rc, "rr_ygemm_i8")
+        else:
+            rc = L.rr_ygemm(self.variant, ptr(self.g), self.npos, self.kpad, ptr(basis.basis),
+                            basis.nz, basis.layout.pix_stride, basis.nbasis, basis.stride,
+                            ptr(y), self._status.ptr, sh)
+            _lib.check(rc, "rr_ygemm")
         return y
 
 
-def run_fused(pack, bases, stream=None, status=None, ygemm="fp64"):
-    """One persistent launch over every (target, template, z).  ygemm other
-    than "fp64" computes y on the tensor cores first (YGemm)."""
+# y = Tb^T W f of the fused scan: "int8x7" (tensor-core GEMM, exact integer
+# accumulation; the fastest), "fp64" (summed inside the scan), or the
+# FP32-accumulated "bf16x3" / "tf32x3" (precision-study variants: they miss
+# |dchi2| <= 1e-3 at DESI S/N)
+DEFAULT_Y = "int8x7"
+_I8_MAX_KPAD = 65536  # int32 headroom of rr_ygemm_i8
+
+
+def resolve_y(ygemm, layout):
+    """The y variant actually used: the default unless given; int8x7 falls
+    back to fp64 when the padded pixel count exceeds its int32 headroom."""
+    v = DEFAULT_Y if ygemm is None else ygemm
+    if v == "int8x7" and int(_lib.lib().rr_ygemm_kpad(layout.pix_stride)) > _I8_MAX_KPAD:
+        v = "fp64"
+    return v
+
+
+def _record(ev, stream):
+    if isinstance(stream, torch.cuda.Stream):
+        ev.record(stream)
+    else:
+        ev.record()
+
+
+def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=None):
+    """One persistent launch over every (target, template, z).  ygemm:
+    None (DEFAULT_Y), "fp64", "int8x7", "bf16x3" or "tf32x3"; other than
+    "fp64", y is computed on the tensor cores first (YGemm).  kernel_events:
+    a list that gets a (start, end) CUDA event pair around the scan launches
+    alone (timing)."""
     L = _lib.lib()
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
     tgs = pack.scan_targets_struct()
-    counter = torch.zeros(3, dtype=torch.int32, device=dev)
+    counter = torch.zeros(4, dtype=torch.int32, device=dev)
     st = status or StatusWord(dev)
+    ygemm = resolve_y(ygemm, pack.layout)
     yg = None if ygemm == "fp64" else YGemm(pack, ygemm, stream=stream, status=st)
     for i0 in range(0, len(bases), _lib.MAX_TEMPLATES):
         chunk = list(range(i0, min(len(bases), i0 + _lib.MAX_TEMPLATES)))
@@ -457,9 +535,16 @@ def run_fused(pack, bases, stream=None, status=None, ygemm="fp64"):
                                          ptr(r.penalty) if b.oii is not None else None,
                                          ptr(r.y_ext) if yg is not None else None))
         arr = (_lib.ScanTemplate * len(tms))(*tms)
+        if kernel_events is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            _record(e0, stream)
         rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
                               stream_handle(stream))
         _lib.check(rc, "rr_zscan_fused")
+        if kernel_events is not None:
+            _record(e1, stream)
+            kernel_events.append((e0, e1))
     run_fused.last_counter = counter
     return results, st
 

@@ -97,6 +97,7 @@ def _pack(targets, layout):
 # fused scan
 # ---------------------------------------------------------------------------
 CHUNK_TARGETS = 128   # targets per pipelined chunk (4 target blocks)
+FIRST_CHUNK = 32      # a small first chunk gets the GPU started early
 
 
 def _bases_for(dtemplates, layout):
@@ -111,37 +112,87 @@ def _bases_for(dtemplates, layout):
     return bases
 
 
-def scan_device(targets, dtemplates, chunk=None):
+def _chunk_bounds(n, chunk):
+    if n <= 2 * chunk:
+        return [(0, n)]
+    bounds = [(0, min(FIRST_CHUNK, chunk))]
+    while bounds[-1][1] < n:
+        i0 = bounds[-1][1]
+        bounds.append((i0, min(n, i0 + chunk)))
+    return bounds
+
+
+_side_streams = {}
+
+
+def _side_stream():
+    d = torch.cuda.current_device()
+    if d not in _side_streams:
+        _side_streams[d] = torch.cuda.Stream()
+    return _side_streams[d]
+
+
+class HostResult:
+    """One template's results in pinned host memory (numpy views)."""
+
+    def __init__(self, ntarget, basis):
+        self.t = [torch.empty((ntarget, basis.nz), dtype=torch.float64, pin_memory=True),
+                  torch.empty((ntarget, basis.nz, basis.nbasis), dtype=torch.float64,
+                              pin_memory=True),
+                  torch.empty((ntarget, basis.nz), dtype=torch.float64, pin_memory=True)]
+        self.zchi2, self.zcoeff, self.penalty = (x.numpy() for x in self.t)
+
+
+def scan_device(targets, dtemplates, chunk=None, host=False):
     """Fused scan of every target against every template.
 
-    Returns a list (one entry per template) of device ScanResult objects
-    with zchi2 (T, nz), zcoeff (T, nz, nbasis), penalty (T, nz).  Large
-    target lists are processed in chunks: the host packing and upload of
-    chunk k + 1 run while the GPU scans chunk k.
+    Returns a list (one entry per template) of results with zchi2 (T, nz),
+    zcoeff (T, nz, nbasis), penalty (T, nz): device ScanResult objects, or
+    with host=True HostResult numpy arrays.  Large target lists are
+    processed in chunks (a small first one, then CHUNK_TARGETS): the host
+    packing and upload of chunk k + 1 run while the GPU scans chunk k, and
+    with host=True chunk k's results are copied to pinned host memory on a
+    side stream while chunk k + 1 runs.
     """
     layout = _layout_for(dtemplates[0], targets)
     bases = _bases_for(dtemplates, layout)
     chunk = chunk or CHUNK_TARGETS
-    if len(targets) <= 2 * chunk:
-        pack = _pack(targets, layout)
-        results, st = run_fused(pack, bases)
-        torch.cuda.current_stream().synchronize()
-        st.check("rr_zscan_fused")
-        return results
     from .device import StatusWord
     st = StatusWord()
+    bounds = _chunk_bounds(len(targets), chunk)
+    main = torch.cuda.current_stream()
+    side = _side_stream() if host else None
+    hout = [HostResult(len(targets), b) for b in bases] if host else None
     parts = []
     keep = []
-    for i0 in range(0, len(targets), chunk):
-        sub = targets[i0:i0 + chunk]
-        pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
-                               lambda: TargetPack(TargetBatch(sub, layout).to_device(),
-                                                  status=st))
+    for i0, i1 in bounds:
+        sub = targets[i0:i1]
+        if len(bounds) == 1:
+            pack = _pack(sub, layout)
+        else:
+            pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
+                                   lambda: TargetPack(TargetBatch(sub, layout).to_device(),
+                                                      status=st))
         res, _ = run_fused(pack, bases, status=st)
-        parts.append(res)
-        keep.append(pack)
-    torch.cuda.current_stream().synchronize()
+        keep.append((pack, res))
+        if host:
+            ev = torch.cuda.Event()
+            ev.record(main)
+            side.wait_event(ev)
+            with torch.cuda.stream(side):
+                for h, r in zip(hout, res):
+                    for dst, src in zip(h.t, (r.zchi2, r.zcoeff, r.penalty)):
+                        dst[i0:i1].copy_(src, non_blocking=True)
+        else:
+            parts.append(res)
+    main.synchronize()
+    if host:
+        side.synchronize()
     st.check("rr_zscan_fused")
+    if host:
+        return hout
+    if len(parts) == 1:
+        return parts[0]
     out = []
     for it in range(len(bases)):
         r = parts[0][it]
@@ -152,13 +203,6 @@ def scan_device(targets, dtemplates, chunk=None):
     return out
 
 
-def _to_host(t):
-    """Device tensor -> numpy through a pinned buffer."""
-    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-    h.copy_(t, non_blocking=True)
-    return h
-
-
 def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False):
     """chi2 vs redshift of every target for one template (zscan.py:807)."""
     ntargets = len(target_ids)
@@ -166,10 +210,8 @@ def calc_zchi2(target_ids, target_data, dtemplate, progress=None, use_gpu=False)
     nbasis = dtemplate.template.nbasis
     if ntargets == 0:
         return np.zeros((0, nz)), np.zeros((0, nz, nbasis)), np.zeros((0, nz))
-    res = scan_device(list(target_data), [dtemplate])[0]
-    zchi2, zcoeff, pen = _to_host(res.zchi2), _to_host(res.zcoeff), _to_host(res.penalty)
-    torch.cuda.current_stream().synchronize()
-    zchi2, zcoeff, pen = zchi2.numpy(), zcoeff.numpy(), pen.numpy()
+    res = scan_device(list(target_data), [dtemplate], host=True)[0]
+    zchi2, zcoeff, pen = res.zchi2, res.zcoeff, res.penalty
     if dtemplate.comm is None and progress is not None:
         for _ in range(ntargets):
             progress.put(1)
@@ -195,12 +237,10 @@ def calc_zchi2_targets(targets, templates, mp_procs=1, use_gpu=True):
         sys.stdout.flush()
     if len(tids) == 0:
         return results
-    out = scan_device(data, list(templates))
-    host = [(_to_host(r.zchi2), _to_host(r.zcoeff), _to_host(r.penalty)) for r in out]
-    torch.cuda.current_stream().synchronize()
-    for t, (zc, co, pe) in zip(templates, host):
+    out = scan_device(data, list(templates), host=True)
+    for t, r in zip(templates, out):
         ft = t.template.full_type
-        zc, co, pe = zc.numpy(), co.numpy(), pe.numpy()
+        zc, co, pe = r.zchi2, r.zcoeff, r.penalty
         for i, tid in enumerate(tids):
             results.setdefault(tid, {})[ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
                                     zcoeff=co[i])

@@ -5,9 +5,10 @@ Tolerances (FP64 everywhere on the GPU):
     output and the oracle's);
   * IGM transmission: relative 1e-13 (CUDA pow/exp vs libm, <= 2 ulp each);
   * chi2: |dchi2| <= 1e-3 absolute (the acceptance bar) and also 2e-5
-    absolute, the fused kernel's own error budget (normal-equation chi2 is
-    kept only when its rounding-error bound is below 1e-5, else the direct
-    residual is summed); identical argmin per target;
+    absolute, the accuracy the fused kernel reaches on these fixtures
+    (normal-equation chi2 is kept only when its rounding-error bound, about
+    ten times the actual error, is below 1e-4; else the direct residual is
+    summed); identical argmin per target;
   * coefficients: |dc| <= 1e-5 * max|c| per (target, z).
 """
 
@@ -301,7 +302,8 @@ def test_best_z_recovers_truth_high_snr(rr):
 
 def test_chunked_pipeline_bit_identical(rr):
     """Pipelined target chunks give bit-identical results to one launch
-    (each lane's sums do not depend on the block it sits in)."""
+    (each lane's sums do not depend on the block it sits in), on the device
+    and through the pinned host copies."""
     from redrock_b200 import zscan
     tg = synth.make_targets(70, seed=71, mask_range=(0.0, 0.4), drop_camera_frac=0.1)
     T, TM = rr["targets"], rr["templates"]
@@ -310,9 +312,14 @@ def test_chunked_pipeline_bit_identical(rr):
     dts = [TM.DistTemplate(TM.from_synth(ts), dwave) for ts in synth.template_set(zsub=151)]
     a = zscan.scan_device(rtg, dts, chunk=1000)
     b = zscan.scan_device(rtg, dts, chunk=16)
-    for x, y in zip(a, b):
+    h = zscan.scan_device(rtg, dts, chunk=16, host=True)
+    for x, y, z in zip(a, b, h):
         assert torch_equal(x.zchi2, y.zchi2) and torch_equal(x.zcoeff, y.zcoeff)
         assert torch_equal(x.penalty, y.penalty)
+        # results copied to pinned host memory chunk by chunk on a side stream
+        assert np.array_equal(z.zchi2, x.zchi2.cpu().numpy())
+        assert np.array_equal(z.zcoeff, x.zcoeff.cpu().numpy())
+        assert np.array_equal(z.penalty, x.penalty.cpu().numpy())
 
 
 def torch_equal(a, b):

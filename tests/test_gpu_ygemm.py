@@ -104,6 +104,50 @@ def test_ygemm_matches_fp64_product(variant):
         assert float(err.max()) <= tol, (variant, b.nbasis, float(err.max()))
 
 
+def test_i8_digits_edge_values():
+    """Entries at and just below a power of two (where the leading base-128
+    digit reaches +-64) and of both signs: the error stays within the
+    scheme's bound K 2^-45 2^(e_t + e_n) (rounding to 49-bit integers plus
+    the dropped digit products of order >= 7).  A lost carry would be an
+    error of the order of 2^(e_t + e_n) itself."""
+    import torch
+    from redrock_b200 import _lib
+    from redrock_b200.device import ptr
+    from redrock_b200.engine import YGemm
+    tg, tset, layout, pack, bases = _case(33, 401, seed=34)
+    yg = YGemm(pack, "int8x7")
+    rng = np.random.default_rng(5)
+    g = yg.g.cpu().numpy()
+    npos = pack.nblock * 32
+    for t in range(npos):
+        e = int(rng.integers(-20, 20))
+        q = rng.choice(layout.pix_stride, size=6, replace=False)
+        g[q[0], t] = np.ldexp(1.0 - 2.0 ** -40, e)
+        g[q[1], t] = -np.ldexp(1.0 - 2.0 ** -40, e)
+        g[q[2], t] = np.ldexp(0.996, e)
+        g[q[3], t] = -np.ldexp(0.9961, e)
+        g[q[4], t] = np.ldexp(0.5, e)
+        g[q[5], t] = -np.ldexp(0.75, e)
+    gt = torch.as_tensor(g, device=yg.g.device)
+    yg.g.copy_(gt)
+    m = np.abs(g).max(axis=0)
+    et = np.where(m > 0, np.frexp(m)[1], 0)
+    ex = np.where(m > 0, et + 4096, 0).astype(np.int32)
+    yg.row_exp.copy_(torch.as_tensor(ex, device=yg.g.device))
+    L = _lib.lib()
+    assert L.rr_slice_g_i8(ptr(yg.g), ptr(yg.row_exp), yg.npos, yg.kpad, ptr(yg.g_digits),
+                           None) == 0
+    for b in bases:
+        y = yg.y(b)
+        t = b.basis[:, :, :b.nbasis]
+        ref = torch.einsum("qp,zqi->pzi", gt[:layout.pix_stride], t)
+        err = (y - ref).abs()[:npos].cpu().numpy()
+        ce = b.i8_digits(yg.kpad)[1].cpu().numpy()[:b.nz * b.nbasis].reshape(b.nz, b.nbasis)
+        en = np.where(ce > 0, ce - 4096, 0)
+        bound = yg.kpad * np.ldexp(1.0, et[:npos, None, None] + en[None] - 45)
+        assert np.all(err <= bound), float(np.max(err / bound))
+
+
 def test_fused_with_tensor_core_y_vs_oracle():
     from redrock_b200.engine import run_fused
     tg, tset, layout, pack, bases = _case(37, 97, seed=33)
