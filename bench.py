@@ -168,11 +168,12 @@ def measure_fp64_peak(L, torch):
     return best
 
 
-def traffic_from_profile():
+def traffic_from_profile(workload, reduced):
     """DRAM bytes per launch of the fused scan kernel from the committed ncu
-    summary (profiles/zscan_fused_traffic.json), if present."""
+    summary (profiles/zscan_fused_traffic.json), for the workload it was
+    captured on (desi500 at full size) only."""
     p = os.path.join(ROOT, "profiles", "zscan_fused_traffic.json")
-    if os.path.exists(p):
+    if workload == "desi500" and not reduced and os.path.exists(p):
         try:
             return json.load(open(p)).get("bytes_per_launch_full_workload")
         except Exception:
@@ -370,7 +371,8 @@ def run_ours(args, rank, world, local_rank):
                    "cuda_graph": bool(args.graph),
                    "y_term": args.ygemm},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic_from_profile(),
+                     "frac": achieved / peak, "traffic": traffic_from_profile(args.workload,
+                                                                  bool(args.ntargets or args.zsub)),
                      "kernel": "zscan_fused_kernel",
                      "kernel_ms": kernel_ms, "flops_per_launch": fused_flops,
                      "flops_note": ("FP64 FLOPs of F(n,P) done by this kernel"

@@ -656,32 +656,40 @@ __global__ void __launch_bounds__(256) pack_g_kernel(const __grid_constant__ GPa
   }
 }
 
-// biased exponent of max_q |T[z][q][i]| per (z, i); one block per z
+// biased exponent of max_q |T[z][q][i]| per (z, i); one block per z, each
+// thread keeps the running maxima of its rows (read once, contiguously)
 __global__ void __launch_bounds__(256) col_exp_kernel(const double* __restrict__ basis,
                                                       int64_t pix_stride, int nbasis,
                                                       int basis_stride, int* col_exp) {
-  __shared__ double s_m[256];
+  __shared__ double s_m[RR_MAX_NBASIS][256];
   const int64_t z = blockIdx.x;
   const double* tz = basis + z * pix_stride * basis_stride;
-  for (int i = 0; i < nbasis; ++i) {
-    double m = 0.0;
-    for (int64_t q = threadIdx.x; q < pix_stride; q += blockDim.x)
-      m = fmax(m, fabs(tz[q * basis_stride + i]));
-    s_m[threadIdx.x] = m;
+  double m[RR_MAX_NBASIS];
+#pragma unroll
+  for (int i = 0; i < RR_MAX_NBASIS; ++i) m[i] = 0.0;
+  for (int64_t q = threadIdx.x; q < pix_stride; q += blockDim.x) {
+    const double* row = tz + q * basis_stride;
+#pragma unroll
+    for (int i = 0; i < RR_MAX_NBASIS; ++i)
+      if (i < nbasis) m[i] = fmax(m[i], fabs(row[i]));
+  }
+#pragma unroll
+  for (int i = 0; i < RR_MAX_NBASIS; ++i) s_m[i][threadIdx.x] = m[i];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int i = 0; i < nbasis; ++i)
+        s_m[i][threadIdx.x] = fmax(s_m[i][threadIdx.x], s_m[i][threadIdx.x + w]);
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) s_m[threadIdx.x] = fmax(s_m[threadIdx.x], s_m[threadIdx.x + w]);
-      __syncthreads();
+  }
+  if (threadIdx.x < nbasis) {
+    int e = 0;
+    const double mx = s_m[threadIdx.x][0];
+    if (mx > 0.0) {
+      frexp(mx, &e);
+      e += kExpBias;
     }
-    if (threadIdx.x == 0) {
-      int e = 0;
-      if (s_m[0] > 0.0) {
-        frexp(s_m[0], &e);
-        e += kExpBias;
-      }
-      col_exp[z * nbasis + i] = e;
-    }
-    __syncthreads();
+    col_exp[z * nbasis + threadIdx.x] = e;
   }
 }
 
