@@ -178,7 +178,30 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ahead, s_ahead, sb);
     const bool ok = mbar_wait(&sb.full[s], uses.parity(s), p.status);
     uses.bump(s);
-    if (active && ok) {
+    if (active && ok && RESID) {
+      const double* rws = sb.rw(s) + lane;
+      const double* ts = sb.t(s) + warp * kWin * stride;
+      // model = R (T c): T c once per basis row of the window (n FMAs), then
+      // the 11-tap band per pixel -- the coefficients are known here, so the
+      // residual needs no full R.T product
+      double tc[kWin];
+#pragma unroll
+      for (int r = 0; r < kWin; ++r) {
+        const double* trow = ts + r * stride;
+        double v = 0.0;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) v = fma(trow[b], c[b], v);
+        tc[r] = v;
+      }
+#pragma unroll
+      for (int q = 0; q < kChunk; ++q) {
+        double mi = 0.0;
+#pragma unroll
+        for (int k = 0; k < kBand; ++k) mi = fma(rws[(q * RR_RW + k) * RR_LANES], tc[q + k], mi);
+        const double res = rws[(q * RR_RW + kBand) * RR_LANES] - mi;
+        acc = fma(res, res, acc);
+      }
+    } else if (active && ok) {
       const double* rws = sb.rw(s) + lane;
       const double* ts = sb.t(s) + warp * kWin * stride;
       // kPix pixels per step: basis row q + k serves pixel q + i with band
@@ -217,14 +240,8 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
         }
 #pragma unroll
         for (int i = 0; i < kPix; ++i) {
-          const double gi = (RESID || !EXTY) ? rws[((q + i) * RR_RW + kBand) * RR_LANES] : 0.0;
-          if (RESID) {
-            double mi = 0.0;
-#pragma unroll
-            for (int b = 0; b < NB; ++b) mi = fma(tp[i][b], c[b], mi);
-            const double res = gi - mi;
-            acc = fma(res, res, acc);
-          } else {
+          const double gi = !EXTY ? rws[((q + i) * RR_RW + kBand) * RR_LANES] : 0.0;
+          {
             if (!EXTY)
 #pragma unroll
               for (int b = 0; b < NB; ++b) y[b] = fma(gi, tp[i][b], y[b]);

@@ -187,3 +187,30 @@ def test_fused_with_tensor_core_y_vs_oracle():
                 d = np.abs(zc - zc0)
                 assert np.all(np.isfinite(zc))
                 assert np.all(d[ok] <= bound[ok]), float(np.max(d[ok] / bound[ok]))
+
+
+@pytest.mark.parametrize("nb", [3, 7])
+def test_uncommon_nbasis_default_path_vs_oracle(nb):
+    """nbasis outside {4, 5, 10} runs in the second fused instantiation; its
+    y comes from the INT8 GEMM (default path) -- both against the oracle."""
+    from redrock_b200 import targets as T
+    from redrock_b200 import templates as TM
+    from redrock_b200 import zscan
+    gal = synth.template_set(zsub=61, stars=())[0]
+    ts = synth.TemplateSpec("GALAXY", f"nb{nb}", gal.wave, gal.flux[:nb].copy(),
+                            gal.redshifts, gal.igm_model)
+    tg = synth.make_targets(5, seed=40 + nb, mask_range=(0.0, 0.3), drop_camera_frac=0.3)
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    dt = TM.DistTemplate(TM.from_synth(ts), dtg.wavegrids())
+    zc, co, pe = zscan.calc_zchi2([t.targetid for t in tg], dtg.local(), dt)
+    grids = synth.camera_grids()
+    tdata = O.template_basis(ts.wave, ts.flux, ts.redshifts, grids, ts.igm_model)
+    oii = O.oii_template(ts.wave, ts.flux)
+    ospecs = [[O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets)
+               for s in t.spectra] for t in tg]
+    ozc, oco, ope = O.calc_zchi2(ospecs, tdata, len(ts.redshifts), nb, OIItemplate=oii)
+    assert np.max(np.abs(zc - ozc)) <= 2e-5
+    np.testing.assert_array_equal(np.argmin(zc, axis=1), np.argmin(ozc, axis=1))
+    scale = np.maximum(np.abs(oco).max(axis=-1, keepdims=True), 1e-300)
+    assert np.all(np.abs(co - oco) <= 1e-5 * scale)
+    np.testing.assert_allclose(pe, ope, rtol=1e-8, atol=1e-8)
