@@ -35,6 +35,7 @@
  *   rr_zscan_pairs_grad     adjoint of the pair scan: dchi2/dz,
  *                           d2chi2/dz2, dchi2/dflux (Newton refinement in
  *                           place of fitz.py:255-261's parabola)
+ *   rr_coadd                targets.py:267-373 Target.compute_coadd
  *   rr_pack_g, rr_ygemm,    zscan.py:741-748 (y = Tb^T W f) for every
  *   rr_ygemm_i8 (+ slicing) (target, z) as one tensor-core GEMM per template
  */
@@ -394,6 +395,31 @@ int rr_slice_basis_i8(const double* basis, int64_t nz, int64_t pix_stride, int n
 int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t kpad,
                 const void* basis_digits, const int* col_exp, int64_t nz, int nbasis,
                 double* y, int* status, rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Coadd of a target's exposures per wavelength grid (targets.py:267-373,
+ * Target.compute_coadd with cosmics_nsig = 0).  Per group of nspec
+ * exposures (entries first .. first + nspec - 1 of exp_data / exp_pix):
+ *   ivar_out  = sum ivar;  flux_out = sum ivar flux / sum ivar (sum flux /
+ *   nspec where sum ivar == 0);  rdata_out[d] = sum data[d] ivar / sum ivar
+ *   (/ 1 where 0), DIA data column-indexed, all sums in exposure order, so
+ * the results are bit-identical to redrock's numpy.  exp_data[e] / exp_pix[e]
+ * are offsets of exposure e's (ndiag, npix) data in rdata and its pixels in
+ * ivar / flux.  ngroup <= 65535; max_npix = largest group npix.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int64_t npix;
+  int32_t ndiag;
+  int32_t nspec;     /* exposures in the group (>= 1) */
+  int64_t first;     /* first exposure index of the group */
+  int64_t out_pix;   /* offset of the group's pixels in ivar_out / flux_out */
+  int64_t out_data;  /* offset of its (ndiag, npix) data in rdata_out */
+} rr_coadd_group;
+
+int rr_coadd(const rr_coadd_group* groups /* device */, int64_t ngroup, int64_t max_npix,
+             const int64_t* exp_data, const int64_t* exp_pix, const double* rdata,
+             const double* ivar, const double* flux, double* rdata_out, double* ivar_out,
+             double* flux_out, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * FMA throughput probe (no counterpart in redrock): the roofline

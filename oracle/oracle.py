@@ -14,6 +14,7 @@ Restates, in numpy/scipy (and a small C file for the rebin), redrock 0.22:
                         Calura12/Kamble20 igm.py:321-364)
   DistTemplate basis    py/redrock/templates.py:584-597
   spectral_data         py/redrock/zscan.py:192-209
+  Target.compute_coadd  py/redrock/targets.py:267-373 (cosmics_nsig = 0)
   calc_zchi2_batch      py/redrock/zscan.py:626-781 (CPU branch :747-780)
   solve_matrices (PCA)  py/redrock/zscan.py:1131-1152
   calc_negOII_penalty   py/redrock/zscan.py:783-800
@@ -282,6 +283,41 @@ class OSpectrum:
         self.flux = np.asarray(flux, dtype=np.float64)
         self.ivar = masked_ivar(ivar, rdata, roffsets)
         self.Rcsr = spectrum_rcsr(rdata, roffsets, len(wave))
+
+
+def compute_coadd(exposures):
+    """Target.compute_coadd with cosmics_nsig = 0 (targets.py:267-373).
+
+    exposures: list of (band, wave, flux, ivar, rdata, roffsets), ivar already
+    masked by its own resolution (Spectrum.__init__).  Returns one
+    (band, wave, flux, ivar, rdata, roffsets) per grid in order of first
+    appearance; the coadd's ivar is masked by the coadded resolution
+    (Spectrum.__init__ of the coadd, targets.py:33-35)."""
+    keys = []
+    for e in exposures:
+        if e[0] not in keys:
+            keys.append(e[0])
+    out = []
+    for key in keys:
+        group = [e for e in exposures if e[0] == key]
+        rdiags = None
+        for e in group:
+            if rdiags is None:
+                rdiags = np.asarray(e[4]) * e[3]
+            else:
+                rdiags += np.asarray(e[4]) * e[3]
+        flux = np.array([e[2] for e in group])
+        ivar = np.array([e[3] for e in group])
+        unweighted = np.sum(flux, axis=0)
+        weights = np.sum(ivar, axis=0)
+        weighted = np.sum(ivar * flux, axis=0)
+        isbad = (weights == 0)
+        f = weighted / (weights + isbad)
+        f[isbad] = unweighted[isbad] / len(group)
+        rdiags /= (weights + isbad)
+        out.append((group[-1][0], group[0][1], f, masked_ivar(weights, rdiags, group[0][5]),
+                    rdiags, group[0][5]))
+    return out
 
 
 def spectral_data(spectra):

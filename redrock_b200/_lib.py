@@ -60,6 +60,11 @@ class ScanTemplate(ctypes.Structure):
                 ("zcoeff", c_void_p), ("penalty", c_void_p), ("y_ext", c_void_p)]
 
 
+class CoaddGroup(ctypes.Structure):
+    _fields_ = [("npix", c_int64), ("ndiag", c_int32), ("nspec", c_int32), ("first", c_int64),
+                ("out_pix", c_int64), ("out_data", c_int64)]
+
+
 class ScanTargets(ctypes.Structure):
     _fields_ = [("rw", c_void_p), ("fwf", c_void_p), ("wsum", c_void_p), ("rows", c_void_p),
                 ("segs", c_void_p), ("nblock", c_int32), ("nseg", c_int32),
@@ -126,6 +131,8 @@ _SIGNATURES = {
                                              c_void_p, c_void_p]),
     "rr_negoii_penalty": (c_int, [c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
     "rr_fma_peak": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p]),
+    "rr_coadd": (c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_ygemm_kpad": (c_int64, [c_int64]),
     "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
                           c_void_p, c_void_p, c_void_p]),

@@ -31,6 +31,10 @@ PATCHES = {
     ("archetypes", "trapz_rebin"): ("rebin", "trapz_rebin"),
     ("archetypes", "transmission_Lyman"): ("igm", "transmission_Lyman"),
 }
+# methods of redrock classes: (module, class, method) -> (our module, function)
+METHOD_PATCHES = {
+    ("targets", "Target", "compute_coadd"): ("coadd", "compute_coadd"),
+}
 FUSED_TARGETS = {
     ("zscan", "calc_zchi2_targets"): ("zscan", "calc_zchi2_targets"),
     ("zfind", "calc_zchi2_targets"): ("zscan", "calc_zchi2_targets"),
@@ -62,4 +66,18 @@ def install(redrock_pkg=None, fused_targets=True, modules=None):
         src = importlib.import_module(f"redrock_b200.{ours}")
         setattr(mod, attr, getattr(src, oattr))
         done.append(f"{sub}.{attr}")
+    for (sub, cls, meth), (ours, oattr) in METHOD_PATCHES.items():
+        if modules is not None:
+            mod = modules.get(sub)
+        else:
+            try:
+                mod = importlib.import_module(f"{redrock_pkg.__name__}.{sub}")
+            except Exception:
+                mod = None
+        klass = getattr(mod, cls, None) if mod is not None else None
+        if klass is None or not hasattr(klass, meth):
+            continue
+        src = importlib.import_module(f"redrock_b200.{ours}")
+        setattr(klass, meth, getattr(src, oattr))
+        done.append(f"{sub}.{cls}.{meth}")
     return done

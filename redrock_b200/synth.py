@@ -328,6 +328,31 @@ def make_targets(ntarget, seed=0, template=None, zrange=(0.0, 1.5), amp=1.0,
     return out
 
 
+def multi_exposure_targets(ntarget, seed=0, nexp=(1, 3)):
+    """Targets with 1-3 exposures per camera -- the input of redrock's
+    Target.compute_coadd.  Each exposure has its own resolution width,
+    noise, extra noise on the flux and 5 % random masking; about 1 % of the
+    pixels of each camera are masked in every exposure (the all-masked
+    branch of the coadd)."""
+    rng = np.random.default_rng(seed)
+    base = make_targets(ntarget, seed=seed + 1, mask_frac=0.0)
+    out = []
+    for t in base:
+        tg = TargetSpec(t.targetid, ztrue=t.ztrue)
+        for s in t.spectra:
+            npix = len(s.wave)
+            dead = rng.uniform(size=npix) < 0.01
+            for _ in range(int(rng.integers(nexp[0], nexp[1] + 1))):
+                rdata, roff = resolution_dia(npix, rng.uniform(0.8, 1.2))
+                noise = rng.uniform(0.5, 2.0, size=npix)
+                ivar = 1.0 / noise ** 2
+                ivar[(rng.uniform(size=npix) < 0.05) | dead] = 0.0
+                flux = s.flux + rng.normal(size=npix) * noise
+                tg.spectra.append(SpectrumSpec(s.band, s.wave, flux, ivar, rdata, roff))
+        out.append(tg)
+    return out
+
+
 def make_population(ntarget, seed=0, qso_frac=0.0, snr_range=None, mask_range=None,
                     drop_camera_frac=0.0, transmission=None, first_id=1000):
     """Mixed GALAXY / QSO-like targets, shuffled: a fraction qso_frac drawn

@@ -6,7 +6,8 @@ functions accept either), for use where redrock itself is not installed.
 
   Spectrum          targets.py:18-142  (ivar masking by R row integral
                                         :33-35, wavehash :44-53, Rcsr :85-89)
-  Target            targets.py:145-265 (gpu_spectral_data :256-263)
+  Target            targets.py:145-265 (gpu_spectral_data :256-263),
+                    compute_coadd targets.py:267-373 (redrock_b200.coadd)
   DistTargets       targets.py:390-489 (wavegrids :468-489)
   DistTargetsCopy   targets.py:521-577
   distribute_targets targets.py:492-518, utils.distribute_work utils.py:185-227
@@ -54,12 +55,17 @@ class Target:
         self.spectra = spectra
         self.meta = {} if meta is None else meta
         if coadd:
-            raise NotImplementedError("Target.compute_coadd is host data preparation outside "
-                                      "the scan engine; pass coadded spectra")
+            self.compute_coadd(cache_Rcsr=False, cosmics_nsig=cosmics_nsig)
         self.gpuweights = None
         self.gpuflux = None
         self.gpuwflux = None
+        # redrock takes the bands of the spectra given, before any coadd
         self.bands = [s.band for s in spectra]
+
+    def compute_coadd(self, cache_Rcsr=False, cosmics_nsig=0.):
+        """Per-grid coadd of the exposures on the GPU (targets.py:267-373)."""
+        from .coadd import coadd_targets
+        coadd_targets([self], cache_Rcsr=cache_Rcsr, cosmics_nsig=cosmics_nsig)
 
     def gpu_spectral_data(self):
         """Concatenated (weights, flux, wflux) as CUDA tensors, cached."""

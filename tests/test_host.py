@@ -111,8 +111,13 @@ def test_installer_rebinds_every_import_site():
     mods.setdefault("zfind", types.SimpleNamespace())
     mods["zfind"].calc_zchi2_targets = "original"
     mods["zscan"].calc_zchi2_targets = "original"
+
+    class Target:
+        compute_coadd = "original"
+    mods["targets"] = types.SimpleNamespace(Target=Target)
     done = install(modules=mods)
-    assert len(done) == len(PATCHES) + 2
+    assert len(done) == len(PATCHES) + 3
+    assert Target.compute_coadd.__module__ == "redrock_b200.coadd"
     for sub, attr in PATCHES:
         assert callable(getattr(mods[sub], attr))
     assert mods["fitz"].calc_zchi2_batch.__module__ == "redrock_b200.zscan"

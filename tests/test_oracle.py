@@ -136,3 +136,20 @@ def test_prior_one_singular(golden):
     zc, co, pe = O.calc_zchi2([sp], tdata, len(zb), 10, OIItemplate=O.oii_template(gal.wave, sflux))
     np.testing.assert_array_equal(zc, golden["singular_zchi2"])
     np.testing.assert_array_equal(co, golden["singular_zcoeff"])
+
+
+def test_coadd_oracle_vs_redrock_golden():
+    """The oracle's compute_coadd reproduces redrock's Target(coadd=True)
+    bit for bit (checksums of flux, ivar and resolution data)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "coadd_golden.npz"))
+    tg = synth.multi_exposure_targets(4, seed=61)
+    assert synth.targets_checksum(tg) == str(g["coadd_targets_sha"])
+    for it, t in enumerate(tg):
+        exps = [(s.band, s.wave, s.flux, O.masked_ivar(s.ivar, s.rdata, s.roffsets), s.rdata,
+                 s.roffsets) for s in t.spectra]
+        out = O.compute_coadd(exps)
+        assert len(out) == int(g[f"coadd_{it}_nspec"][1])
+        for j, (band, wave, f, w, rd, ro) in enumerate(out):
+            assert band == str(g[f"coadd_{it}_{j}_band"])
+            assert synth.checksum([f, w, rd]) == str(g[f"coadd_{it}_{j}_sha"])
