@@ -73,8 +73,13 @@ enum rr_igm_model { /* igm.py:367 igm_models */
 
 enum rr_solve_method { /* zscan.py:1107-1203 solve_matrices */
   RR_SOLVE_PCA = 0,        /* linear solve; exactly singular -> HUGE_CHI2 */
-  RR_SOLVE_UNSUPPORTED = 1 /* every z gets HUGE_CHI2 and zero coefficients,
+  RR_SOLVE_UNSUPPORTED = 1, /* every z gets HUGE_CHI2 and zero coefficients,
                               as redrock does for NotImplementedError */
+  RR_SOLVE_NNLS = 2,       /* NMF / NNLS: min ||M c - y||, c >= 0 (scipy nnls
+                              on (M, y), zscan.py:1153-1169); plain path only */
+  RR_SOLVE_BVLS = 3        /* min ||M c - y||, lo <= c <= hi (scipy lsq_linear
+                              method='bvls', zscan.py:1170-1199); plain path
+                              only (rr_zchi2_batch_plain_ex) */
 };
 
 #define RR_HUGE_CHI2 9999999.0   /* zscan.py:18 */
@@ -302,6 +307,19 @@ int rr_pack_band_rows(const rr_spectrum_desc* specs /* device */, int64_t nspec,
                       double* band, int* status, rr_stream_t stream);
 
 size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz, int32_t nbasis);
+
+/* rr_zchi2_batch_plain with the bounds of RR_SOLVE_BVLS: a host array
+ * [2][nbasis] (lower row, then upper; +-INFINITY allowed) or NULL for
+ * (-inf, inf) -- redrock's solver_args['bounds'].  For RR_SOLVE_NNLS and
+ * RR_SOLVE_BVLS chi2 is the direct residual sum w (f - Tb c)^2 (as for
+ * every method of this path); a failed bounded solve (singular free set,
+ * iteration limit) gives HUGE_CHI2 like redrock's caught exception. */
+int rr_zchi2_batch_plain_ex(const double* band, const double* w, const double* wflux,
+                            const double* flux, const int64_t* pix_basis, int64_t npix_total,
+                            const double* basis, int64_t pix_stride, int32_t nz, int32_t nbasis,
+                            int32_t basis_stride, const double* prior, int32_t method,
+                            const double* bounds, double* zchi2, double* zcoeff, void* workspace,
+                            size_t workspace_bytes, int* status, rr_stream_t stream);
 
 int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflux,
                          const double* flux, const int64_t* pix_basis, int64_t npix_total,

@@ -16,7 +16,7 @@ Restates, in numpy/scipy (and a small C file for the rebin), redrock 0.22:
   spectral_data         py/redrock/zscan.py:192-209
   Target.compute_coadd  py/redrock/targets.py:267-373 (cosmics_nsig = 0)
   calc_zchi2_batch      py/redrock/zscan.py:626-781 (CPU branch :747-780)
-  solve_matrices (PCA)  py/redrock/zscan.py:1131-1152
+  solve_matrices        py/redrock/zscan.py:1107-1201 (PCA, NMF/NNLS, BVLS)
   calc_negOII_penalty   py/redrock/zscan.py:783-800
   calc_zchi2            py/redrock/zscan.py:807-889
   calc_zchi2_one        py/redrock/zscan.py:169-190, 213-243
@@ -330,7 +330,32 @@ def solve_pca(M, y):
     return np.linalg.solve(M, y.reshape(y.shape + (1,))).reshape(y.shape)
 
 
-def calc_zchi2_batch(spectra, tdata, weights, flux, wflux, nz, nbasis, method='PCA', prior=None):
+def solve_matrices(M, y, method='PCA', solver_args=None):
+    """solve_matrices, CPU branch (zscan.py:1107-1201): PCA linear solve;
+    NMF / NNLS: scipy.optimize.nnls(M, y); BVLS: lsq_linear(M, y, bounds,
+    method='bvls'); other names: NotImplementedError."""
+    from scipy.optimize import lsq_linear, nnls
+    m = method.upper()
+    if m == 'PCA':
+        return solve_pca(M, y)
+    if m in ('NMF', 'NNLS'):
+        try:
+            return nnls(M, y)[0]
+        except Exception:
+            raise np.linalg.LinAlgError
+    if m == 'BVLS':
+        if solver_args is not None and 'bounds' in solver_args:
+            bounds = solver_args['bounds']
+        else:
+            bounds = np.zeros((2, y.shape[-1]))
+            bounds[0] = -np.inf
+            bounds[1] = np.inf
+        return lsq_linear(M, y, bounds=bounds, method='bvls').x
+    raise NotImplementedError(method)
+
+
+def calc_zchi2_batch(spectra, tdata, weights, flux, wflux, nz, nbasis, method='PCA', prior=None,
+                     solver_args=None):
     zchi2 = np.zeros(nz)
     if weights.sum() == 0:
         zchi2[:] = HUGE_CHI2
@@ -342,12 +367,9 @@ def calc_zchi2_batch(spectra, tdata, weights, flux, wflux, nz, nbasis, method='P
         y = Tb.T.dot(wflux)
         if prior is not None:
             M += prior
-        if method.upper() != 'PCA':
-            zchi2[i] = HUGE_CHI2
-            continue
         try:
-            zcoeff[i, :] = solve_pca(M, y)
-        except np.linalg.LinAlgError:
+            zcoeff[i, :] = solve_matrices(M, y, method, solver_args)
+        except (np.linalg.LinAlgError, NotImplementedError):
             zchi2[i] = HUGE_CHI2
             continue
         model = Tb.dot(zcoeff[i, :])

@@ -15,7 +15,7 @@ LIBPATH = os.path.join(HERE, "librr_b200.so")
 
 RR_OK, RR_EINVAL, RR_ERANGE, RR_ECUDA, RR_ETIMEOUT, RR_ENOTSUP, RR_ESCRATCH = range(7)
 RR_IGM_NONE, RR_IGM_CALURA12, RR_IGM_KAMBLE20, RR_IGM_INOUE14 = range(4)
-RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED = 0, 1
+RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED, RR_SOLVE_NNLS, RR_SOLVE_BVLS = 0, 1, 2, 3
 RR_YGEMM_NONE, RR_YGEMM_BF16X3, RR_YGEMM_TF32X3, RR_YGEMM_INT8X7 = range(4)
 YGEMM_VARIANTS = {"fp64": RR_YGEMM_NONE, "bf16x3": RR_YGEMM_BF16X3, "tf32x3": RR_YGEMM_TF32X3,
                   "int8x7": RR_YGEMM_INT8X7}
@@ -125,6 +125,10 @@ _SIGNATURES = {
                                      c_void_p, c_int64, c_int32, c_int32, c_int32, c_void_p,
                                      c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
                                      c_void_p]),
+    "rr_zchi2_batch_plain_ex": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                        c_void_p, c_int64, c_int32, c_int32, c_int32, c_void_p,
+                                        c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t,
+                                        c_void_p, c_void_p]),
     "rr_zchi2_batch_plain_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_int64, c_void_p, c_int64, c_int32, c_int32,
                                              c_int32, c_void_p, c_int32, c_void_p, c_void_p,

@@ -36,6 +36,7 @@
 #include <mutex>
 
 #include "rr_common.cuh"
+#include "rr_lsq_dev.cuh"
 #include "rr_solve_dev.cuh"
 
 namespace rr {
@@ -64,6 +65,12 @@ static_assert(kChunk % kPix == 0, "chunk must hold whole pixel steps");
 constexpr int kWin = kChunk + 2 * kHalfBand;  // basis rows per chunk window
 constexpr int kStages = RR_SCAN_STAGES;      // copy pipeline depth
 constexpr int kRwChunkDoubles = kChunk * RR_RW * RR_LANES;
+
+// bounds of RR_SOLVE_BVLS (NNLS uses [0, inf) internally)
+struct SolveBounds {
+  double lo[RR_MAX_NBASIS];
+  double hi[RR_MAX_NBASIS];
+};
 
 struct FusedParams {
   rr_scan_targets tg;
@@ -584,7 +591,45 @@ __global__ void plain_solve_kernel(const double* __restrict__ mtri, const double
   bad[z] = ok ? 0 : 1;
 }
 
-// chi2[z] = sum_p w (f - Tb c)^2, deterministic reduction; HUGE if bad.
+// Bounded solves of (M + prior) c ~ y in redrock's scipy sense (min
+// ||(M + P) c - y||, rr_lsq_dev.cuh), one thread per z: RR_SOLVE_NNLS and
+// RR_SOLVE_BVLS.  Separate from the PCA kernel so the common path keeps its
+// registers.
+template <int NB>
+__global__ void plain_lsq_kernel(const double* __restrict__ mtri, const double* __restrict__ y,
+                                 int nz, const double* __restrict__ prior, int method,
+                                 const __grid_constant__ SolveBounds bounds,
+                                 double* __restrict__ zcoeff, unsigned char* __restrict__ bad) {
+  constexpr int kTri = NB * (NB + 1) / 2;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= nz) return;
+  double full[NB][NB], yy[NB], c[NB];
+  for (int i = 0; i < NB; ++i) {
+    yy[i] = y[(int64_t)z * NB + i];
+    for (int j = 0; j <= i; ++j) {
+      double v = mtri[(int64_t)z * kTri + i * (i + 1) / 2 + j];
+      if (prior) v += prior[i * NB + j];
+      full[i][j] = full[j][i] = v;
+    }
+  }
+  bool ok;
+  if (method == RR_SOLVE_NNLS) {
+    ok = nnls_solve<NB>(full, yy, c);
+  } else {
+    double lo[NB], hi[NB];
+    for (int i = 0; i < NB; ++i) {
+      lo[i] = bounds.lo[i];
+      hi[i] = bounds.hi[i];
+    }
+    ok = bvls_solve<NB>(full, yy, lo, hi, c);
+  }
+  for (int i = 0; i < NB; ++i) zcoeff[(int64_t)z * NB + i] = ok ? c[i] : 0.0;
+  bad[z] = ok ? 0 : 1;
+}
+
+// chi2[z] = sum_p w (f - Tb c)^2, deterministic reduction; HUGE if bad
+// (for every method: the constrained solutions are not stationary points of
+// f^T W f - c^T y, so chi2 is always the direct residual here).
 template <int NB>
 __global__ void plain_chi2_kernel(const double* __restrict__ tb, const double* __restrict__ w,
                                   const double* __restrict__ flux, int64_t npix,
@@ -816,8 +861,8 @@ template <int NB>
 static int plain_launch(const double* band, const double* w, const double* wflux,
                         const double* flux, const int64_t* pix_basis, int64_t npix,
                         const double* basis, int64_t pix_stride, int nz, int stride,
-                        const double* prior, int method, double* zchi2, double* zcoeff,
-                        unsigned char* ws, cudaStream_t st) {
+                        const double* prior, int method, const SolveBounds& bounds,
+                        double* zchi2, double* zcoeff, unsigned char* ws, cudaStream_t st) {
   constexpr int kTri = NB * (NB + 1) / 2;
   double* tb = reinterpret_cast<double*>(ws);
   double* mtri = reinterpret_cast<double*>(ws + align256((size_t)nz * npix * NB * sizeof(double)));
@@ -831,21 +876,37 @@ static int plain_launch(const double* band, const double* w, const double* wflux
   RR_CHECK_LAUNCH();
   plain_gram_kernel<NB><<<nz, 128, 0, st>>>(tb, w, wflux, npix, mtri, yv);
   RR_CHECK_LAUNCH();
-  plain_solve_kernel<NB><<<(nz + 127) / 128, 128, 0, st>>>(mtri, yv, nz, prior, method, zcoeff, bad);
+  if (method == RR_SOLVE_NNLS || method == RR_SOLVE_BVLS)
+    plain_lsq_kernel<NB><<<(nz + 63) / 64, 64, 0, st>>>(mtri, yv, nz, prior, method, bounds,
+                                                        zcoeff, bad);
+  else
+    plain_solve_kernel<NB><<<(nz + 127) / 128, 128, 0, st>>>(mtri, yv, nz, prior, method, zcoeff,
+                                                              bad);
   RR_CHECK_LAUNCH();
   plain_chi2_kernel<NB><<<nz, 128, 0, st>>>(tb, w, flux, npix, zcoeff, bad, zchi2);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
 
-extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflux,
+static int plain_entry(const double* band, const double* w, const double* wflux,
                                     const double* flux, const int64_t* pix_basis,
                                     int64_t npix_total, const double* basis, int64_t pix_stride,
                                     int32_t nz, int32_t nbasis, int32_t basis_stride,
                                     const double* prior, int32_t method, double* zchi2,
                                     double* zcoeff, void* workspace, size_t workspace_bytes,
-                                    int* status, rr_stream_t stream) {
+                                    int* status, rr_stream_t stream, const double* bounds) {
   (void)status;
+  SolveBounds sb;
+  for (int i = 0; i < RR_MAX_NBASIS; ++i) {
+    sb.lo[i] = -INFINITY;
+    sb.hi[i] = INFINITY;
+  }
+  if (bounds && nbasis >= 1 && nbasis <= RR_MAX_NBASIS)
+    for (int i = 0; i < nbasis; ++i) {
+      sb.lo[i] = bounds[i];
+      sb.hi[i] = bounds[nbasis + i];
+      if (!(sb.lo[i] <= sb.hi[i])) return RR_EINVAL;
+    }
   if (nz < 0 || npix_total < 1 || nbasis < 1 || nbasis > RR_MAX_NBASIS) return RR_EINVAL;
   if (basis_stride < nbasis) return RR_EINVAL;
   if (nz == 0) return RR_OK;
@@ -858,7 +919,7 @@ extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const d
 #define RR_PLAIN_CASE(N)                                                                          \
   case N:                                                                                         \
     return plain_launch<N>(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz,    \
-                           basis_stride, prior, method, zchi2, zcoeff, ws, st);
+                           basis_stride, prior, method, sb, zchi2, zcoeff, ws, st);
   switch (nbasis) {
     RR_PLAIN_CASE(1)
     RR_PLAIN_CASE(2)
@@ -873,6 +934,30 @@ extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const d
     default: return RR_EINVAL;
   }
 #undef RR_PLAIN_CASE
+}
+
+extern "C" int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflux,
+                                    const double* flux, const int64_t* pix_basis,
+                                    int64_t npix_total, const double* basis, int64_t pix_stride,
+                                    int32_t nz, int32_t nbasis, int32_t basis_stride,
+                                    const double* prior, int32_t method, double* zchi2,
+                                    double* zcoeff, void* workspace, size_t workspace_bytes,
+                                    int* status, rr_stream_t stream) {
+  return plain_entry(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz, nbasis,
+                     basis_stride, prior, method, zchi2, zcoeff, workspace, workspace_bytes,
+                     status, stream, nullptr);
+}
+
+extern "C" int rr_zchi2_batch_plain_ex(const double* band, const double* w, const double* wflux,
+                                       const double* flux, const int64_t* pix_basis,
+                                       int64_t npix_total, const double* basis, int64_t pix_stride,
+                                       int32_t nz, int32_t nbasis, int32_t basis_stride,
+                                       const double* prior, int32_t method, const double* bounds,
+                                       double* zchi2, double* zcoeff, void* workspace,
+                                       size_t workspace_bytes, int* status, rr_stream_t stream) {
+  return plain_entry(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz, nbasis,
+                     basis_stride, prior, method, zchi2, zcoeff, workspace, workspace_bytes,
+                     status, stream, bounds);
 }
 
 // ---------------------------------------------------------------------------

@@ -719,8 +719,10 @@ class PlainTarget:
 _plain_ws = {}
 
 
-def run_plain(pt, basis, prior=None, method=_lib.RR_SOLVE_PCA, stream=None):
-    """zchi2 (nz,), zcoeff (nz, nb) device tensors for one target."""
+def run_plain(pt, basis, prior=None, method=_lib.RR_SOLVE_PCA, stream=None, bounds=None):
+    """zchi2 (nz,), zcoeff (nz, nb) device tensors for one target.  bounds:
+    (lower, upper) of RR_SOLVE_BVLS (scalars or nbasis arrays), else
+    (-inf, inf)."""
     L = _lib.lib()
     dev = device()
     nz, nb = basis.nz, basis.nbasis
@@ -732,12 +734,17 @@ def run_plain(pt, basis, prior=None, method=_lib.RR_SOLVE_PCA, stream=None):
         ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
         _plain_ws[dev.index] = ws
     dprior = None if prior is None else to_device(prior)
-    rc = L.rr_zchi2_batch_plain(ptr(pt.band), ptr(pt.w), ptr(pt.wflux), ptr(pt.flux),
-                                ptr(pt.pix_basis), pt.npix, ptr(basis.basis),
-                                basis.layout.pix_stride, nz, nb, basis.stride, ptr(dprior), method,
-                                ptr(zchi2), ptr(zcoeff), ptr(ws), ws.numel(), pt._status.ptr,
-                                stream_handle(stream))
-    _lib.check(rc, "rr_zchi2_batch_plain")
+    hb = None
+    if bounds is not None:
+        hb = np.ascontiguousarray(np.stack([np.broadcast_to(np.asarray(bounds[0], np.float64), (nb,)),
+                                            np.broadcast_to(np.asarray(bounds[1], np.float64), (nb,))]))
+    rc = L.rr_zchi2_batch_plain_ex(ptr(pt.band), ptr(pt.w), ptr(pt.wflux), ptr(pt.flux),
+                                   ptr(pt.pix_basis), pt.npix, ptr(basis.basis),
+                                   basis.layout.pix_stride, nz, nb, basis.stride, ptr(dprior),
+                                   method, None if hb is None else hb.ctypes.data, ptr(zchi2),
+                                   ptr(zcoeff), ptr(ws), ws.numel(), pt._status.ptr,
+                                   stream_handle(stream))
+    _lib.check(rc, "rr_zchi2_batch_plain_ex")
     return zchi2, zcoeff
 
 

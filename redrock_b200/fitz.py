@@ -128,6 +128,11 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     decisions that follow (ZWARN bits, velocity separation) are the same."""
     if archetype is not None:
         raise NotImplementedError("archetype refinement is not implemented by the GPU engine")
+    from . import _lib
+    from .templates import solve_code
+    if solve_code(template) in (_lib.RR_SOLVE_NNLS, _lib.RR_SOLVE_BVLS):
+        raise NotImplementedError("fine-grid refinement of NMF/NNLS/BVLS templates is not "
+                                  "implemented by the GPU engine (the coarse scan is)")
     redshifts = np.asarray(redshifts)
     nz = 15 if zminfit_npoints is None else zminfit_npoints
     maxv = MAX_VELO_DIFF_STAR if template.template_type == 'STAR' else MAX_VELO_DIFF

@@ -99,12 +99,20 @@ def from_synth(tspec):
 
 
 def solve_code(template):
-    m = str(getattr(template, 'solve_matrices_algorithm', 'PCA')).upper()
+    """rr_solve_method of a template's solve_matrices_algorithm
+    (zscan.py:1107-1203): PCA; NMF / NNLS; BVLS; anything else is
+    redrock's NotImplementedError (HUGE_CHI2)."""
+    return solve_code_of(getattr(template, 'solve_matrices_algorithm', 'PCA'))
+
+
+def solve_code_of(name):
+    m = 'PCA' if name is None else str(name).upper()
     if m == 'PCA':
         return _lib.RR_SOLVE_PCA
-    if m in ('NMF', 'NNLS', 'BVLS'):
-        raise NotImplementedError(f"solve_matrices_algorithm {m} (non-negative / bounded least "
-                                  "squares) is not implemented by the GPU scan engine")
+    if m in ('NMF', 'NNLS'):
+        return _lib.RR_SOLVE_NNLS
+    if m == 'BVLS':
+        return _lib.RR_SOLVE_BVLS
     return _lib.RR_SOLVE_UNSUPPORTED
 
 

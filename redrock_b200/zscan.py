@@ -27,9 +27,9 @@ import torch
 
 from . import _lib
 from .device import to_device, to_numpy
-from .engine import (DeviceBasis, GridLayout, IdCache, PlainTarget, TargetBatch, TargetPack,
-                     run_fused, run_plain)
-from .templates import oii_sums, solve_code
+from .engine import (DeviceBasis, GridLayout, IdCache, PlainTarget, ScanResult, TargetBatch,
+                     TargetPack, run_fused, run_plain)
+from .templates import oii_sums, solve_code, solve_code_of
 
 HUGE_CHI2 = 9999999.0
 
@@ -143,6 +143,43 @@ class HostResult:
         self.zchi2, self.zcoeff, self.penalty = (x.numpy() for x in self.t)
 
 
+# solve methods the fused scan handles; NNLS / BVLS templates (their chi2 is
+# the direct residual of a bounded solve) go through the plain chain
+_FUSED_METHODS = (_lib.RR_SOLVE_PCA, _lib.RR_SOLVE_UNSUPPORTED)
+
+
+def _plain_scan(targets, basis, layout):
+    """One template with a bounded solve: the plain per-target chain for
+    every target (calc_zchi2's loop, zscan.py:853-887), results on the
+    device like the fused scan's."""
+    res = ScanResult(len(targets), basis, torch.device("cuda", torch.cuda.current_device()))
+    for i, t in enumerate(targets):
+        w = np.concatenate([s.ivar for s in t.spectra])
+        if w.sum() == 0:
+            res.zchi2[i] = HUGE_CHI2
+            res.zcoeff[i] = 0.0
+            continue
+        pt = PlainTarget(t.spectra, layout)
+        zc, co = run_plain(pt, basis, method=basis.method)
+        res.zchi2[i] = zc
+        res.zcoeff[i] = co
+        if basis.oii is not None:
+            res.penalty[i] = calc_negOII_penalty_sums(basis.oii, co)
+        pt._status.check("rr_zchi2_batch_plain_ex")
+    return res
+
+
+def calc_negOII_penalty_sums(oii_sums_dev, coeff_t):
+    """calc_negOII_penalty from the per-basis window sums (device)."""
+    from .device import ptr, stream_handle
+    nz, nb = coeff_t.shape
+    out = torch.empty(nz, dtype=torch.float64, device=coeff_t.device)
+    rc = _lib.lib().rr_negoii_penalty(ptr(coeff_t.contiguous()), nz, nb, ptr(oii_sums_dev),
+                                      ptr(out), stream_handle())
+    _lib.check(rc, "rr_negoii_penalty")
+    return out
+
+
 def scan_device(targets, dtemplates, chunk=None, host=False):
     """Fused scan of every target against every template.
 
@@ -155,7 +192,25 @@ def scan_device(targets, dtemplates, chunk=None, host=False):
     side stream while chunk k + 1 runs.
     """
     layout = _layout_for(dtemplates[0], targets)
-    bases = _bases_for(dtemplates, layout)
+    all_bases = _bases_for(dtemplates, layout)
+    plain_ix = [i for i, b in enumerate(all_bases) if b.method not in _FUSED_METHODS]
+    if plain_ix:
+        fused_ix = [i for i in range(len(all_bases)) if i not in plain_ix]
+        out = [None] * len(all_bases)
+        if fused_ix:
+            part = scan_device(targets, [dtemplates[i] for i in fused_ix], chunk=chunk, host=host)
+            for i, r in zip(fused_ix, part):
+                out[i] = r
+        for i in plain_ix:
+            r = _plain_scan(targets, all_bases[i], layout)
+            if host:
+                h = HostResult(len(targets), all_bases[i])
+                for dst, src in zip(h.t, (r.zchi2, r.zcoeff, r.penalty)):
+                    dst.copy_(src)
+                r = h
+            out[i] = r
+        return out
+    bases = all_bases
     chunk = chunk or CHUNK_TARGETS
     from .device import StatusWord
     st = StatusWord()
@@ -265,19 +320,17 @@ def calc_zchi2_batch(spectra, tdata, weights, flux, wflux, nz, nbasis,
     wh = to_numpy(weights)
     if wh.sum() == 0:
         return np.full(nz, HUGE_CHI2), np.zeros((nz, nbasis))
-    method = _lib.RR_SOLVE_PCA
-    if solve_matrices_algorithm is not None:
-        m = str(solve_matrices_algorithm).upper()
-        if m in ('NMF', 'NNLS', 'BVLS'):
-            raise NotImplementedError(f"solve_matrices_algorithm {m} is not implemented by the "
-                                      "GPU scan engine")
-        if m != 'PCA':
-            method = _lib.RR_SOLVE_UNSUPPORTED
+    # solve_matrices (zscan.py:1107-1203): PCA, NMF/NNLS, BVLS (bounds from
+    # solver_args, default unbounded), else NotImplementedError -> HUGE
+    method = solve_code_of(solve_matrices_algorithm)
+    bounds = None
+    if method == _lib.RR_SOLVE_BVLS and solver_args is not None and 'bounds' in solver_args:
+        bounds = solver_args['bounds']
     layout = _plain_layout(spectra, tdata)
     sub = {k: tdata[k] for k in layout.keys}
     basis = DeviceBasis.from_tdata(sub, layout)
     pt = PlainTarget(spectra, layout, weights, flux, wflux)
-    zchi2, zcoeff = run_plain(pt, basis, prior=prior, method=method)
+    zchi2, zcoeff = run_plain(pt, basis, prior=prior, method=method, bounds=bounds)
     torch.cuda.current_stream().synchronize()
     pt._status.check("rr_zchi2_batch_plain")
     if use_gpu:

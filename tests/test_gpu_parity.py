@@ -241,11 +241,6 @@ def test_singular_and_methods(rr, golden):
     np.testing.assert_array_equal(zc, golden["singular_zchi2"])
     np.testing.assert_array_equal(co, golden["singular_zcoeff"])
     np.testing.assert_array_equal(pe, golden["singular_penalty"])
-    # NMF has no GPU solver: a clear error instead of a silent CPU run
-    tm2 = TM.Template(spectype="STAR", subtype="X", redshifts=golden["prior_z"], wave=gal.wave,
-                      flux=gal.flux, method="NMF")
-    with pytest.raises(NotImplementedError):
-        TM.DistTemplate(tm2, dtg.wavegrids())
 
 
 def test_plain_batch_prior_and_one(rr, golden):

@@ -153,3 +153,34 @@ def test_coadd_oracle_vs_redrock_golden():
         for j, (band, wave, f, w, rd, ro) in enumerate(out):
             assert band == str(g[f"coadd_{it}_{j}_band"])
             assert synth.checksum([f, w, rd]) == str(g[f"coadd_{it}_{j}_sha"])
+
+
+def test_bounded_solves_oracle_vs_redrock_golden():
+    """The oracle's NNLS / BVLS branches of solve_matrices reproduce
+    redrock's calc_zchi2_batch and its NMF calc_zchi2."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "lsq_golden.npz"))
+    tg = synth.make_targets(2, seed=11, amp=1.0)
+    assert synth.targets_checksum(tg) == str(g["lsq_targets_sha"])
+    gal = synth.template_set()[0]
+    zb = g["lsq_z"]
+    nb = gal.flux.shape[0]
+    tdata = O.template_basis(gal.wave, gal.flux, zb, synth.camera_grids(), gal.igm_model)
+    lo, hi = g["lsq_bounds"]
+    for it, t in enumerate(tg):
+        sp = [O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets) for s in t.spectra]
+        w, f, wf = O.spectral_data(sp)
+        for name, alg, args in (("nnls", "NNLS", None),
+                                ("bvls", "BVLS", {"bounds": (np.full(nb, lo), np.full(nb, hi))}),
+                                ("bvls_free", "BVLS", None)):
+            zc, co = O.calc_zchi2_batch(sp, tdata, w, f, wf, len(zb), nb, alg, solver_args=args)
+            np.testing.assert_allclose(zc, g[f"lsq_{name}_{it}_zchi2"], rtol=1e-10, atol=1e-8)
+            np.testing.assert_allclose(co, g[f"lsq_{name}_{it}_zcoeff"], rtol=1e-8, atol=1e-10)
+    osp = [[O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets) for s in t.spectra]
+           for t in tg]
+    # redrock caches the [OII] template for GALAXY PCA templates only
+    # (templates.py:170-174), so an NMF template has no penalty
+    zc, co, pe = O.calc_zchi2(osp, tdata, len(zb), nb, "NMF", OIItemplate=None)
+    np.testing.assert_allclose(zc, g["lsq_nmf_zchi2"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(co, g["lsq_nmf_zcoeff"], rtol=1e-8, atol=1e-10)
+    np.testing.assert_allclose(pe, g["lsq_nmf_penalty"], rtol=1e-8, atol=1e-10)
