@@ -160,20 +160,26 @@ __device__ __forceinline__ void write_eval(const rr_scan_template& tm, int64_t r
   }
 }
 
-// One sweep of a tile's pixels through the two-stage copy pipeline.
-// RESID = false: accumulate the Gram matrix m and y.
-// RESID = true:  accumulate the direct residual sum (g - Tb'.c)^2 into acc
-//                (only lanes with do_lane set do the arithmetic).
+// One sweep of a tile's pixels through the two-stage copy pipeline.  Each
+// thread owns ZT redshifts of its target (warp w scans z0 + w ZT + j,
+// j < ZT); its packed-row loads serve all ZT of them.
+// RESID = false: accumulate the Gram matrices m[j] (and y[j] unless EXTY).
+// RESID = true:  accumulate the direct residual sums (g - Tb'.c)^2 into
+//                acc[j] for the (lane, j) with active[j] set.
 // Returns false (uniformly across the CTA) if a copy wait timed out.
-template <int NB, bool RESID, bool EXTY>
+template <int NB, bool RESID, bool EXTY, int ZT>
 __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_template& tm, int block,
-                                      int z0, int nzt, bool active, StageBufs& sb,
-                                      Uses& uses, double (&m)[NB * (NB + 1) / 2],
-                                      double (&y)[NB], const double (&c)[NB], double& acc) {
+                                      int z0, int nzt, const bool (&active)[ZT], StageBufs& sb,
+                                      Uses& uses, double (&m)[ZT][NB * (NB + 1) / 2],
+                                      double (&y)[ZT][NB], const double (&c)[ZT][NB],
+                                      double (&acc)[ZT]) {
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int stride = tm.basis_stride;
   const int64_t nchunk = p.chunks_total;
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < ZT; ++j) any = any || active[j];
   // prologue: the first kStages - 1 chunks in flight
   if (threadIdx.x == 0)
     for (int i = 0; i < kStages - 1 && i < nchunk; ++i) issue_chunk(p, tm, block, z0, nzt, i, i, sb);
@@ -185,78 +191,90 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     if (threadIdx.x == 0 && more) issue_chunk(p, tm, block, z0, nzt, ahead, s_ahead, sb);
     const bool ok = mbar_wait(&sb.full[s], uses.parity(s), p.status);
     uses.bump(s);
-    if (active && ok && RESID) {
+    if (any && ok && RESID) {
       const double* rws = sb.rw(s) + lane;
-      const double* ts = sb.t(s) + warp * kWin * stride;
-      // model = R (T c): T c once per basis row of the window (n FMAs), then
-      // the 11-tap band per pixel -- the coefficients are known here, so the
-      // residual needs no full R.T product
-      double tc[kWin];
 #pragma unroll
-      for (int r = 0; r < kWin; ++r) {
-        const double* trow = ts + r * stride;
-        double v = 0.0;
+      for (int j = 0; j < ZT; ++j) {
+        if (!active[j]) continue;
+        const double* ts = sb.t(s) + (warp * ZT + j) * kWin * stride;
+        // model = R (T c): T c once per basis row of the window (n FMAs),
+        // then the 11-tap band per pixel -- the coefficients are known
+        // here, so the residual needs no full R.T product
+        double tc[kWin];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) v = fma(trow[b], c[b], v);
-        tc[r] = v;
+        for (int r = 0; r < kWin; ++r) {
+          const double* trow = ts + r * stride;
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b) v = fma(trow[b], c[j][b], v);
+          tc[r] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q) {
+          double mi = 0.0;
+#pragma unroll
+          for (int k = 0; k < kBand; ++k)
+            mi = fma(rws[(q * RR_RW + k) * RR_LANES], tc[q + k], mi);
+          const double res = rws[(q * RR_RW + kBand) * RR_LANES] - mi;
+          acc[j] = fma(res, res, acc[j]);
+        }
       }
-#pragma unroll
-      for (int q = 0; q < kChunk; ++q) {
-        double mi = 0.0;
-#pragma unroll
-        for (int k = 0; k < kBand; ++k) mi = fma(rws[(q * RR_RW + k) * RR_LANES], tc[q + k], mi);
-        const double res = rws[(q * RR_RW + kBand) * RR_LANES] - mi;
-        acc = fma(res, res, acc);
-      }
-    } else if (active && ok) {
+    } else if (any && ok) {
       const double* rws = sb.rw(s) + lane;
-      const double* ts = sb.t(s) + warp * kWin * stride;
+      const double* ts = sb.t(s) + warp * ZT * kWin * stride;
       // kPix pixels per step: basis row q + k serves pixel q + i with band
-      // index k - i, so each row is read once for all kPix pixels
+      // index k - i, so each row is read once for all kPix pixels (and the
+      // packed rows once for all ZT redshifts)
 #pragma unroll kQUnroll
       for (int q = 0; q < kChunk; q += kPix) {
-        double tp[kPix][NB];
+        double tp[ZT][kPix][NB];
 #pragma unroll
-        for (int i = 0; i < kPix; ++i)
+        for (int j = 0; j < ZT; ++j)
 #pragma unroll
-          for (int b = 0; b < NB; ++b) tp[i][b] = 0.0;
+          for (int i = 0; i < kPix; ++i)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) tp[j][i][b] = 0.0;
 #pragma unroll
         for (int k = 0; k < kBand + kPix - 1; ++k) {
-          const double* trow = ts + (q + k) * stride;
           double rk[kPix];
 #pragma unroll
           for (int i = 0; i < kPix; ++i)
             rk[i] = (k - i >= 0 && k - i < kBand) ? rws[((q + i) * RR_RW + k - i) * RR_LANES] : 0.0;
 #pragma unroll
-          for (int b = 0; b + 1 < NB; b += 2) {
-            const double2 tv = *reinterpret_cast<const double2*>(trow + b);
+          for (int j = 0; j < ZT; ++j) {
+            const double* trow = ts + (j * kWin + q + k) * stride;
 #pragma unroll
-            for (int i = 0; i < kPix; ++i) {
-              if (k - i >= 0 && k - i < kBand) {
-                tp[i][b] = fma(rk[i], tv.x, tp[i][b]);
-                tp[i][b + 1] = fma(rk[i], tv.y, tp[i][b + 1]);
+            for (int b = 0; b + 1 < NB; b += 2) {
+              const double2 tv = *reinterpret_cast<const double2*>(trow + b);
+#pragma unroll
+              for (int i = 0; i < kPix; ++i) {
+                if (k - i >= 0 && k - i < kBand) {
+                  tp[j][i][b] = fma(rk[i], tv.x, tp[j][i][b]);
+                  tp[j][i][b + 1] = fma(rk[i], tv.y, tp[j][i][b + 1]);
+                }
               }
             }
-          }
-          if (NB & 1) {
-            const double tv = trow[NB - 1];
+            if (NB & 1) {
+              const double tv = trow[NB - 1];
 #pragma unroll
-            for (int i = 0; i < kPix; ++i)
-              if (k - i >= 0 && k - i < kBand) tp[i][NB - 1] = fma(rk[i], tv, tp[i][NB - 1]);
+              for (int i = 0; i < kPix; ++i)
+                if (k - i >= 0 && k - i < kBand) tp[j][i][NB - 1] = fma(rk[i], tv, tp[j][i][NB - 1]);
+            }
           }
         }
 #pragma unroll
         for (int i = 0; i < kPix; ++i) {
           const double gi = !EXTY ? rws[((q + i) * RR_RW + kBand) * RR_LANES] : 0.0;
-          {
+#pragma unroll
+          for (int j = 0; j < ZT; ++j) {
             if (!EXTY)
 #pragma unroll
-              for (int b = 0; b < NB; ++b) y[b] = fma(gi, tp[i][b], y[b]);
+              for (int b = 0; b < NB; ++b) y[j][b] = fma(gi, tp[j][i][b], y[j][b]);
 #pragma unroll
             for (int a = 0; a < NB; ++a)
 #pragma unroll
               for (int b = 0; b <= a; ++b)
-                m[a * (a + 1) / 2 + b] = fma(tp[i][a], tp[i][b], m[a * (a + 1) / 2 + b]);
+                m[j][a * (a + 1) / 2 + b] = fma(tp[j][i][a], tp[j][i][b], m[j][a * (a + 1) / 2 + b]);
           }
         }
       }
@@ -278,74 +296,97 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
   return true;
 }
 
-// EXTY: y comes from tm.y_ext (rr_ygemm) instead of the pixel sweep.
-template <int NB, bool EXTY>
+// EXTY: y comes from tm.y_ext (rr_ygemm) instead of the pixel sweep.  ZT:
+// redshifts per thread; the tile is 32 targets x kWarps ZT redshifts.
+template <int NB, bool EXTY, int ZT>
 __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int block, int z0,
                           StageBufs& sb, Uses& uses, bool& failed) {
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int nzt = min(kWarps, tm.nz - z0);
+  const int nzt = min(kWarps * ZT, tm.nz - z0);
   constexpr int kTri = NB * (NB + 1) / 2;
-  double m[kTri];
-  double y[NB];
-  double c[NB];
-  double acc = 0.0;
+  double m[ZT][kTri];
+  double y[ZT][NB];
+  double c[ZT][NB];
+  double acc[ZT];
+  bool inz[ZT];
 #pragma unroll
-  for (int i = 0; i < kTri; ++i) m[i] = 0.0;
+  for (int j = 0; j < ZT; ++j) {
+    acc[j] = 0.0;
+    inz[j] = warp * ZT + j < nzt;
 #pragma unroll
-  for (int i = 0; i < NB; ++i) y[i] = 0.0;
-  const bool inz = warp < nzt;
+    for (int i = 0; i < kTri; ++i) m[j][i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NB; ++i) y[j][i] = 0.0;
+  }
   const int32_t row = p.tg.rows[block * RR_LANES + lane];
-  if (!sweep<NB, false, EXTY>(p, tm, block, z0, nzt, inz, sb, uses, m, y, c, acc)) {
+  if (!sweep<NB, false, EXTY, ZT>(p, tm, block, z0, nzt, inz, sb, uses, m, y, c, acc)) {
     failed = true;
     return;
   }
-  const bool valid = inz && row >= 0;
-  bool fix = false;
-  double chi2 = 0.0, err = 0.0, wsum = 0.0;
-  if (valid) {
-    const double fwf = p.tg.fwf[block * RR_LANES + lane];
-    wsum = p.tg.wsum[block * RR_LANES + lane];
-    if (EXTY) {
-      const double* ye = tm.y_ext + ((int64_t)(block * RR_LANES + lane) * tm.nz + z0 + warp) * NB;
+  bool fix[ZT];
+  bool anyfix = false;
+  const double fwf = row >= 0 ? p.tg.fwf[block * RR_LANES + lane] : 0.0;
+  const double wsum = row >= 0 ? p.tg.wsum[block * RR_LANES + lane] : 0.0;
 #pragma unroll
-      for (int b = 0; b < NB; ++b) y[b] = ye[b];
+  for (int j = 0; j < ZT; ++j) {
+    fix[j] = false;
+    const int z = z0 + warp * ZT + j;
+    if (inz[j] && row >= 0) {
+      if (EXTY) {
+        const double* ye = tm.y_ext + ((int64_t)(block * RR_LANES + lane) * tm.nz + z) * NB;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) y[j][b] = ye[b];
+      }
+      double chi2 = 0.0, err = 0.0;
+      const bool ok = solve_eval<NB>(tm.method, tm.prior, m[j], y[j], fwf, wsum, c[j], chi2, err);
+      fix[j] = ok && err > kChi2FixTol;
+      write_eval<NB>(tm, row, z, c[j], chi2, wsum);
     }
-    const bool ok = solve_eval<NB>(tm.method, tm.prior, m, y, fwf, wsum, c, chi2, err);
-    fix = ok && err > kChi2FixTol;
-    write_eval<NB>(tm, row, z0 + warp, c, chi2, wsum);
+    anyfix = anyfix || fix[j];
   }
   // ill-conditioned fits: re-evaluate chi2 as the direct weighted residual
   // sum w (f - Tb c)^2 (redrock's own formula, zscan.py:777-780), which does
   // not suffer the cancellation of f^T W f - c^T y
-  if (__syncthreads_or(fix)) {
+  if (__syncthreads_or(anyfix)) {
     if (threadIdx.x == 0 && p.resweep_counter) atomicAdd(p.resweep_counter, 1);
-    const unsigned lanes = __ballot_sync(0xffffffffu, fix);
-    if (lane == 0 && lanes && p.resweep_counter) atomicAdd(p.resweep_counter + 1, __popc(lanes));
-    acc = 0.0;
-    if (!sweep<NB, true, EXTY>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
+    int nfix = 0;
+#pragma unroll
+    for (int j = 0; j < ZT; ++j) nfix += __popc(__ballot_sync(0xffffffffu, fix[j]));
+    if (lane == 0 && nfix && p.resweep_counter) atomicAdd(p.resweep_counter + 1, nfix);
+#pragma unroll
+    for (int j = 0; j < ZT; ++j) acc[j] = 0.0;
+    if (!sweep<NB, true, EXTY, ZT>(p, tm, block, z0, nzt, fix, sb, uses, m, y, c, acc)) {
       failed = true;
       return;
     }
-    if (fix) tm.zchi2[(int64_t)row * tm.nz + z0 + warp] = acc;
+#pragma unroll
+    for (int j = 0; j < ZT; ++j)
+      if (fix[j]) tm.zchi2[(int64_t)row * tm.nz + z0 + warp * ZT + j] = acc[j];
   }
 }
 
-// nbasis values compiled into each instantiation of the fused kernel: the
-// common template sizes (QSO 4, STAR 5, GALAXY 10) share one instantiation
-// so a full GALAXY/QSO/STAR scan is a single persistent launch; the rest go
-// to a second one (keeping all ten in one kernel makes the register
-// allocator spill on every path).
-__host__ __device__ constexpr bool in_common_set(int nb) { return nb == 4 || nb == 5 || nb == 10; }
+// Launch groups of the fused kernel (one instantiation each, so a group's
+// register allocation does not depend on the others): nbasis 10 (GALAXY;
+// one redshift per thread), nbasis 4 and 5 (QSO, STAR; RR_SMALL_ZT
+// redshifts per thread, which share each packed-row load from shared
+// memory -- with one redshift these small bases are bound by shared-memory
+// wavefronts rather than the FP64 pipe), and all other nbasis.
+#ifndef RR_SMALL_ZT
+#define RR_SMALL_ZT 2
+#endif
+__host__ __device__ constexpr int group_of(int nb) {
+  return nb == 10 ? 0 : ((nb == 4 || nb == 5) ? 1 : 2);
+}
+__host__ __device__ constexpr int zt_of_group(int g) { return g == 1 ? RR_SMALL_ZT : 1; }
 
-// EXTY: every template of the launch has y_ext set (rr_ygemm), and the
-// pixel sweep skips y.
-template <bool COMMON, bool EXTY>
+template <int GROUP, bool EXTY>
 __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
+  constexpr int ZT = zt_of_group(GROUP);
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ int64_t s_tile;
   StageBufs sb;
-  sb.stage_doubles = kRwChunkDoubles + kWarps * kWin * p.max_stride;
+  sb.stage_doubles = kRwChunkDoubles + kWarps * ZT * kWin * p.max_stride;
   sb.full = full;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
@@ -366,11 +407,11 @@ __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_k
     const rr_scan_template& tm = p.tm[t];
     const int64_t local = tile - p.tile_start[t];
     const int block = (int)(local % p.tg.nblock);
-    const int z0 = (int)(local / p.tg.nblock) * kWarps;
+    const int z0 = (int)(local / p.tg.nblock) * kWarps * ZT;
 #define RR_TILE_CASE(N)                                                   \
   case N:                                                                 \
-    if constexpr (in_common_set(N) == COMMON) {                           \
-      scan_tile<N, EXTY>(p, tm, block, z0, sb, uses, failed);             \
+    if constexpr (group_of(N) == GROUP) {                                 \
+      scan_tile<N, EXTY, ZT>(p, tm, block, z0, sb, uses, failed);         \
     } else {                                                              \
       set_status(p.status, RR_EINVAL);                                    \
       failed = true;                                                      \
@@ -706,16 +747,18 @@ extern "C" const char* rr_status_string(int status) {
 #undef RR_CHECK_LAUNCH
 #define RR_CHECK_LAUNCH() RR_CUDA_TRY(cudaGetLastError())
 
-static size_t fused_smem_bytes(int max_stride) {
-  return (size_t)kStages * (kRwChunkDoubles + (size_t)kWarps * kWin * max_stride) * sizeof(double);
+static size_t fused_smem_bytes(int max_stride, int zt) {
+  return (size_t)kStages * (kRwChunkDoubles + (size_t)kWarps * zt * kWin * max_stride) *
+         sizeof(double);
 }
 
 // Launch one instantiation of the fused kernel over the templates selected
 // by `pick` (indices into templates), using counter as its tile counter.
-template <bool COMMON, bool EXTY>
+template <int GROUP, bool EXTY>
 static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                         const int* pick, int npick, int* counter, int* resweep, int* status,
                         cudaStream_t stream) {
+  constexpr int kZt = zt_of_group(GROUP);
   FusedParams p;
   memset(&p, 0, sizeof(p));
   p.tg = *targets;
@@ -732,7 +775,7 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   for (int i = 0; i < npick; ++i) {
     const rr_scan_template& tm = templates[pick[i]];
     p.tm[i] = tm;
-    const int64_t zt = (tm.nz + kWarps - 1) / kWarps;
+    const int64_t zt = (tm.nz + kWarps * kZt - 1) / (kWarps * kZt);
     p.tile_start[i + 1] = p.tile_start[i] + zt * targets->nblock;
     max_stride = tm.basis_stride > max_stride ? tm.basis_stride : max_stride;
   }
@@ -742,20 +785,20 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   p.status = status;
   const int64_t ntiles = p.tile_start[npick];
   if (ntiles == 0) return RR_OK;
-  const size_t smem = fused_smem_bytes(max_stride);
-  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<COMMON, EXTY>,
+  const size_t smem = fused_smem_bytes(max_stride, kZt);
+  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<GROUP, EXTY>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 0;
   RR_CUDA_TRY(cudaGetDevice(&dev));
   RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
   int per_sm = 1;
-  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<COMMON, EXTY>,
+  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<GROUP, EXTY>,
                                                             kThreads, smem));
   if (per_sm < 1) per_sm = 1;
   const int64_t slots = (int64_t)nsm * per_sm;
   const int64_t grid = ntiles < slots ? ntiles : slots;
-  zscan_fused_kernel<COMMON, EXTY><<<(unsigned)grid, kThreads, smem, stream>>>(p);
+  zscan_fused_kernel<GROUP, EXTY><<<(unsigned)grid, kThreads, smem, stream>>>(p);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
@@ -777,9 +820,9 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     rw_end = sd.rw_offset + sd.npix_pad > rw_end ? sd.rw_offset + sd.npix_pad : rw_end;
   }
   if (rw_end > targets->npix_block) return RR_EINVAL;
-  // launch groups: (common nbasis, y_ext) -> one persistent launch each
-  int group[4][RR_MAX_TEMPLATES];
-  int ng[4] = {0, 0, 0, 0};
+  // launch groups: (nbasis group, y_ext) -> one persistent launch each
+  int group[6][RR_MAX_TEMPLATES];
+  int ng[6] = {0, 0, 0, 0, 0, 0};
   for (int t = 0; t < ntemplate; ++t) {
     const rr_scan_template& tm = templates[t];
     if (tm.nbasis < 1 || tm.nbasis > RR_MAX_NBASIS || tm.nz < 0) return RR_EINVAL;
@@ -791,19 +834,21 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
       if (targets->segs[s].basis_offset + targets->segs[s].npix_pad + kHalfBand > tm.pix_stride)
         return RR_EINVAL;
     if (tm.y_ext && (reinterpret_cast<uintptr_t>(tm.y_ext) & 7) != 0) return RR_EINVAL;
-    const int gi = (in_common_set(tm.nbasis) ? 0 : 1) + (tm.y_ext ? 2 : 0);
+    const int gi = group_of(tm.nbasis) + (tm.y_ext ? 3 : 0);
     group[gi][ng[gi]++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
   RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, 2 * sizeof(int), st));
-  // each launch resets its counter first (stream order), so common-set
-  // launches share tile_counter[0] and the others tile_counter[1]
+  // each launch resets its counter first (stream order), so the launches
+  // share tile_counter[0]
   int* resweep = tile_counter + 2;
   int rc = RR_OK;
-  if (!rc && ng[0]) rc = launch_fused<true, false>(targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
-  if (!rc && ng[1]) rc = launch_fused<false, false>(targets, templates, group[1], ng[1], tile_counter + 1, resweep, status, st);
-  if (!rc && ng[2]) rc = launch_fused<true, true>(targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
-  if (!rc && ng[3]) rc = launch_fused<false, true>(targets, templates, group[3], ng[3], tile_counter + 1, resweep, status, st);
+  if (!rc && ng[0]) rc = launch_fused<0, false>(targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
+  if (!rc && ng[1]) rc = launch_fused<1, false>(targets, templates, group[1], ng[1], tile_counter, resweep, status, st);
+  if (!rc && ng[2]) rc = launch_fused<2, false>(targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
+  if (!rc && ng[3]) rc = launch_fused<0, true>(targets, templates, group[3], ng[3], tile_counter, resweep, status, st);
+  if (!rc && ng[4]) rc = launch_fused<1, true>(targets, templates, group[4], ng[4], tile_counter, resweep, status, st);
+  if (!rc && ng[5]) rc = launch_fused<2, true>(targets, templates, group[5], ng[5], tile_counter, resweep, status, st);
   return rc;
 }
 
