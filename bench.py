@@ -207,6 +207,17 @@ def run_ours(args, rank, world, local_rank):
 
     ev_kernel = []
 
+    tiles = None
+    tuned = None
+    if args.autotune:
+        # tile shapes picked by the autotuner before anything is timed
+        from redrock_b200 import autotune
+        bases0 = [DeviceBasis.build(s, layout, status=st) for s in srcs]
+        pack0 = TargetPack(dbatch, status=st)
+        tuned = autotune.tune(pack0, bases0)
+        tiles = autotune.tiles_of(tuned)
+        del bases0, pack0
+
     def step(record, ygemm=args.ygemm, sink=ev_fused):
         bases = [DeviceBasis.build(s, layout, status=st) for s in srcs]
         pack = TargetPack(dbatch, status=st)
@@ -215,7 +226,8 @@ def run_ours(args, rank, world, local_rank):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
         res, _ = run_fused(pack, bases, status=st, ygemm=ygemm,
-                           kernel_events=ev_kernel if (record and sink is ev_fused) else None)
+                           kernel_events=ev_kernel if (record and sink is ev_fused) else None,
+                           tiles=tiles)
         if record:
             e1.record()
             sink.append((e0, e1))
@@ -369,7 +381,13 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
                    "parallelism": f"targets sharded {world}-way, no collective",
                    "cuda_graph": bool(args.graph),
-                   "y_term": args.ygemm},
+                   "y_term": args.ygemm,
+                   "tile": {"targets": 32, "redshifts_per_thread": tiles or "default (nbasis 4, 5: 2)",
+                            "warps": 8, "pixels_per_stage": 24,
+                            "chosen_by": ("autotuner (kernel time per candidate, ms: "
+                                          + str({k: v for k, v in tuned.items()
+                                                 if not isinstance(k, int)}) + ")")
+                            if tuned else "defaults"}},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(args.workload,
                                                                   bool(args.ntargets or args.zsub)),
@@ -520,6 +538,8 @@ def main():
     ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
                     help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
                          "summed in the FP64 scan (fp64)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the small-basis tile shapes by timing them before the run")
     ap.add_argument("--ygemm-study", action="store_true",
                     help="also time every y variant once and report its chi2/coeff error")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -225,6 +225,20 @@ typedef struct {
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                    int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
 
+/* Tile shape of the fused scan: a tile is 32 targets (one per lane) x 8 ZT
+ * redshifts (ZT per thread, 8 warps) x 24-pixel stages.  nbasis 10 and the
+ * uncommon sizes run at ZT = 1; nbasis 4 may run at ZT = 1-3 and nbasis 5
+ * at ZT = 1-2 (0 = the default, 2).  rr_zscan_fused uses the defaults; the
+ * host autotuner (redrock_b200/autotune.py) times the choices. */
+typedef struct {
+  int32_t zt_nbasis4;
+  int32_t zt_nbasis5;
+} rr_scan_options;
+
+int rr_zscan_fused_opt(const rr_scan_targets* targets, const rr_scan_template* templates,
+                       int ntemplate, int* tile_counter, const rr_scan_options* opt, int* status,
+                       rr_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * Pair scan: chi2, coefficients and penalty for an arbitrary list of
  * (target, redshift) pairs, the template rebinned (+ IGM) on the fly for

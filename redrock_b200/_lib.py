@@ -65,6 +65,10 @@ class CoaddGroup(ctypes.Structure):
                 ("out_pix", c_int64), ("out_data", c_int64)]
 
 
+class ScanOptions(ctypes.Structure):
+    _fields_ = [("zt_nbasis4", c_int32), ("zt_nbasis5", c_int32)]
+
+
 class ScanTargets(ctypes.Structure):
     _fields_ = [("rw", c_void_p), ("fwf", c_void_p), ("wsum", c_void_p), ("rows", c_void_p),
                 ("segs", c_void_p), ("nblock", c_int32), ("nseg", c_int32),
@@ -108,6 +112,9 @@ _SIGNATURES = {
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_zscan_fused": (c_int, [ctypes.POINTER(ScanTargets), ctypes.POINTER(ScanTemplate), c_int,
                                c_void_p, c_void_p, c_void_p]),
+    "rr_zscan_fused_opt": (c_int, [ctypes.POINTER(ScanTargets), ctypes.POINTER(ScanTemplate),
+                                   c_int, c_void_p, ctypes.POINTER(ScanOptions), c_void_p,
+                                   c_void_p]),
     "rr_pack_rows": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
                              c_void_p, c_void_p, c_int, c_int64, c_void_p, c_void_p, c_void_p,
                              c_void_p, c_void_p, c_void_p]),

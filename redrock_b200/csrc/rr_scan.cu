@@ -366,23 +366,23 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   }
 }
 
-// Launch groups of the fused kernel (one instantiation each, so a group's
-// register allocation does not depend on the others): nbasis 10 (GALAXY;
-// one redshift per thread), nbasis 4 and 5 (QSO, STAR; RR_SMALL_ZT
-// redshifts per thread, which share each packed-row load from shared
-// memory -- with one redshift these small bases are bound by shared-memory
-// wavefronts rather than the FP64 pipe), and all other nbasis.
-#ifndef RR_SMALL_ZT
-#define RR_SMALL_ZT 2
-#endif
+// Launch groups of the fused kernel, one instantiation per (group,
+// redshifts per thread ZT), so a group's register allocation does not
+// depend on the others: nbasis 10 (GALAXY; ZT 1), 4 (QSO; ZT 1-3), 5
+// (STAR; ZT 1-2), all other nbasis (ZT 1).  Several redshifts per thread
+// share each packed-row load from shared memory: with one redshift the
+// small bases are bound by shared-memory wavefronts rather than the FP64
+// pipe.  The ZT of the small groups is a launch option (rr_scan_options),
+// picked by the host autotuner; defaults below.
 __host__ __device__ constexpr int group_of(int nb) {
-  return nb == 10 ? 0 : ((nb == 4 || nb == 5) ? 1 : 2);
+  return nb == 10 ? 0 : (nb == 4 ? 1 : (nb == 5 ? 2 : 3));
 }
-__host__ __device__ constexpr int zt_of_group(int g) { return g == 1 ? RR_SMALL_ZT : 1; }
+constexpr int kNGroups = 4;
+constexpr int kDefaultZt[kNGroups] = {1, 2, 2, 1};
+constexpr int kMaxZt[kNGroups] = {1, 3, 2, 1};
 
-template <int GROUP, bool EXTY>
+template <int GROUP, bool EXTY, int ZT>
 __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_kernel(const __grid_constant__ FusedParams p) {
-  constexpr int ZT = zt_of_group(GROUP);
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ int64_t s_tile;
   StageBufs sb;
@@ -754,11 +754,11 @@ static size_t fused_smem_bytes(int max_stride, int zt) {
 
 // Launch one instantiation of the fused kernel over the templates selected
 // by `pick` (indices into templates), using counter as its tile counter.
-template <int GROUP, bool EXTY>
+template <int GROUP, bool EXTY, int ZT>
 static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                         const int* pick, int npick, int* counter, int* resweep, int* status,
                         cudaStream_t stream) {
-  constexpr int kZt = zt_of_group(GROUP);
+  constexpr int kZt = ZT;
   FusedParams p;
   memset(&p, 0, sizeof(p));
   p.tg = *targets;
@@ -786,25 +786,39 @@ static int launch_fused(const rr_scan_targets* targets, const rr_scan_template* 
   const int64_t ntiles = p.tile_start[npick];
   if (ntiles == 0) return RR_OK;
   const size_t smem = fused_smem_bytes(max_stride, kZt);
-  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<GROUP, EXTY>,
+  RR_CUDA_TRY(cudaFuncSetAttribute(zscan_fused_kernel<GROUP, EXTY, ZT>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 0;
   RR_CUDA_TRY(cudaGetDevice(&dev));
   RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
   int per_sm = 1;
-  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<GROUP, EXTY>,
+  RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<GROUP, EXTY, ZT>,
                                                             kThreads, smem));
   if (per_sm < 1) per_sm = 1;
   const int64_t slots = (int64_t)nsm * per_sm;
   const int64_t grid = ntiles < slots ? ntiles : slots;
-  zscan_fused_kernel<GROUP, EXTY><<<(unsigned)grid, kThreads, smem, stream>>>(p);
+  zscan_fused_kernel<GROUP, EXTY, ZT><<<(unsigned)grid, kThreads, smem, stream>>>(p);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
 
-extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
-                              int ntemplate, int* tile_counter, int* status, rr_stream_t stream) {
+// launch with the runtime ZT of a group (one of its compiled values)
+template <int GROUP, bool EXTY>
+static int launch_group(int zt, const rr_scan_targets* targets, const rr_scan_template* templates,
+                        const int* pick, int npick, int* counter, int* resweep, int* status,
+                        cudaStream_t stream) {
+  if (zt < 1 || zt > kMaxZt[GROUP]) return RR_EINVAL;
+  if constexpr (kMaxZt[GROUP] >= 3)
+    if (zt == 3) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 3 ? 3 : 1)>(targets, templates, pick, npick, counter, resweep, status, stream);
+  if constexpr (kMaxZt[GROUP] >= 2)
+    if (zt == 2) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 2 ? 2 : 1)>(targets, templates, pick, npick, counter, resweep, status, stream);
+  return launch_fused<GROUP, EXTY, 1>(targets, templates, pick, npick, counter, resweep, status, stream);
+}
+
+static int zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
+                       int ntemplate, int* tile_counter, const rr_scan_options* opt, int* status,
+                       rr_stream_t stream) {
   if (!targets || !templates || !tile_counter) return RR_EINVAL;
   if (ntemplate < 1 || ntemplate > RR_MAX_TEMPLATES) return RR_EINVAL;
   if (targets->nblock < 1 || targets->nseg < 1 || targets->nseg > 16) return RR_EINVAL;
@@ -820,9 +834,18 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
     rw_end = sd.rw_offset + sd.npix_pad > rw_end ? sd.rw_offset + sd.npix_pad : rw_end;
   }
   if (rw_end > targets->npix_block) return RR_EINVAL;
+  int zt[kNGroups];
+  for (int g = 0; g < kNGroups; ++g) zt[g] = kDefaultZt[g];
+  if (opt) {
+    if (opt->zt_nbasis4 < 0 || opt->zt_nbasis4 > kMaxZt[1] || opt->zt_nbasis5 < 0 ||
+        opt->zt_nbasis5 > kMaxZt[2])
+      return RR_EINVAL;
+    if (opt->zt_nbasis4) zt[1] = opt->zt_nbasis4;
+    if (opt->zt_nbasis5) zt[2] = opt->zt_nbasis5;
+  }
   // launch groups: (nbasis group, y_ext) -> one persistent launch each
-  int group[6][RR_MAX_TEMPLATES];
-  int ng[6] = {0, 0, 0, 0, 0, 0};
+  int group[2 * kNGroups][RR_MAX_TEMPLATES];
+  int ng[2 * kNGroups] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int t = 0; t < ntemplate; ++t) {
     const rr_scan_template& tm = templates[t];
     if (tm.nbasis < 1 || tm.nbasis > RR_MAX_NBASIS || tm.nz < 0) return RR_EINVAL;
@@ -834,7 +857,7 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
       if (targets->segs[s].basis_offset + targets->segs[s].npix_pad + kHalfBand > tm.pix_stride)
         return RR_EINVAL;
     if (tm.y_ext && (reinterpret_cast<uintptr_t>(tm.y_ext) & 7) != 0) return RR_EINVAL;
-    const int gi = group_of(tm.nbasis) + (tm.y_ext ? 3 : 0);
+    const int gi = group_of(tm.nbasis) + (tm.y_ext ? kNGroups : 0);
     group[gi][ng[gi]++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
@@ -843,13 +866,27 @@ extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_temp
   // share tile_counter[0]
   int* resweep = tile_counter + 2;
   int rc = RR_OK;
-  if (!rc && ng[0]) rc = launch_fused<0, false>(targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
-  if (!rc && ng[1]) rc = launch_fused<1, false>(targets, templates, group[1], ng[1], tile_counter, resweep, status, st);
-  if (!rc && ng[2]) rc = launch_fused<2, false>(targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
-  if (!rc && ng[3]) rc = launch_fused<0, true>(targets, templates, group[3], ng[3], tile_counter, resweep, status, st);
-  if (!rc && ng[4]) rc = launch_fused<1, true>(targets, templates, group[4], ng[4], tile_counter, resweep, status, st);
-  if (!rc && ng[5]) rc = launch_fused<2, true>(targets, templates, group[5], ng[5], tile_counter, resweep, status, st);
+  if (!rc && ng[0]) rc = launch_group<0, false>(zt[0], targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
+  if (!rc && ng[1]) rc = launch_group<1, false>(zt[1], targets, templates, group[1], ng[1], tile_counter, resweep, status, st);
+  if (!rc && ng[2]) rc = launch_group<2, false>(zt[2], targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
+  if (!rc && ng[3]) rc = launch_group<3, false>(zt[3], targets, templates, group[3], ng[3], tile_counter, resweep, status, st);
+  if (!rc && ng[4]) rc = launch_group<0, true>(zt[0], targets, templates, group[4], ng[4], tile_counter, resweep, status, st);
+  if (!rc && ng[5]) rc = launch_group<1, true>(zt[1], targets, templates, group[5], ng[5], tile_counter, resweep, status, st);
+  if (!rc && ng[6]) rc = launch_group<2, true>(zt[2], targets, templates, group[6], ng[6], tile_counter, resweep, status, st);
+  if (!rc && ng[7]) rc = launch_group<3, true>(zt[3], targets, templates, group[7], ng[7], tile_counter, resweep, status, st);
   return rc;
+}
+
+extern "C" int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
+                              int ntemplate, int* tile_counter, int* status, rr_stream_t stream) {
+  return zscan_fused(targets, templates, ntemplate, tile_counter, nullptr, status, stream);
+}
+
+extern "C" int rr_zscan_fused_opt(const rr_scan_targets* targets,
+                                  const rr_scan_template* templates, int ntemplate,
+                                  int* tile_counter, const rr_scan_options* opt, int* status,
+                                  rr_stream_t stream) {
+  return zscan_fused(targets, templates, ntemplate, tile_counter, opt, status, stream);
 }
 
 extern "C" int rr_pack_targets(const rr_spectrum_desc* specs, int64_t nspec,

@@ -505,12 +505,15 @@ def _record(ev, stream):
         ev.record()
 
 
-def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=None):
+def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=None,
+              tiles=None):
     """One persistent launch over every (target, template, z).  ygemm:
     None (DEFAULT_Y), "fp64", "int8x7", "bf16x3" or "tf32x3"; other than
     "fp64", y is computed on the tensor cores first (YGemm).  kernel_events:
     a list that gets a (start, end) CUDA event pair around the scan launches
-    alone (timing)."""
+    alone (timing).  tiles: redshifts per thread {nbasis: ZT} for the small
+    bases (nbasis 4: 1-3, nbasis 5: 1-2; rr_scan_options), else the
+    defaults."""
     L = _lib.lib()
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
@@ -539,8 +542,13 @@ def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=N
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             _record(e0, stream)
-        rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
-                              stream_handle(stream))
+        if tiles:
+            opt = _lib.ScanOptions(int(tiles.get(4, 0)), int(tiles.get(5, 0)))
+            rc = L.rr_zscan_fused_opt(ctypes.byref(tgs), arr, len(tms), ptr(counter),
+                                      ctypes.byref(opt), st.ptr, stream_handle(stream))
+        else:
+            rc = L.rr_zscan_fused(ctypes.byref(tgs), arr, len(tms), ptr(counter), st.ptr,
+                                  stream_handle(stream))
         _lib.check(rc, "rr_zscan_fused")
         if kernel_events is not None:
             _record(e1, stream)

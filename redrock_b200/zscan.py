@@ -97,6 +97,7 @@ def _pack(targets, layout):
 # fused scan
 # ---------------------------------------------------------------------------
 CHUNK_TARGETS = 128   # targets per pipelined chunk (4 target blocks)
+AUTOTUNE = True       # time the small-basis tile shapes once per workload signature
 FIRST_CHUNK = 32      # a small first chunk gets the GPU started early
 
 
@@ -228,7 +229,11 @@ def scan_device(targets, dtemplates, chunk=None, host=False):
             pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
                                    lambda: TargetPack(TargetBatch(sub, layout).to_device(),
                                                       status=st))
-        res, _ = run_fused(pack, bases, status=st)
+        tiles = None
+        if AUTOTUNE:
+            from . import autotune
+            tiles = autotune.tiles_of(autotune.choice(pack, bases) or autotune.tune(pack, bases))
+        res, _ = run_fused(pack, bases, status=st, tiles=tiles)
         keep.append((pack, res))
         if host:
             ev = torch.cuda.Event()

@@ -374,3 +374,29 @@ def test_precision_stress_high_snr(rr):
         assert_chi2(zc, ozc)
         np.testing.assert_array_equal(np.argmin(zc, axis=1), np.argmin(ozc, axis=1))
         assert_coeff(co, oco)
+
+
+def test_tile_shapes_bit_identical_and_autotuner(rr):
+    """Every compiled tile shape (redshifts per thread for nbasis 4 and 5)
+    gives bit-identical results (each (target, z) keeps its own sums in the
+    same order), and the autotuner picks among them."""
+    import torch
+    from redrock_b200 import autotune
+    from redrock_b200.engine import (DeviceBasis, GridLayout, TargetBatch, TargetPack,
+                                     TemplateSource, run_fused)
+    tg = rr["targets"].from_synth(synth.make_targets(45, seed=83, drop_camera_frac=0.2))
+    tms = [rr["templates"].from_synth(t) for t in synth.template_set(zsub=37)]
+    layout = GridLayout.from_dwave(synth.camera_grids())
+    bases = [DeviceBasis.build(TemplateSource.from_template(t), layout) for t in tms]
+    pack = TargetPack(TargetBatch(tg, layout).to_device())
+    ref, st = run_fused(pack, bases, tiles={4: 1, 5: 1})
+    st.check("zt1")
+    for tiles in ({4: 2, 5: 2}, {4: 3, 5: 1}, {4: 3, 5: 2}):
+        res, st = run_fused(pack, bases, tiles=tiles)
+        st.check(str(tiles))
+        for a, b in zip(ref, res):
+            assert torch.equal(a.zchi2, b.zchi2) and torch.equal(a.zcoeff, b.zcoeff)
+            assert torch.equal(a.penalty, b.penalty)
+    best = autotune.tune(pack, bases)
+    assert best[4] in (1, 2, 3) and best[5] in (1, 2)
+    assert autotune.choice(pack, bases) is best
