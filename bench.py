@@ -538,8 +538,8 @@ def main():
     ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
                     help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
                          "summed in the FP64 scan (fp64)")
-    ap.add_argument("--autotune", action="store_true",
-                    help="pick the small-basis tile shapes by timing them before the run")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="use the default tile shapes instead of timing them before the run")
     ap.add_argument("--ygemm-study", action="store_true",
                     help="also time every y variant once and report its chi2/coeff error")
     ap.add_argument("--no-cpu-baseline", action="store_true")
