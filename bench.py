@@ -292,6 +292,7 @@ def run_ours(args, rank, world, local_rank):
     value = world * evals / (ms / 1e3)
 
     study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
+    adj = adjoint_study(rtg, tms, torch) if (args.adjoint and rank == 0) else None
 
     # ---- end to end through the public API, host buffers ------------------
     e2e = None
@@ -407,7 +408,40 @@ def run_ours(args, rank, world, local_rank):
     }
     if study is not None:
         out["ygemm_study"] = study
+    if adj is not None:
+        out["adjoint"] = adj
     return out
+
+
+def adjoint_study(rtg, tms, torch):
+    """Config 2: chi2, dchi2/dz, d2chi2/dz2 and dchi2/dflux (the adjoint pair
+    kernel, rr_zscan_pairs_grad) for every target of the workload against
+    every template at 3 redshifts each (as for the top 3 minima)."""
+    from redrock_b200.adjoint import PairContext
+    from redrock_b200.engine import pair_ranges_ok, run_pairs_grad
+    rng = np.random.default_rng(5)
+    npairs = 0
+    ms = 0.0
+    for tm in tms:
+        ctx = PairContext(rtg, tm)
+        z = np.asarray(tm.redshifts)
+        pz = rng.choice(z[1:-1], size=3 * len(rtg))
+        pt = np.repeat(np.arange(len(rtg)), 3).astype(np.int32)
+        ok = pair_ranges_ok(ctx.src, ctx.layout, pz)
+        pt, pz = pt[ok], pz[ok]
+        run_pairs_grad(ctx.rows, ctx.src, pt, pz, want_dflux=True)   # warm-up
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        run_pairs_grad(ctx.rows, ctx.src, pt, pz, want_dflux=True)
+        b.record()
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+        npairs += len(pz)
+    return {"pairs": npairs, "ms": ms, "value": npairs / (ms / 1e3),
+            "unit": "gradient evals/s (chi2, dchi2/dz, d2chi2/dz2, dchi2/dflux per (target, z))",
+            "kernel": "zscan_pairs_kernel<NB, grad> (template rebinned + IGM per pair)"}
 
 
 def ygemm_study(args, step, torch, evals):
@@ -538,6 +572,8 @@ def main():
     ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
                     help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
                          "summed in the FP64 scan (fp64)")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="also time the adjoint pair kernel on 3 redshifts per target and template")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="use the default tile shapes instead of timing them before the run")
     ap.add_argument("--ygemm-study", action="store_true",

@@ -22,6 +22,7 @@ import numpy as np
 
 from . import fitz as _fitz
 from .templates import parse_fulltype
+from .engine import GridLayout, RowPack
 from .zscan import calc_zchi2_targets
 
 MAX_VELO_DIFF = 1000.0
@@ -140,12 +141,17 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
                                   "redrock_b200.shard) instead of an MPI communicator")
     results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
     local = list(targets.local())
+    # the targets' packed rows for the fine-grid pair scans do not depend on
+    # the template: pack them once for every template's refinement
+    layout = GridLayout.from_dwave(targets.wavegrids()) if local else None
+    rowpack = RowPack.from_targets(local, layout) if local else None
     sort = np.array([t.template.full_type for t in templates]).argsort()
     for t in np.array(list(templates), dtype=object)[sort]:
         ft = t.template.full_type
         chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
         fits = _fitz.fitz_targets(chi2, t.template.redshifts, local, t.template,
-                                  nminima=nminima, zminfit_npoints=zminfit_npoints)
+                                  nminima=nminima, zminfit_npoints=zminfit_npoints,
+                                  layout=layout, rowpack=rowpack)
         for tg, zf in zip(local, fits):
             results[tg.id][ft]['zfit'] = zf
     for tg in local:
