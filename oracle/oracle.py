@@ -20,9 +20,14 @@ Restates, in numpy/scipy (and a small C file for the rebin), redrock 0.22:
   calc_negOII_penalty   py/redrock/zscan.py:783-800
   calc_zchi2            py/redrock/zscan.py:807-889
   calc_zchi2_one        py/redrock/zscan.py:169-190, 213-243
+  per_camera_coeff      py/redrock/zscan.py:245-348 (CPU branch)
+  get_best_archetype,   py/redrock/archetypes.py:228-400 (trapz rebin, CPU)
+  nearest_neighbour_model
+  prior_on_coeffs       py/redrock/fitz.py:113-130
+  legendre_dict         py/redrock/targets.py:237-254, utils.py:260-271
 
 Pinned against fixtures generated by running redrock itself
-(tests/golden/make_golden.py, tests/test_oracle.py).
+(tests/golden/make_*golden.py, tests/test_oracle.py).
 """
 
 from __future__ import annotations
@@ -460,3 +465,146 @@ def chi2_grad_z(spectra, wave, flux, z, dwave, igm_model):
     c = solve_pca(M, Tb.T.dot(wf))
     r = f - Tb.dot(c)
     return np.dot(w * r, r), -2.0 * np.dot(w * r, dTb.dot(c))
+
+
+# ---------------------------------------------------------------------------
+# archetypes
+# ---------------------------------------------------------------------------
+
+def reduced_wavelength(wave):
+    """utils.py:260-271: wavelengths mapped linearly onto [-1, 1]."""
+    return 2 * (wave - wave.min()) / (wave.max() - wave.min()) - 1
+
+
+def legendre_dict(dwave, nleg):
+    """Target.legendre (targets.py:237-254): P_0..P_{nleg-1} per grid."""
+    import scipy.special
+    return {hs: np.array([scipy.special.legendre(i)(reduced_wavelength(w)) for i in range(nleg)])
+            .reshape(nleg, len(w)) for hs, w in dwave.items()}
+
+
+def prior_on_coeffs(n_nbh, deg_legendre, sigma, ncamera):
+    """fitz.py:113-130: 1/sigma^2 on the Legendre terms, 0 on archetypes."""
+    nbasis = n_nbh + deg_legendre * ncamera
+    prior = np.zeros((nbasis, nbasis))
+    np.fill_diagonal(prior, 1 / (sigma ** 2))
+    for i in range(n_nbh):
+        prior[i][i] = 0.
+    return prior
+
+
+def per_camera_coeff(spectra, tdata, weights, flux, wflux, nleg, narch, method, n_nbh, prior,
+                     bands):
+    """per_camera_coeff_with_least_square_batch, CPU branch (zscan.py:245-348):
+    one fit per archetype with each camera's Legendre terms in their own
+    columns; coefficients in [archetypes, Legendre per band] order."""
+    ncam = len(bands)
+    nbasis = n_nbh + nleg * ncam
+    method = method.upper()
+    solver_args = {}
+    if method == 'BVLS':
+        bounds = np.zeros((2, nbasis))
+        bounds[0][n_nbh:] = -np.inf
+        bounds[1] = np.inf
+        solver_args['bounds'] = bounds
+    zzchi2 = np.zeros(narch)
+    zzcoeff = np.zeros((narch, nbasis))
+    for j in range(narch):
+        t2 = {}
+        for i, hs in enumerate(tdata):
+            a = np.zeros((tdata[hs].shape[1], nbasis))
+            a[:, :n_nbh] = tdata[hs][j, :, :n_nbh]
+            a[:, n_nbh + i * nleg:n_nbh + (i + 1) * nleg] = tdata[hs][j, :, n_nbh:]
+            t2[hs] = a[None]
+        c2, co = calc_zchi2_batch(spectra, t2, weights, flux, wflux, 1, nbasis, method, prior,
+                                  solver_args)
+        zzchi2[j] = c2[0]
+        zzcoeff[j] = co[0]
+    if n_nbh > 1:
+        alpha = zzcoeff[0:1, :n_nbh]
+    else:
+        alpha = zzcoeff[:, :1]
+    blocks = np.split(zzcoeff[:, n_nbh:], ncam, axis=1) if nleg >= 1 else []
+    # one block per distinct band, in order of first appearance in bands
+    seen = {}
+    for i, b in enumerate(bands):
+        seen[b] = blocks[i] if blocks else None
+    cols = [alpha] + ([seen[b] for b in seen] if nleg >= 1 else [])
+    return zzchi2, np.concatenate(cols, axis=1)
+
+
+class OArchetype:
+    """Archetype set: wave (nwave,), flux (narch, nwave), rrtype, and the
+    subtypes with the row number appended (archetypes.py:35-70)."""
+
+    def __init__(self, wave, flux, rrtype, subtype):
+        self.wave = np.asarray(wave, dtype=np.float64)
+        self.flux = np.asarray(flux, dtype=np.float64)
+        self.narch = self.flux.shape[0]
+        self.rrtype = rrtype
+        self.subtype = np.array([f"{s}_{i}" for i, s in enumerate(subtype)])
+        self.full_type = np.array([f"{rrtype}:::{s}" for s in self.subtype])
+        self.igm_model = 'Inoue14'
+
+    def rebin(self, z, dwave, indx=None):
+        """rebin_template_batch, trapz (archetypes.py:129-183):
+        dict -> (nbin, narch)."""
+        flux = self.flux if indx is None else self.flux[indx]
+        return {hs: trapz_rebin((1. + z) * self.wave, flux, w) for hs, w in dwave.items()}
+
+
+def nearest_neighbour_model(arch, spectra, bands, legendre, weights, flux, wflux, dwave, z,
+                            n_nearest, zzchi2, per_camera, binned, prior):
+    """archetypes.py:228-294 with binned (already x IGM) passed in."""
+    nleg = legendre[next(iter(legendre))].shape[0]
+    iBest = np.argsort(zzchi2)[0:n_nearest]
+    tdata = {}
+    for hs in dwave:
+        a = binned[hs][:, iBest][None]
+        if nleg > 0:
+            a = np.append(a, legendre[hs].T[None], axis=2)
+        tdata[hs] = a
+    nbasis = tdata[hs].shape[2]
+    if per_camera:
+        c2, co = per_camera_coeff(spectra, tdata, weights, flux, wflux, nleg, 1, 'bvls',
+                                  n_nearest, prior, bands)
+    else:
+        c2, co = calc_zchi2_batch(spectra, tdata, weights, flux, wflux, 1, nbasis)
+    return c2[0], co[0], arch.rrtype + ':::' + ';'.join(arch.subtype[k] for k in iBest)
+
+
+def get_best_archetype(arch, spectra, bands, legendre, weights, flux, wflux, dwave, z,
+                       per_camera, n_nearest, trans=None, solve_method='bvls', prior=None):
+    """Archetype.get_best_archetype, CPU branch (archetypes.py:295-400).
+    ``trans``: dict of 1-D transmissions (or None) per grid at z."""
+    nleg = legendre[next(iter(legendre))].shape[0]
+    if trans is None:
+        trans = {hs: transmission_Lyman(z, w, model=arch.igm_model) for hs, w in dwave.items()}
+    binned = arch.rebin(z, dwave)
+    nn_prior = None
+    if n_nearest is not None:
+        nn_prior = prior.copy()
+        prior = prior[n_nearest - 1:, n_nearest - 1:]
+    tdata = {}
+    for hs in dwave:
+        if trans[hs] is not None:
+            binned[hs] = binned[hs] * trans[hs][:, None]
+        a = binned[hs].T[:, :, None]
+        if nleg > 0:
+            a = np.append(a, np.tile(legendre[hs].T[None], (arch.narch, 1, 1)), axis=2)
+        tdata[hs] = a
+    nbasis = tdata[hs].shape[2]
+    if per_camera:
+        c2, co = per_camera_coeff(spectra, tdata, weights, flux, wflux, nleg, arch.narch,
+                                  solve_method, 1, prior, bands)
+    else:
+        bounds = np.zeros((2, nbasis))
+        bounds[0][1:] = -np.inf
+        bounds[1] = np.inf
+        c2, co = calc_zchi2_batch(spectra, tdata, weights, flux, wflux, arch.narch, nbasis,
+                                  solve_method.upper(), None, {'bounds': bounds})
+    if n_nearest is not None:
+        return nearest_neighbour_model(arch, spectra, bands, legendre, weights, flux, wflux,
+                                       dwave, z, n_nearest, c2, per_camera, binned, nn_prior)
+    i = np.argmin(c2)
+    return c2[i], co[i], arch.full_type[i]

@@ -16,8 +16,12 @@ first batch are fetched in further launches only for targets that need
 them), so the decisions are redrock's.
 
 ``fitz_targets`` is the batched entry point (many targets, one template);
-``fitz`` keeps redrock's single-target signature.  Archetype fits are not
-implemented (NotImplementedError).
+``fitz`` keeps redrock's single-target signature.  With an archetype set,
+each refined minimum is then fitted with every archetype
+(``archetype.get_best_archetype``: one batched bounded solve on the device)
+and the result carries the archetype's chi2, coefficients, Legendre
+coefficients and name next to the template's own coefficients
+(fitz.py:331-357).
 """
 
 from __future__ import annotations
@@ -32,6 +36,17 @@ MAX_VELO_DIFF = 1000.0      # constants.py:7
 MAX_VELO_DIFF_STAR = 100.0  # constants.py:8
 Z_FITLIMIT = 2 ** 5         # zwarning.py:20
 BAD_MINFIT = 2 ** 10        # zwarning.py:25
+
+
+def prior_on_coeffs(n_nbh, deg_legendre, sigma, ncamera):
+    """Diagonal prior 1/sigma^2 on the Legendre coefficients, none on the
+    n_nbh archetype coefficients (fitz.py:113-130)."""
+    nbasis = n_nbh + deg_legendre * ncamera
+    prior = np.zeros((nbasis, nbasis), dtype='float64')
+    np.fill_diagonal(prior, 1 / (sigma ** 2))
+    for i in range(n_nbh):
+        prior[i][i] = 0.
+    return prior
 
 
 def get_dv(z, zref):
@@ -126,8 +141,6 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     steps on chi2(z) (the adjoint kernel's dchi2/dz and envelope curvature)
     inside that three-point cell, with zerr = sqrt(2 / d2chi2/dz2); the
     decisions that follow (ZWARN bits, velocity separation) are the same."""
-    if archetype is not None:
-        raise NotImplementedError("archetype refinement is not implemented by the GPU engine")
     from . import _lib
     from .templates import solve_code
     if solve_code(template) in (_lib.RR_SOLVE_NNLS, _lib.RR_SOLVE_BVLS):
@@ -262,6 +275,9 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                 r['zwarn'] |= BAD_MINFIT
             else:
                 raise ValueError('edges must be within input x range')
+            if archetype is not None:
+                _archetype_fit(targets[j], r, zmin, good, template, archetype, use_gpu,
+                               deg_legendre, per_camera, n_nearest, prior_sigma)
 
     out = []
     for j, t in enumerate(targets):
@@ -285,6 +301,51 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             tmp[k] = np.vstack([r[k] for r in res])
         out.append(tmp)
     return out
+
+
+def _archetype_fit(target, r, zmin, good, template, archetype, use_gpu, deg_legendre,
+                   per_camera, n_nearest, prior_sigma):
+    """Replace a refined minimum's fit by the best archetype fit at its
+    redshift (fitz.py:263-293, 331-357).  The IGM transmission at the
+    parabola minimum comes along as redrock computes it (none when the
+    template could not be evaluated there).  redrock leaves ``ncamera``
+    undefined when prior_sigma is None (a NameError); here it is the number
+    of grids with per_camera, else 1, in every case."""
+    from .archetypes import split_archetype_coeff
+    from .igm import transmission_Lyman
+    from .templates import parse_fulltype
+    from .zscan import spectral_data
+    spectra = target.spectra
+    dwave = {s.wavehash: s.wave for s in spectra}
+    weights, flux, wflux = spectral_data(spectra)
+    if target.nleg != deg_legendre or getattr(target, "_legendre", None) is None:
+        target.legendre(deg_legendre)
+    trans = {hs: None for hs in dwave}
+    if good:
+        for k in dwave:
+            trans[k] = transmission_Lyman(np.array([zmin]), dwave[k], use_gpu=False,
+                                          always_return_array=False, model=template.igm_model)
+        pca_coeff = np.asarray(r['coeff'])[0, :]
+    else:
+        pca_coeff = np.copy(r['coeff'])
+    ncamera = len(dwave) if per_camera else 1
+    prior = None
+    if prior_sigma is not None:
+        prior = prior_on_coeffs(1 if n_nearest is None else n_nearest, deg_legendre, prior_sigma,
+                                ncamera)
+    chi2min, coeff, fulltype = archetype.get_best_archetype(
+        target, weights, flux, wflux, dwave, r['z'], per_camera, n_nearest, trans=trans,
+        use_gpu=use_gpu, prior=prior)
+    subtype = parse_fulltype(fulltype)[1]
+    archcoeff, legcoeff = split_archetype_coeff(subtype, coeff, ncamera, deg_legendre)
+    if per_camera:
+        legcoeff = [np.vstack(legcoeff)]
+    prev = dict(r)
+    r.clear()   # redrock's key order for archetype results
+    r.update(z=prev['z'], zerr=prev['zerr'], zwarn=prev['zwarn'], chi2=chi2min, zz=prev['zz'],
+             zzchi2=prev['zzchi2'], coeff=archcoeff, legcoeff=legcoeff, fulltype=fulltype,
+             fitmethod=archetype.method, pca_coeff=pca_coeff,
+             pca_spectype=template._rrtype, pca_subtype=template.sub_type)
 
 
 def fitz(zchi2, redshifts, target, template, nminima=3, archetype=None, use_gpu=False,

@@ -30,6 +30,11 @@ PATCHES = {
     ("zfind", "fitz"): ("fitz", "fitz"),
     ("archetypes", "trapz_rebin"): ("rebin", "trapz_rebin"),
     ("archetypes", "transmission_Lyman"): ("igm", "transmission_Lyman"),
+    ("archetypes", "calc_zchi2_batch"): ("zscan", "calc_zchi2_batch"),
+    ("archetypes", "per_camera_coeff_with_least_square_batch"):
+        ("zscan", "per_camera_coeff_with_least_square_batch"),
+    ("zscan", "per_camera_coeff_with_least_square_batch"):
+        ("zscan", "per_camera_coeff_with_least_square_batch"),
 }
 # methods of redrock classes: (module, class, method) -> (our module, function)
 METHOD_PATCHES = {

@@ -197,6 +197,37 @@ def star_basis(subtype, step=0.2, lo=3500.0, hi=10000.0):
 
 
 @dataclass
+class ArchetypeSpec:
+    """A redrock-format archetype set: ``flux`` (narch, nwave) on a linear
+    rest grid, one subtype name per row, spectral class ``rrtype``."""
+    rrtype: str
+    wave: np.ndarray
+    flux: np.ndarray
+    subtype: list
+    version: str = "synthetic"
+
+
+def archetype_set(narch=24, seed=5, rrtype="GALAXY", step=0.5, lo=800.0, hi=10000.0):
+    """Positive rest-frame galaxy-like spectra: a power-law continuum with a
+    4000 A break and a weak ripple, plus the [OII], Hb, [OIII], Ha+[NII],
+    [SII], Lya and MgII lines (sigma 2-6 A) with random strengths."""
+    rng = np.random.default_rng(seed)
+    wave = np.arange(lo, hi + step / 2, step)
+    lines = (1215.67, 2798.75, 3727.0, 4861.3, 4958.9, 5006.8, 6562.8, 6583.4, 6716.4, 6730.8)
+    flux = np.zeros((narch, len(wave)))
+    for i in range(narch):
+        slope = rng.uniform(-2.5, -0.5)
+        cont = (wave / 5000.0) ** slope
+        cont *= 1.0 - rng.uniform(0.0, 0.5) / (1.0 + np.exp((wave - 4000.0) / 30.0))
+        cont *= 1.0 + 0.05 * np.sin(2 * np.pi * wave / rng.uniform(300.0, 900.0))
+        amp = rng.uniform(0.0, 3.0, size=len(lines)) * (rng.uniform(size=len(lines)) < 0.8)
+        sig = rng.uniform(2.0, 6.0)
+        flux[i] = cont + sum(a * _gauss(wave, c, sig) for a, c in zip(amp, lines))
+    sub = ["ELG" if i % 3 == 0 else ("LRG" if i % 3 == 1 else "BGS") for i in range(narch)]
+    return ArchetypeSpec(rrtype, wave, flux, sub)
+
+
+@dataclass
 class TemplateSpec:
     spectype: str
     subtype: str

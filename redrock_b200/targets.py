@@ -61,11 +61,33 @@ class Target:
         self.gpuwflux = None
         # redrock takes the bands of the spectra given, before any coadd
         self.bands = [s.band for s in spectra]
+        self.nleg = 0
+        self._legendre = None
+        self._gpulegendre = None
 
     def compute_coadd(self, cache_Rcsr=False, cosmics_nsig=0.):
         """Per-grid coadd of the exposures on the GPU (targets.py:267-373)."""
         from .coadd import coadd_targets
         coadd_targets([self], cache_Rcsr=cache_Rcsr, cosmics_nsig=cosmics_nsig)
+
+    def legendre(self, nleg, use_gpu=False):
+        """Legendre polynomials P_0..P_{nleg-1} of each grid's reduced
+        wavelength, dict[wavehash] -> (nleg, npix), cached per nleg
+        (targets.py:237-254); CUDA tensors when use_gpu."""
+        if self._legendre is None or self.nleg != nleg:
+            import scipy.special
+            dwave = {s.wavehash: s.wave for s in self.spectra}
+            self._legendre = {hs: np.array([scipy.special.legendre(i)(reduced_wavelength(w))
+                                            for i in range(nleg)]).reshape(nleg, len(w))
+                              for hs, w in dwave.items()}
+            self._gpulegendre = None
+            self.nleg = nleg
+        if use_gpu:
+            if self._gpulegendre is None:
+                from .device import to_device
+                self._gpulegendre = {hs: to_device(a) for hs, a in self._legendre.items()}
+            return self._gpulegendre
+        return self._legendre
 
     def gpu_spectral_data(self):
         """Concatenated (weights, flux, wflux) as CUDA tensors, cached."""
@@ -75,6 +97,14 @@ class Target:
             self.gpuflux = to_device(np.concatenate([s.flux for s in self.spectra]))
             self.gpuwflux = self.gpuweights * self.gpuflux
         return (self.gpuweights, self.gpuflux, self.gpuwflux)
+
+
+def reduced_wavelength(wave):
+    """Wavelengths mapped linearly onto [-1, 1] (utils.py:260-271)."""
+    wave = np.asarray(wave)
+    wavemax = wave.max()
+    wavemin = wave.min()
+    return 2 * (wave - wavemin) / (wavemax - wavemin) - 1
 
 
 def distribute_work(nproc, ids, weights=None, capacities=None):

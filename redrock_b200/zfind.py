@@ -10,10 +10,17 @@
      bits then chi2, keep ``nminima`` per spectral type, delta-chi2 and
      SMALL_DELTA_CHI2 (``calc_deltachi2``, zfind.py:103-155).
 
+With ``archetypes`` (dict spectype -> Archetype) each refined minimum of a
+template with an archetype set is refitted with the archetypes
+(``fitz_targets(archetype=...)``), and the finalisation adds redrock's
+archetype columns (pca_coeff / pca_spectype / pca_subtype, legcoeff) and the
+NEGATIVE_MODEL bit (zfind.py:470-580).
+
 It returns ``(allresults, allzfit)`` like redrock, except that ``allzfit`` is
 a dict of numpy columns (``astropy.table.Table(allzfit)`` gives redrock's
 table) with redrock's column names and order of rows.  Single-process only
-(``targets.comm`` None); archetypes and priors are not supported.
+(``targets.comm`` None); redshift priors and chi2_scan input are not
+supported.
 """
 
 from __future__ import annotations
@@ -83,20 +90,48 @@ def sort_zfit_dict(zfit):
     zfit.pop('__badfit__')
 
 
-def _finalise_target(tid, fits, nminima):
+# archetype mode: result columns that fall back to another column of a
+# template fitted without archetypes, and columns filled with zeros
+# (utils.py:273-279)
+PCA_MAP = {"pca_coeff": "coeff", "pca_subtype": "subtype", "pca_spectype": "spectype"}
+ZERO_LIKE_KEYS = {"archcoeff", "legcoeff"}
+
+
+def _pad_cols(val, ref):
+    return np.pad(val, ((0, 0), (0, max(0, ref.shape[1] - val.shape[1]))),
+                  constant_values=0)[:, :ref.shape[1]]
+
+
+def _finalise_target(tid, fits, nminima, arch=None):
+    """One target's rows of the zfit table (zfind.py:466-616).  ``arch``:
+    None, or dict(spectypes=archetype spectypes, all_spectypes=template
+    spectypes, n_nearest=...)."""
     tzfit = []
     for fulltype, tmp in fits:
+        tmp = dict(tmp)
+        if arch is not None and 'fulltype' in tmp:
+            spectype, subtype = [], []
+            for el in tmp['fulltype']:
+                a, b = parse_fulltype(el[0])
+                spectype.append(a)
+                subtype.append(b)
+            del tmp['fulltype']
+        else:
+            spectype, subtype = parse_fulltype(fulltype)
         nmin = len(tmp['chi2'])
         if nmin == 0:
             print(f'WARNING: no {fulltype} chi2 vs. z minima for targetid {tid}')
             continue
-        spectype, subtype = parse_fulltype(fulltype)
-        tmp = dict(tmp)
-        tmp['spectype'] = np.full((nmin, 1), spectype)
-        tmp['subtype'] = np.full((nmin, 1), subtype)
+        if np.isscalar(spectype):
+            tmp['spectype'] = np.full((nmin, 1), spectype)
+            tmp['subtype'] = np.full((nmin, 1), subtype)
+        else:
+            tmp['spectype'] = np.array([spectype]).reshape((nmin, 1))
+            tmp['subtype'] = np.array([subtype]).reshape((nmin, 1))
         tmp['ncoeff'] = np.array([tmp['coeff'].shape[1]] * nmin).reshape((nmin, 1))
-        mv = MAX_VELO_DIFF_STAR if spectype.upper() == 'STAR' else MAX_VELO_DIFF
-        tmp['max_velo_diff'] = np.full((nmin, 1), mv)
+        star = (spectype.upper() == 'STAR') if np.isscalar(spectype) else \
+            (spectype[0].upper() == 'STAR')
+        tmp['max_velo_diff'] = np.full((nmin, 1), MAX_VELO_DIFF_STAR if star else MAX_VELO_DIFF)
         tzfit.append(tmp)
     maxncoeff = max(t['coeff'].shape[1] for t in tzfit)
     for t in tzfit:
@@ -105,11 +140,43 @@ def _finalise_target(tid, fits, nminima):
             t['coeff'] = np.append(t['coeff'], np.zeros((t['coeff'].shape[0], n)), axis=1)
     out = {}
     for k in tzfit[0].keys():
-        out[k] = np.vstack([t[k] for t in tzfit])
+        ref = tzfit[0][k]
+        vals = []
+        val = None
+        for row in tzfit:
+            if k in row:
+                val = row[k]
+                if arch is not None and k in PCA_MAP:
+                    val = _pad_cols(val, ref)
+            elif arch is not None and k in PCA_MAP and PCA_MAP[k] in row:
+                val = _pad_cols(row[PCA_MAP[k]], ref)
+            elif k in ZERO_LIKE_KEYS:
+                val = np.zeros_like(ref)
+            # otherwise the previous row's value repeats, as in redrock's loop
+            vals.append(val)
+        out[k] = np.vstack(vals)
         if k != 'coeff' and out[k].shape[1] == 1:
             out[k] = out[k].flatten()
     n = len(out['chi2'])
     out['targetid'] = np.array([tid] * n)
+    if arch is not None:
+        nn = arch['n_nearest']
+        if len(arch['spectypes']) == len(arch['all_spectypes']):
+            if nn is None:
+                if out['coeff'].ndim == 1:
+                    out['coeff'] = out['coeff'].reshape(-1, 1)
+                ibad = out['coeff'][:, 0] <= 0.
+            else:
+                ibad = np.any(out['coeff'][:, :nn] < 0, axis=1)
+        else:
+            ibad = np.isin(out['spectype'], np.array(arch['spectypes']))
+            for k in np.where(ibad)[0]:
+                if nn is None:
+                    if out['coeff'][:, 0][k] >= 0.:
+                        ibad[k] = False
+                elif np.all(out['coeff'][:, :nn][k] >= 0):
+                    ibad[k] = False
+        out['zwarn'][ibad] |= NEGATIVE_MODEL
     out['zwarn'][out['npixels'] == 0] |= NODATA
     out['zwarn'][out['npixels'] < 10 * out['ncoeff']] |= LITTLE_COVERAGE
     sort_zfit_dict(out)
@@ -132,9 +199,9 @@ def _finalise_target(tid, fits, nminima):
 
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
-          n_nearest=None, prior_sigma=None):
-    if archetypes or priors is not None or chi2_scan is not None:
-        raise NotImplementedError("archetypes, priors and chi2_scan input are not supported by "
+          n_nearest=None, prior_sigma=None, ncamera=None):
+    if priors is not None or chi2_scan is not None:
+        raise NotImplementedError("redshift priors and chi2_scan input are not supported by "
                                   "the GPU zfind driver")
     if targets.comm is not None and targets.comm.size > 1:
         raise NotImplementedError("use one process per GPU with its own targets (see "
@@ -146,12 +213,23 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
     layout = GridLayout.from_dwave(targets.wavegrids()) if local else None
     rowpack = RowPack.from_targets(local, layout) if local else None
     sort = np.array([t.template.full_type for t in templates]).argsort()
+    arch = None
+    if archetypes:
+        all_spectypes = []
+        for t in templates:
+            if t.template.template_type not in all_spectypes:
+                all_spectypes.append(t.template.template_type)
+        arch = dict(spectypes=list(archetypes.keys()), all_spectypes=all_spectypes,
+                    n_nearest=n_nearest)
     for t in np.array(list(templates), dtype=object)[sort]:
         ft = t.template.full_type
+        archetype = archetypes.get(t.template._rrtype) if archetypes else None
         chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
         fits = _fitz.fitz_targets(chi2, t.template.redshifts, local, t.template,
-                                  nminima=nminima, zminfit_npoints=zminfit_npoints,
-                                  layout=layout, rowpack=rowpack)
+                                  nminima=nminima, archetype=archetype, use_gpu=use_gpu,
+                                  deg_legendre=deg_legendre, zminfit_npoints=zminfit_npoints,
+                                  per_camera=per_camera, n_nearest=n_nearest,
+                                  prior_sigma=prior_sigma, layout=layout, rowpack=rowpack)
         for tg, zf in zip(local, fits):
             results[tg.id][ft]['zfit'] = zf
     for tg in local:
@@ -163,7 +241,7 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
         for ft in allresults[tid]:
             if ft != 'meta':
                 del allresults[tid][ft]['zfit']
-        rows.append(_finalise_target(tid, fits, nminima))
+        rows.append(_finalise_target(tid, fits, nminima, arch))
     # stack the per-target tables (astropy.table.vstack equivalent)
     cols = ['targetid'] + [k for k in rows[0] if k != 'targetid']
     allzfit = {}
@@ -185,6 +263,8 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
     if allzfit['spectype'].dtype != '<U6':
         allzfit['spectype'] = allzfit['spectype'].astype('<U6')
     maxcoeff = np.max([t.template.nbasis for t in templates])
+    if archetypes and per_camera:
+        maxcoeff = max(maxcoeff, ncamera * deg_legendre + (1 if n_nearest is None else n_nearest))
     co = allzfit['coeff']
     ntarg, ncoeff = (co.shape[0], 1) if co.ndim == 1 else co.shape
     if ncoeff != maxcoeff:

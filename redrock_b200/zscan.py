@@ -353,6 +353,60 @@ def calc_zchi2_one(spectra, weights, flux, wflux, tdata, solve_matrices_algorith
     return float(zc[0]), np.asarray(to_numpy(co))[0]
 
 
+def per_camera_coeff_with_least_square_batch(target, tdata, weights, flux, wflux, nleg, narch,
+                                             method=None, n_nbh=None, prior=None, use_gpu=False,
+                                             bands=None):
+    """Archetype fit with a separate set of Legendre terms per camera
+    (zscan.py:245-348).
+
+    ``tdata[hs]`` is (narch, npix, n_nbh + nleg): n_nbh archetype columns
+    followed by the camera's Legendre polynomials.  Each camera's Legendre
+    block moves to its own columns of an (narch, npix, n_nbh + nleg * ncam)
+    basis -- built on the device -- and all narch fits run as one batch of
+    the solve chain (``calc_zchi2_batch`` with nz = narch), BVLS keeping
+    the archetype coefficients >= 0.  Coefficients come back as
+    [archetype terms, then each camera's Legendre terms in ``bands``
+    order].  With n_nbh > 1 redrock keeps only the first row's archetype
+    terms, so that case needs narch == 1, as redrock's caller has it.
+    """
+    spectra = target.spectra
+    ncam = len(bands)
+    nbasis = n_nbh + nleg * ncam
+    method = method.upper()
+    solver_args = {}
+    if method == 'BVLS':
+        bounds = np.zeros((2, nbasis))
+        bounds[0][n_nbh:] = -np.inf
+        bounds[1] = np.inf
+        solver_args['bounds'] = bounds
+    wide = {}
+    for i, hs in enumerate(tdata):
+        a = to_device(tdata[hs])
+        w = torch.zeros((a.shape[0], a.shape[1], nbasis), dtype=torch.float64, device=a.device)
+        w[:, :, :n_nbh] = a[:, :, :n_nbh]
+        w[:, :, n_nbh + i * nleg:n_nbh + (i + 1) * nleg] = a[:, :, n_nbh:]
+        wide[hs] = w
+    zzchi2, zzcoeff = calc_zchi2_batch(spectra, wide, weights, flux, wflux, narch, nbasis,
+                                       solve_matrices_algorithm=method, solver_args=solver_args,
+                                       prior=prior)
+    # redrock's column bookkeeping: an 'alpha' entry, then one entry per band
+    # in ``bands`` order (dict insertion order), filled camera by camera
+    parts = {'alpha': [zzcoeff[:, k] for k in range(n_nbh)]}
+    if nleg > 0:
+        for b in bands:
+            parts[b] = []
+    if n_nbh > 1:
+        parts['alpha'] = np.array([parts['alpha'][k][0] for k in range(n_nbh)])[None, :]
+    else:
+        parts['alpha'] = parts['alpha'][0][:, None]
+    if nleg >= 1:
+        blocks = np.split(zzcoeff[:, n_nbh:], ncam, axis=1)
+        by_band = {band: blocks[i] for i, band in enumerate(bands)}
+        for band in sorted(bands):
+            parts[band] = by_band[band]
+    return zzchi2, np.concatenate(list(parts.values()), axis=1)
+
+
 def calc_zchi2_plain(target_ids, target_data, dtemplate):
     """calc_zchi2 through the plain per-target kernel chain (the structure of
     redrock's own GPU branch: one chain of launches and one host read-back

@@ -58,9 +58,6 @@ def test_fitz_single_target_signature(golden):
     r = fitz.fitz(golden["scan_GALAXY_zchi2"][0] + golden["scan_GALAXY_penalty"][0],
                   ts.redshifts, T.from_synth(tg)[0], TM.from_synth(ts), nminima=3)
     np.testing.assert_allclose(r["z"], golden["fitz_GALAXY_0_z"], atol=1e-7)
-    with pytest.raises(NotImplementedError):
-        fitz.fitz(golden["scan_GALAXY_zchi2"][0], ts.redshifts, T.from_synth(tg)[0],
-                  TM.from_synth(ts), archetype=object())
 
 
 def test_fitz_newton_refinement(golden):

@@ -126,7 +126,7 @@ def test_installer_rebinds_every_import_site():
 
 def test_flop_model():
     import bench
-    # SURVEY 8(d) figures at P = 7958
+    # the per-eval flop model at P = 7958 px (GALAXY, QSO, STAR)
     assert round(bench.flops_per_eval(10, 7958)) == 2785853
     assert round(bench.flops_per_eval(4, 7958)) == 923189
     assert round(bench.flops_per_eval(5, 7958)) == 1193802

@@ -1,4 +1,5 @@
 """The oracle (CPU restatement) against fixtures produced by redrock itself."""
+import os
 import numpy as np
 import pytest
 
@@ -184,3 +185,40 @@ def test_bounded_solves_oracle_vs_redrock_golden():
     np.testing.assert_allclose(zc, g["lsq_nmf_zchi2"], rtol=1e-10, atol=1e-8)
     np.testing.assert_allclose(co, g["lsq_nmf_zcoeff"], rtol=1e-8, atol=1e-10)
     np.testing.assert_allclose(pe, g["lsq_nmf_penalty"], rtol=1e-8, atol=1e-10)
+
+
+def _archetype_golden():
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "archetype_golden.npz"))
+
+
+def test_archetype_oracle_vs_redrock():
+    """The oracle's archetype fit (rebin x IGM, Legendre terms, batched
+    bounded solves, nearest archetypes) reproduces redrock's
+    get_best_archetype on every case of the fixture."""
+    from tests.archetype_cases import CASES, archetype_targets
+    g = _archetype_golden()
+    spec, tg = archetype_targets()
+    assert synth.targets_checksum(tg) == str(g["arch_targets_sha"])
+    assert synth.checksum([spec.wave, spec.flux]) == str(g["arch_flux_sha"])
+    arch = O.OArchetype(spec.wave, spec.flux, spec.rrtype, spec.subtype)
+    for name, (per_camera, nleg, nn, psig, method) in CASES.items():
+        for j, t in enumerate(tg):
+            sp = _ospectra(t)
+            z = t.ztrue
+            dwave = {s.wavehash: s.wave for s in sp}
+            w, f, wf = O.spectral_data(sp)
+            trans = {}
+            for hs, wv in dwave.items():
+                T = O.transmission_Lyman(np.array([z]), wv, model='Inoue14',
+                                         always_return_array=False)
+                trans[hs] = None if T is None else T[0]
+            ncam = len(dwave) if per_camera else 1
+            prior = (None if psig is None else
+                     O.prior_on_coeffs(1 if nn is None else nn, nleg, psig, ncam))
+            c2, co, ft = O.get_best_archetype(arch, sp, [s.band for s in t.spectra],
+                                              O.legendre_dict(dwave, nleg), w, f, wf, dwave, z,
+                                              per_camera, nn, trans, method, prior)
+            assert ft == str(g[f"arch_{name}_{j}_fulltype"]), (name, j)
+            np.testing.assert_allclose(c2, g[f"arch_{name}_{j}_chi2"], rtol=1e-10)
+            gc = g[f"arch_{name}_{j}_coeff"]
+            np.testing.assert_allclose(co, gc, rtol=0, atol=1e-8 * max(1.0, np.abs(gc).max()))
