@@ -35,7 +35,8 @@
  *   rr_zscan_pairs_grad     adjoint of the pair scan: dchi2/dz,
  *                           d2chi2/dz2, dchi2/dflux (Newton refinement in
  *                           place of fitz.py:255-261's parabola)
- *   rr_coadd                targets.py:267-373 Target.compute_coadd
+ *   rr_coadd, rr_coadd_ex,  targets.py:267-373 Target.compute_coadd
+ *   rr_coadd_cosmics        (with cosmic-ray rejection)
  *   rr_pack_g, rr_ygemm,    zscan.py:741-748 (y = Tb^T W f) for every
  *   rr_ygemm_i8 (+ slicing) (target, z) as one tensor-core GEMM per template
  */
@@ -430,7 +431,7 @@ int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t 
 
 /* ------------------------------------------------------------------------
  * Coadd of a target's exposures per wavelength grid (targets.py:267-373,
- * Target.compute_coadd with cosmics_nsig = 0).  Per group of nspec
+ * Target.compute_coadd).  Per group of nspec
  * exposures (entries first .. first + nspec - 1 of exp_data / exp_pix):
  *   ivar_out  = sum ivar;  flux_out = sum ivar flux / sum ivar (sum flux /
  *   nspec where sum ivar == 0);  rdata_out[d] = sum data[d] ivar / sum ivar
@@ -452,6 +453,23 @@ int rr_coadd(const rr_coadd_group* groups /* device */, int64_t ngroup, int64_t 
              const int64_t* exp_data, const int64_t* exp_pix, const double* rdata,
              const double* ivar, const double* flux, double* rdata_out, double* ivar_out,
              double* flux_out, rr_stream_t stream);
+/* rr_coadd with the resolution data weighted by ivar_rdata (NULL = ivar):
+ * after cosmic-ray rejection redrock weights R by the exposures' own ivar
+ * and the flux by the masked one (targets.py:300-301 vs 356-358). */
+int rr_coadd_ex(const rr_coadd_group* groups, int64_t ngroup, int64_t max_npix,
+                const int64_t* exp_data, const int64_t* exp_pix, const double* rdata,
+                const double* ivar_rdata, const double* ivar, const double* flux,
+                double* rdata_out, double* ivar_out, double* flux_out, rr_stream_t stream);
+/* Cosmic-ray rejection of compute_coadd(cosmics_nsig > 0), targets.py:310-354:
+ * ivar_out (layout of ivar, npix_total values) = ivar with the outlier
+ * pixels of groups of >= 2 exposures set to 0, bit-identical to redrock.
+ * wave holds each group's wavelengths at its out_pix offset; nsig2 =
+ * cosmics_nsig**2; work = 2 * npix_total doubles.  An exposure without a
+ * pixel of ivar > 0 sets *status = RR_EINVAL (numpy raises ValueError). */
+int rr_coadd_cosmics(const rr_coadd_group* groups, int64_t ngroup, const int64_t* exp_pix,
+                     const double* wave, const double* ivar, const double* flux, double nsig2,
+                     double* ivar_out, double* work, int64_t npix_total, int* status,
+                     rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * FMA throughput probe (no counterpart in redrock): the roofline

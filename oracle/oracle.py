@@ -14,7 +14,8 @@ Restates, in numpy/scipy (and a small C file for the rebin), redrock 0.22:
                         Calura12/Kamble20 igm.py:321-364)
   DistTemplate basis    py/redrock/templates.py:584-597
   spectral_data         py/redrock/zscan.py:192-209
-  Target.compute_coadd  py/redrock/targets.py:267-373 (cosmics_nsig = 0)
+  Target.compute_coadd  py/redrock/targets.py:267-373 (with the cosmic-ray
+                        rejection of :310-354)
   calc_zchi2_batch      py/redrock/zscan.py:626-781 (CPU branch :747-780)
   solve_matrices        py/redrock/zscan.py:1107-1201 (PCA, NMF/NNLS, BVLS)
   calc_negOII_penalty   py/redrock/zscan.py:783-800
@@ -290,8 +291,46 @@ class OSpectrum:
         self.Rcsr = spectrum_rcsr(rdata, roffsets, len(wave))
 
 
-def compute_coadd(exposures):
-    """Target.compute_coadd with cosmics_nsig = 0 (targets.py:267-373).
+def _cosmic_grad(wave, flux, ivar):
+    """One exposure's flux gradient and its variance (targets.py:310-332):
+    ivar == 0 pixels interpolated from ivar > 0 ones, ivar <= 0 left over
+    set to the smallest positive ivar."""
+    good = ivar > 0
+    bad = ivar == 0
+    tflux = flux.copy()
+    tivar = ivar.copy()
+    tflux[bad] = np.interp(wave[bad], wave[good], flux[good])
+    tivar[bad] = np.interp(wave[bad], wave[good], ivar[good])
+    bad = tivar <= 0
+    tivar[bad] = np.min(tivar[tivar > 0])
+    tvar = 1 / tivar
+    tflux[1:] = tflux[1:] - tflux[:-1]
+    tvar[1:] = tvar[1:] + tvar[:-1]
+    tflux[0] = 0
+    return tflux, tvar
+
+
+def cosmic_mask(wave, flux, ivar, nsig):
+    """ivar (nspec, npix) with the cosmic-ray outliers set to 0
+    (targets.py:337-354): gradient chi2 across exposures against nsig^2;
+    the exposure with the largest term of a flagged pixel is masked."""
+    ivar = np.array(ivar, dtype=np.float64)
+    grads = [_cosmic_grad(wave, f, v) for f, v in zip(flux, ivar)]
+    if len(grads) > 1 and nsig > 0:
+        grad = np.array([g[0] for g in grads])
+        gradivar = 1 / np.array([g[1] for g in grads])
+        nspec = grad.shape[0]
+        meangrad = np.sum(gradivar * grad, axis=0) / np.sum(gradivar)
+        deltagrad = grad - meangrad
+        chi2 = np.sum(gradivar * deltagrad ** 2, axis=0) / (nspec - 1)
+        for j in np.where(chi2 > nsig ** 2)[0]:
+            k = np.argmax(gradivar[:, j] * deltagrad[:, j] ** 2)
+            ivar[k][j] = 0.
+    return ivar
+
+
+def compute_coadd(exposures, cosmics_nsig=0.):
+    """Target.compute_coadd (targets.py:267-373).
 
     exposures: list of (band, wave, flux, ivar, rdata, roffsets), ivar already
     masked by its own resolution (Spectrum.__init__).  Returns one
@@ -313,6 +352,8 @@ def compute_coadd(exposures):
                 rdiags += np.asarray(e[4]) * e[3]
         flux = np.array([e[2] for e in group])
         ivar = np.array([e[3] for e in group])
+        if cosmics_nsig > 0:
+            ivar = cosmic_mask(group[0][1], flux, ivar, cosmics_nsig)
         unweighted = np.sum(flux, axis=0)
         weights = np.sum(ivar, axis=0)
         weighted = np.sum(ivar * flux, axis=0)

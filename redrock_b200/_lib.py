@@ -144,6 +144,10 @@ _SIGNATURES = {
     "rr_fma_peak": (c_int, [c_int, c_int, c_int, c_void_p, c_void_p]),
     "rr_coadd": (c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                          c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "rr_coadd_ex": (c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "rr_coadd_cosmics": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_double, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "rr_ygemm_kpad": (c_int64, [c_int64]),
     "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
                           c_void_p, c_void_p, c_void_p]),

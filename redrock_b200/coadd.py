@@ -12,8 +12,13 @@ applies redrock's 0.99 resolution-integral ivar mask.  ``compute_coadd`` is
 the per-target method form (installed on redrock's ``Target`` by
 ``redrock_b200.install``).
 
-Cosmic-ray rejection (``cosmics_nsig > 0``, off by default in redrock's DESI
-driver) is not implemented and raises ``NotImplementedError``.
+With ``cosmics_nsig > 0`` (off by default in redrock's DESI driver) the
+exposures' outlier pixels are first masked by ``rr_coadd_cosmics`` --
+gradient chi2 across the exposures of a grid against nsig^2, the worst
+exposure of each flagged pixel gets ivar 0 (targets.py:310-354) -- and the
+coadd then weights flux by the masked ivar and the resolution data by the
+exposures' own ivar, as redrock does.  Both steps are bit-identical to
+redrock's numpy.
 """
 
 from __future__ import annotations
@@ -25,7 +30,7 @@ import scipy.sparse
 import torch
 
 from . import _lib
-from .device import device, ptr, stream_handle, struct_bytes, to_device
+from .device import StatusWord, device, ptr, stream_handle, struct_bytes, to_device
 
 
 def _groups(target):
@@ -38,11 +43,8 @@ def _groups(target):
 
 def coadd_targets(targets, cache_Rcsr=False, cosmics_nsig=0.):
     """Replace each target's spectra by its per-grid coadds (in place)."""
-    if cosmics_nsig > 0:
-        raise NotImplementedError("cosmic-ray rejection in the coadd (cosmics_nsig > 0) is not "
-                                  "implemented by the GPU engine")
     plan = []
-    descs, rdata, ivar, flux, exp_data, exp_pix = [], [], [], [], [], []
+    descs, rdata, ivar, flux, exp_data, exp_pix, gwave = [], [], [], [], [], [], []
     d_off = p_off = out_pix = out_data = 0
     for t in targets:
         for key, specs in _groups(t):
@@ -64,6 +66,7 @@ def coadd_targets(targets, cache_Rcsr=False, cosmics_nsig=0.):
                 d_off += d.size
                 p_off += npix
             descs.append(_lib.CoaddGroup(npix, ndiag, len(specs), first, out_pix, out_data))
+            gwave.append(np.asarray(s0.wave, dtype=np.float64))
             plan.append((t, specs, npix, ndiag, out_pix, out_data))
             out_pix += npix
             out_data += ndiag * npix
@@ -81,13 +84,28 @@ def coadd_targets(targets, cache_Rcsr=False, cosmics_nsig=0.):
     oiv = torch.empty(max(out_pix, 1), dtype=torch.float64, device=dev)
     ofl = torch.empty(max(out_pix, 1), dtype=torch.float64, device=dev)
     max_npix = max(p[2] for p in plan)
+    div_w = div
+    if cosmics_nsig > 0:
+        # the cosmic-ray mask first; redrock's threshold is cosmics_nsig**2
+        div_w = torch.empty_like(div)
+        work = torch.empty(2 * div.numel(), dtype=torch.float64, device=dev)
+        dwv = to_device(np.concatenate(gwave))
+        st = StatusWord()
+        rc = L.rr_coadd_cosmics(ptr(dg), len(descs), ptr(dep), ptr(dwv), ptr(div), ptr(dfl),
+                                float(cosmics_nsig ** 2), ptr(div_w), ptr(work), div.numel(),
+                                st.ptr, stream_handle())
+        _lib.check(rc, "rr_coadd_cosmics")
+        if int(st.t.item()):
+            raise ValueError("cosmic-ray rejection: an exposure has no pixel with ivar > 0 "
+                             "(numpy.interp: array of sample points is empty)")
     for g0 in range(0, len(descs), 65535):
         # groups in slices of the grid's y limit; offsets stay global
         n = min(65535, len(descs) - g0)
         gsize = ctypes.sizeof(_lib.CoaddGroup)
-        rc = L.rr_coadd(dg.data_ptr() + g0 * gsize, n, max_npix, ptr(ded), ptr(dep), ptr(drd),
-                        ptr(div), ptr(dfl), ptr(ord_), ptr(oiv), ptr(ofl), stream_handle())
-        _lib.check(rc, "rr_coadd")
+        rc = L.rr_coadd_ex(dg.data_ptr() + g0 * gsize, n, max_npix, ptr(ded), ptr(dep), ptr(drd),
+                           ptr(div), ptr(div_w), ptr(dfl), ptr(ord_), ptr(oiv), ptr(ofl),
+                           stream_handle())
+        _lib.check(rc, "rr_coadd_ex")
     hrd, hiv, hfl = ord_.cpu().numpy(), oiv.cpu().numpy(), ofl.cpu().numpy()
     new = {}
     for t, specs, npix, ndiag, op, od in plan:

@@ -359,12 +359,13 @@ def make_targets(ntarget, seed=0, template=None, zrange=(0.0, 1.5), amp=1.0,
     return out
 
 
-def multi_exposure_targets(ntarget, seed=0, nexp=(1, 3)):
+def multi_exposure_targets(ntarget, seed=0, nexp=(1, 3), cosmics=0):
     """Targets with 1-3 exposures per camera -- the input of redrock's
     Target.compute_coadd.  Each exposure has its own resolution width,
     noise, extra noise on the flux and 5 % random masking; about 1 % of the
     pixels of each camera are masked in every exposure (the all-masked
-    branch of the coadd)."""
+    branch of the coadd).  ``cosmics`` > 0 adds that many cosmic-ray hits
+    per exposure: 1-3 adjacent pixels raised by 20-200 sigma."""
     rng = np.random.default_rng(seed)
     base = make_targets(ntarget, seed=seed + 1, mask_frac=0.0)
     out = []
@@ -379,6 +380,10 @@ def multi_exposure_targets(ntarget, seed=0, nexp=(1, 3)):
                 ivar = 1.0 / noise ** 2
                 ivar[(rng.uniform(size=npix) < 0.05) | dead] = 0.0
                 flux = s.flux + rng.normal(size=npix) * noise
+                for _ in range(cosmics):
+                    j = int(rng.integers(npix - 3))
+                    w = int(rng.integers(1, 4))
+                    flux[j:j + w] += rng.uniform(20.0, 200.0) * noise[j:j + w]
                 tg.spectra.append(SpectrumSpec(s.band, s.wave, flux, ivar, rdata, roff))
         out.append(tg)
     return out

@@ -222,3 +222,25 @@ def test_archetype_oracle_vs_redrock():
             np.testing.assert_allclose(c2, g[f"arch_{name}_{j}_chi2"], rtol=1e-10)
             gc = g[f"arch_{name}_{j}_coeff"]
             np.testing.assert_allclose(co, gc, rtol=0, atol=1e-8 * max(1.0, np.abs(gc).max()))
+
+
+@pytest.mark.parametrize("nsig", [4.0, 2.5])
+def test_coadd_cosmics_oracle_vs_redrock_golden(nsig):
+    """Cosmic-ray rejection in the oracle's coadd matches redrock's
+    Target(coadd=True, cosmics_nsig=nsig) bit for bit, and it masks pixels
+    (the coadds differ from the ones without rejection)."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "coadd_golden.npz"))
+    ct = synth.multi_exposure_targets(4, seed=62, cosmics=4)
+    assert synth.targets_checksum(ct) == str(g["cosmic_targets_sha"])
+    changed = 0
+    for it, t in enumerate(ct):
+        exps = [(s.band, s.wave, s.flux, O.masked_ivar(s.ivar, s.rdata, s.roffsets), s.rdata,
+                 s.roffsets) for s in t.spectra]
+        out = O.compute_coadd(exps, cosmics_nsig=nsig)
+        plain = O.compute_coadd(exps)
+        key = f"cosmic{nsig:g}_{it}"
+        assert len(out) == int(g[f"{key}_nspec"][1])
+        for j, ((band, wave, f, w, rd, ro), p) in enumerate(zip(out, plain)):
+            assert synth.checksum([f, w, rd]) == str(g[f"{key}_{j}_sha"]), (it, j)
+            changed += int(not np.array_equal(w, p[3]))
+    assert changed > 0
