@@ -160,9 +160,12 @@ __device__ bool nnls_solve(const double (&A)[NB][NB], const double (&b)[NB], dou
   }
 }
 
+// lo / hi point at the caller's bounds (read-only; in the plain chain the
+// kernel's __grid_constant__ parameter, so no local copies are made).
 template <int NB>
 __device__ bool bvls_solve(const double (&A)[NB][NB], const double (&b)[NB],
-                           const double (&lo)[NB], const double (&hi)[NB], double (&x)[NB]) {
+                           const double* __restrict__ lo, const double* __restrict__ hi,
+                           double (&x)[NB]) {
   constexpr double kTol = 1e-10;
   int onb[NB];  // -1 at lower bound, +1 at upper bound, 0 free
   int cols[NB];

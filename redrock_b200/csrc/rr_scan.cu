@@ -272,12 +272,11 @@ __global__ void plain_lsq_kernel(const double* __restrict__ mtri, const double* 
   if (method == RR_SOLVE_NNLS) {
     ok = nnls_solve<NB>(full, yy, c);
   } else {
-    double lo[NB], hi[NB];
-    for (int i = 0; i < NB; ++i) {
-      lo[i] = bounds.lo[i];
-      hi[i] = bounds.hi[i];
-    }
-    ok = bvls_solve<NB>(full, yy, lo, hi, c);
+    // the bounds are read in place from the parameter: with local copies
+    // (double lo[NB], hi[NB] filled from it) nvcc 12.9 gave the copies
+    // the same local-memory slots as the solver's own work arrays, and
+    // BVLS read its bounds from the overwritten storage
+    ok = bvls_solve<NB>(full, yy, bounds.lo, bounds.hi, c);
   }
   for (int i = 0; i < NB; ++i) zcoeff[(int64_t)z * NB + i] = ok ? c[i] : 0.0;
   bad[z] = ok ? 0 : 1;
