@@ -18,8 +18,9 @@ NEGATIVE_MODEL bit (zfind.py:470-580).
 
 It returns ``(allresults, allzfit)`` like redrock, except that ``allzfit`` is
 a dict of numpy columns (``astropy.table.Table(allzfit)`` gives redrock's
-table) with redrock's column names and order of rows.  Single-process only
-(``targets.comm`` None); redshift priors and chi2_scan input are not
+table) with redrock's column names and order of rows.  ``priors`` is a
+``redrock_b200.priors.Priors`` (or redrock's) object, or a prior file name.
+Single-process only (``targets.comm`` None); chi2_scan input is not
 supported.
 """
 
@@ -200,13 +201,21 @@ def _finalise_target(tid, fits, nminima, arch=None):
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
           n_nearest=None, prior_sigma=None, ncamera=None):
-    if priors is not None or chi2_scan is not None:
-        raise NotImplementedError("redshift priors and chi2_scan input are not supported by "
-                                  "the GPU zfind driver")
+    if chi2_scan is not None:
+        raise NotImplementedError("chi2_scan input (a redrock details file) is not supported "
+                                  "by the GPU zfind driver")
+    if priors is not None and not hasattr(priors, 'eval'):
+        from .priors import Priors
+        priors = Priors(priors)
     if targets.comm is not None and targets.comm.size > 1:
         raise NotImplementedError("use one process per GPU with its own targets (see "
                                   "redrock_b200.shard) instead of an MPI communicator")
     results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
+    if priors is not None:
+        # redshift prior on the coarse chi2 of every template (zfind.py:318-322)
+        for tg in results.keys():
+            for ft in results[tg].keys():
+                results[tg][ft]['zchi2'] += priors.eval(tg, results[tg][ft]['redshifts'])
     local = list(targets.local())
     # the targets' packed rows for the fine-grid pair scans do not depend on
     # the template: pack them once for every template's refinement

@@ -39,3 +39,36 @@ def test_zfind_vs_redrock(golden):
     g = golden["zfind_coeff"]
     scale = np.maximum(np.abs(g).max(axis=1, keepdims=True), 1e-300)
     assert np.all(np.abs(zfit["coeff"] - g) <= 1e-5 * scale)
+
+
+@pytest.mark.parametrize("name", ["gaussian", "tophat"])
+def test_zfind_with_priors_vs_redrock(name):
+    """Redshift priors (Gaussian, top-hat; one target without a prior) added
+    to the coarse chi2 before the refinement, as redrock's zfind does."""
+    import os
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.priors import Priors
+    from redrock_b200.zfind import zfind
+    from tests.prior_cases import prior_arrays, zfind_inputs
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "prior_golden.npz"))
+    ztg, sel = zfind_inputs()
+    tid, z0, sig, func = prior_arrays(name, ztg)
+    dz = T.DistTargetsCopy(T.from_synth(ztg))
+    dts = []
+    for ts in synth.template_set():
+        if ts.full_type in sel:
+            ts.redshifts = ts.redshifts[::sel[ts.full_type]]
+            dts.append(TM.DistTemplate(TM.from_synth(ts), dz.wavegrids()))
+    _, zfit = zfind(dz, dts, nminima=3, priors=Priors(targetid=tid, z=z0, sigma=sig,
+                                                      function=func))
+    cols = list(g[f"prior_{name}_columns"])
+    assert list(zfit.keys()) == cols
+    for k in ("targetid", "spectype", "subtype", "zwarn", "znum", "ncoeff", "npixels"):
+        np.testing.assert_array_equal(zfit[k], g[f"prior_{name}_{k}"], err_msg=k)
+    np.testing.assert_allclose(zfit["z"], g[f"prior_{name}_z"], rtol=0, atol=1e-7)
+    np.testing.assert_allclose(zfit["zerr"], g[f"prior_{name}_zerr"], rtol=1e-5)
+    assert np.max(np.abs(zfit["chi2"] - g[f"prior_{name}_chi2"])) <= 1e-3
+    d = zfit["deltachi2"] - g[f"prior_{name}_deltachi2"]
+    assert np.max(np.abs(d[np.isfinite(d)])) <= 1e-3
+    np.testing.assert_array_equal(np.isfinite(zfit["deltachi2"]),
+                                  np.isfinite(g[f"prior_{name}_deltachi2"]))

@@ -154,3 +154,23 @@ def test_find_minima_and_minfit():
     assert abs(x0 - 0.21) < 1e-12 and abs(xerr - 0.05) < 1e-12 and abs(y0 - 2.0) < 1e-9
     assert zw == 0
     assert minfit(x[:2], x[:2])[3] == 2 ** 10
+
+
+def test_prior_functions():
+    """priors.py:62-130: Gaussian and Lorentzian terms; the top-hat is 0
+    inside |z - z0| < width/2, NaN outside, +inf one point beyond each end
+    (or on the end point itself); a target without a prior adds 0."""
+    from redrock_b200.priors import Priors
+    z = np.linspace(0.0, 1.0, 11)
+    p = Priors(targetid=np.array([7]), z=np.array([0.5]), sigma=np.array([0.25]),
+               function='gaussian')
+    np.testing.assert_allclose(p.eval(7, z), ((z - 0.5) / 0.25) ** 2)
+    assert p.eval(8, z) == 0.0
+    np.testing.assert_allclose(Priors.lorentzien(z, 0.5, 0.25),
+                               -2 * np.log(1 / (1 + ((z - 0.5) / 0.25) ** 2)))
+    t = Priors.tophat(z, 0.5, 0.25)
+    assert np.isnan(t[:3]).all() and np.isnan(t[8:]).all()
+    assert t[3] == np.inf and t[7] == np.inf and (t[4:7] == 0).all()
+    t = Priors.tophat(z, 0.0, 0.25)
+    assert t[0] == 0 and t[1] == np.inf or t[0] == np.inf
+    assert np.isnan(Priors.tophat(z, 5.0, 0.1)).all()
