@@ -37,6 +37,7 @@
  *                           place of fitz.py:255-261's parabola)
  *   rr_coadd, rr_coadd_ex,  targets.py:267-373 Target.compute_coadd
  *   rr_coadd_cosmics        (with cosmic-ray rejection)
+ *   rr_archetype_fit        archetypes.py:228-400 archetype fits, batched
  *   rr_pack_g, rr_ygemm,    zscan.py:741-748 (y = Tb^T W f) for every
  *   rr_ygemm_i8 (+ slicing) (target, z) as one tensor-core GEMM per template
  */
@@ -469,6 +470,43 @@ int rr_coadd_ex(const rr_coadd_group* groups, int64_t ngroup, int64_t max_npix,
 int rr_coadd_cosmics(const rr_coadd_group* groups, int64_t ngroup, const int64_t* exp_pix,
                      const double* wave, const double* ivar, const double* flux, double nsig2,
                      double* ivar_out, double* work, int64_t npix_total, int* status,
+                     rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Archetype fits for many (target, redshift) pairs at once
+ * (archetypes.py:228-400: Archetype.get_best_archetype /
+ * nearest_neighbour_model, whose solves are calc_zchi2_batch and
+ * per_camera_coeff_with_least_square_batch, zscan.py:245-348, 626-781).
+ *
+ * Pair i: the target's pixels pix_off .. pix_off + npix - 1 of the
+ * concatenated band rows (npix x 11, row p multiplies basis rows
+ * pix_basis[p] - 5 .. + 5, as rr_pack_band_rows writes them), w, wflux =
+ * w f and flux; its archetype columns arch[arch_off + a * pix_stride + row]
+ * (a < narch: rebinned x IGM, zero outside the grids) and nl Legendre
+ * columns leg[leg_off + k * pix_stride + row].  Job j of pair i fits the m
+ * archetypes jobs[(i * njob + j) * m ..] followed by the nl Legendre
+ * columns: nb = m + nl <= RR_MAX_NBASIS coefficients solved from
+ * (Tb^T W Tb + prior) c = Tb^T W f with method RR_SOLVE_PCA / NNLS / BVLS
+ * (bounds: host [2][nb], NULL = unbounded), chi2 = sum w (f - Tb c)^2 (the
+ * prior excluded).  Outputs chi2[i * njob + j] and coeff[(i * njob + j) *
+ * nb ..]; a failed solve or an archetype index outside [0, narch) gives
+ * RR_HUGE_CHI2 and zero coefficients.  prior: device nb x nb or NULL.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int64_t pix_off;
+  int64_t npix;
+  int64_t arch_off;
+  int64_t leg_off;
+} rr_arch_pair;
+
+/* work: device scratch of rr_archetype_fit_work_bytes(npair, njob, m + nl) */
+size_t rr_archetype_fit_work_bytes(int64_t npair, int32_t njob, int32_t nb);
+int rr_archetype_fit(const rr_arch_pair* pairs /* device */, int64_t npair, const double* band,
+                     const int64_t* pix_basis, const double* w, const double* wflux,
+                     const double* flux, const double* arch, int32_t narch, const double* leg,
+                     int64_t pix_stride, const int32_t* jobs, int32_t njob, int32_t m,
+                     int32_t nl, const double* prior, int32_t method, const double* bounds,
+                     double* chi2, double* coeff, void* work, size_t work_bytes,
                      rr_stream_t stream);
 
 /* ------------------------------------------------------------------------

@@ -60,6 +60,11 @@ class ScanTemplate(ctypes.Structure):
                 ("zcoeff", c_void_p), ("penalty", c_void_p), ("y_ext", c_void_p)]
 
 
+class ArchPair(ctypes.Structure):
+    _fields_ = [("pix_off", c_int64), ("npix", c_int64), ("arch_off", c_int64),
+                ("leg_off", c_int64)]
+
+
 class CoaddGroup(ctypes.Structure):
     _fields_ = [("npix", c_int64), ("ndiag", c_int32), ("nspec", c_int32), ("first", c_int64),
                 ("out_pix", c_int64), ("out_data", c_int64)]
@@ -148,6 +153,11 @@ _SIGNATURES = {
                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_coadd_cosmics": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                  c_double, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "rr_archetype_fit_work_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
+    "rr_archetype_fit": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p, c_void_p, c_int32, c_void_p, c_int64, c_void_p,
+                                 c_int32, c_int32, c_int32, c_void_p, c_int32, c_void_p,
+                                 c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "rr_ygemm_kpad": (c_int64, [c_int64]),
     "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
                           c_void_p, c_void_p, c_void_p]),

@@ -45,6 +45,20 @@ def split_archetype_coeff(subtype, coeff, nbands, nleg):
     return archcoeff, [rest[i * nleg:(i + 1) * nleg] for i in range(nbands)]
 
 
+def per_camera_order(c, n_nbh, nleg, bands):
+    """Coefficients of one per-camera fit in redrock's order
+    (zscan.py:322-347): the n_nbh archetype terms, then for each band in
+    order of first appearance in ``bands`` the Legendre block of its last
+    occurrence."""
+    c = np.asarray(c)
+    out = [c[:n_nbh]]
+    if nleg >= 1:
+        blocks = np.split(c[n_nbh:], len(bands))
+        by_band = {b: blocks[i] for i, b in enumerate(bands)}
+        out += [by_band[b] for b in dict.fromkeys(bands)]
+    return np.concatenate(out)
+
+
 def _interp(x, xp, fp):
     """Linear interpolation that extrapolates the end segments, like
     scipy's interp1d(kind='linear', fill_value='extrapolate')."""
@@ -158,6 +172,179 @@ class Archetype:
             model = R.dot(model)
         return model
 
+    def best_archetypes(self, items, per_camera, n_nearest, solve_method='bvls', prior=None,
+                        max_bytes=1 << 31):
+        """get_best_archetype for many (target, z, trans) items at once:
+        the rebin of every archetype at every item's redshift (one launch
+        per grid), the basis assembly and the fits of all archetypes of
+        all items in one ``rr_archetype_fit`` launch, and with n_nearest a
+        second launch for the nearest-archetype combinations.  ``trans`` is
+        a dict of 1-D transmissions (or None) per grid, or None to compute
+        it.  ``prior`` is the prior of the n_nearest combination when
+        n_nearest is given (redrock's argument), else of the single fit.
+        Returns [(chi2, coefficients, fulltype)] in item order."""
+        out = [None] * len(items)
+        # items are processed in groups whose archetype columns fit max_bytes
+        from .engine import GridLayout
+        dwave_all = {}
+        for t, _, _ in items:
+            for s in t.spectra:
+                dwave_all.setdefault(s.wavehash, s.wave)
+        layout = GridLayout.from_dwave(dwave_all)
+        per_item = self._narch * layout.pix_stride * 8
+        step = max(1, int(max_bytes // max(per_item, 1)))
+        for i0 in range(0, len(items), step):
+            sub = items[i0:i0 + step]
+            res = self._fit_group(sub, layout, per_camera, n_nearest, solve_method, prior)
+            out[i0:i0 + len(sub)] = res
+        return out
+
+    def _fit_group(self, items, layout, per_camera, n_nearest, solve_method, prior):
+        from . import _lib
+        from .device import device, ptr, stream_handle, struct_bytes
+        from .engine import PlainTarget
+        from .templates import solve_code_of
+        from .zscan import HUGE_CHI2
+        dev = device()
+        L = _lib.lib()
+        npair = len(items)
+        # targets: band rows, weights and flux, concatenated
+        tix, tlist = {}, []
+        for t, _, _ in items:
+            if id(t) not in tix:
+                tix[id(t)] = len(tlist)
+                tlist.append(t)
+        pts = [PlainTarget(t.spectra, layout) for t in tlist]
+        offs = np.cumsum([0] + [pt.npix for pt in pts])
+        band = torch.cat([pt.band for pt in pts])
+        pixb = torch.cat([pt.pix_basis for pt in pts])
+        w = torch.cat([pt.w for pt in pts])
+        fl = torch.cat([pt.flux for pt in pts])
+        wf = torch.cat([pt.wflux for pt in pts])
+        for pt in pts:
+            pt._status.check("rr_pack_band_rows")
+        wsum = [float(np.sum(np.concatenate([s.ivar for s in t.spectra]))) for t in tlist]
+        # archetype columns (npair, narch, pix_stride): rebin x IGM
+        zs = np.array([float(z) for _, z, _ in items])
+        arch = torch.zeros((npair, self._narch, layout.pix_stride), dtype=torch.float64,
+                           device=dev)
+        for g, hs in enumerate(layout.keys):
+            wv = next(s.wave for t, _, _ in items for s in t.spectra if s.wavehash == hs)
+            n = layout.npix[g]
+            b = trapz_rebin(self.wave, self.dflux, wv, myz=zs, use_gpu=True)  # (npair, n, narch)
+            tr = np.ones((npair, n))
+            for i, (t, z, trans) in enumerate(items):
+                if trans is None:
+                    T = transmission_Lyman(z, wv, use_gpu=False, model=self.igm_model)
+                else:
+                    T = trans.get(hs)
+                    if T is not None:
+                        T = np.asarray(T)
+                        T = T[0] if T.ndim == 2 else T
+                if T is not None:
+                    tr[i] = T
+            b = b * to_device(tr)[:, :, None]
+            off = layout.pix_offset[g]
+            arch[:, :, off:off + n] = b.permute(0, 2, 1)
+        # Legendre columns, one set per distinct grid order of the targets
+        nleg = tlist[0].nleg
+        sets, set_of = {}, []
+        for t, _, _ in items:
+            hs_order = tuple(dict.fromkeys(s.wavehash for s in t.spectra))
+            key = (hs_order, tuple(t.bands) if per_camera else None)
+            if key not in sets:
+                leg = t.legendre(nleg)
+                ncam = len(t.bands) if per_camera else 1
+                nl = nleg * ncam
+                a = np.zeros((max(nl, 1), layout.pix_stride))
+                for i, hs in enumerate(hs_order):
+                    g = layout.index[hs]
+                    off, n = layout.pix_offset[g], layout.npix[g]
+                    for k in range(nleg):
+                        col = (i * nleg + k) if per_camera else k
+                        if col < nl:
+                            a[col, off:off + n] = leg[hs][k]
+                sets[key] = (len(sets), a, nl)
+            set_of.append(sets[key][0])
+        nls = {v[2] for v in sets.values()}
+        if len(nls) != 1:
+            raise ValueError("targets with different numbers of cameras in one archetype batch")
+        nl = nls.pop()
+        legs = [None] * len(sets)
+        for _, (k, a, _) in sets.items():
+            legs[k] = a
+        dleg = to_device(np.concatenate([a.ravel() for a in legs]))
+        leg_stride = max(nl, 1) * layout.pix_stride
+
+        def launch(m, jobs, njob, method, bounds, pri):
+            nb = m + nl
+            pairs = [_lib.ArchPair(int(offs[tix[id(t)]]), int(pts[tix[id(t)]].npix),
+                                   i * self._narch * layout.pix_stride, set_of[i] * leg_stride)
+                     for i, (t, _, _) in enumerate(items)]
+            dpairs = to_device(struct_bytes(pairs), torch.uint8)
+            djobs = to_device(np.ascontiguousarray(jobs, dtype=np.int32), torch.int32)
+            chi2 = torch.empty(npair * njob, dtype=torch.float64, device=dev)
+            co = torch.empty((npair * njob, nb), dtype=torch.float64, device=dev)
+            if pri is not None and np.shape(pri) != (nb, nb):
+                raise ValueError(f"prior of shape {np.shape(pri)} for {nb} coefficients")
+            dpri = None if pri is None else to_device(np.ascontiguousarray(pri, np.float64))
+            hb = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
+            nwork = int(L.rr_archetype_fit_work_bytes(npair, njob, nb))
+            work = torch.empty(max(nwork, 8), dtype=torch.uint8, device=dev)
+            rc = L.rr_archetype_fit(ptr(dpairs), npair, ptr(band), ptr(pixb), ptr(w), ptr(wf),
+                                    ptr(fl), ptr(arch), self._narch, ptr(dleg), layout.pix_stride,
+                                    ptr(djobs), njob, m, nl, ptr(dpri), method,
+                                    None if hb is None else hb.ctypes.data, ptr(chi2), ptr(co),
+                                    ptr(work), work.numel(), stream_handle())
+            _lib.check(rc, "rr_archetype_fit")
+            return (chi2.cpu().numpy().reshape(npair, njob),
+                    co.cpu().numpy().reshape(npair, njob, nb))
+
+        # every archetype with the Legendre terms (archetypes.py:369-393)
+        nb1 = 1 + nl
+        p1 = prior
+        if n_nearest is not None and prior is not None:
+            p1 = prior[n_nearest - 1:, ][:, n_nearest - 1:]
+        b1 = np.zeros((2, nb1))
+        b1[0][1:] = -np.inf
+        b1[1] = np.inf
+        code = solve_code_of(solve_method)
+        jobs = np.tile(np.arange(self._narch, dtype=np.int32), npair)
+        c2, co = launch(1, jobs, self._narch, code, b1 if code == _lib.RR_SOLVE_BVLS else None,
+                        p1 if per_camera else None)
+        for i, (t, _, _) in enumerate(items):
+            if wsum[tix[id(t)]] == 0:
+                c2[i] = HUGE_CHI2
+                co[i] = 0.0
+        if n_nearest is None:
+            res = []
+            for i, (t, _, _) in enumerate(items):
+                k = int(np.argmin(c2[i]))
+                c = per_camera_order(co[i, k], 1, nleg, t.bands) if per_camera else co[i, k]
+                res.append((c2[i, k], c, self._full_type[k]))
+            return res
+        # the n_nearest archetypes of lowest chi2 together (archetypes.py:228-294)
+        best = np.stack([np.argsort(c2[i])[0:n_nearest] for i in range(npair)])
+        nb2 = n_nearest + nl
+        if per_camera:
+            b2 = np.zeros((2, nb2))
+            b2[0][n_nearest:] = -np.inf
+            b2[1] = np.inf
+            c2n, con = launch(n_nearest, best.ravel(), 1, _lib.RR_SOLVE_BVLS, b2, prior)
+        else:
+            c2n, con = launch(n_nearest, best.ravel(), 1, _lib.RR_SOLVE_PCA, None, None)
+        res = []
+        for i, (t, _, _) in enumerate(items):
+            c = con[i, 0]
+            if wsum[tix[id(t)]] == 0:
+                c2n[i, 0] = HUGE_CHI2
+                c = np.zeros_like(c)
+            if per_camera:
+                c = per_camera_order(c, n_nearest, nleg, t.bands)
+            ft = make_fulltype(self._rrtype, ';'.join('%s' % self._subtype[k] for k in best[i]))
+            res.append((c2n[i, 0], c, ft))
+        return res
+
     def nearest_neighbour_model(self, target, weights, flux, wflux, dwave, z, n_nearest,
                                 zzchi2, trans, per_camera, dedges=None, binned=None,
                                 use_gpu=False, prior=None, ncam=None):
@@ -196,54 +383,17 @@ class Archetype:
                            trans=None, solve_method='bvls', prior=None, use_gpu=False):
         """Best archetype (or nearest-archetype combination) at redshift z
         (archetypes.py:295-400): every archetype is fitted with the target's
-        Legendre terms in one batched bounded solve.  ``trans`` (the IGM
-        transmission per grid at z, as (1, npix) arrays or None) is reduced
-        to 1-D in place, as redrock does.  Returns (chi2, coefficients,
-        fulltype)."""
-        nleg = target.nleg
-        legendre = target.legendre(nleg=nleg, use_gpu=True)
-        if trans is None:
-            trans = {hs: transmission_Lyman(z, w, use_gpu=False, model=self.igm_model)
-                     for hs, w in dwave.items()}
-        else:
+        Legendre terms in one batched launch (``best_archetypes``).  The
+        fit uses the target's own spectra (weights, flux and wflux are
+        redrock's concatenation of them).  ``trans`` (the IGM transmission
+        per grid at z, as (1, npix) arrays or None) is reduced to 1-D in
+        place, as redrock does.  Returns (chi2, coefficients, fulltype)."""
+        if trans is not None:
             for hs in trans:
                 if trans[hs] is not None:
                     trans[hs] = trans[hs][0, :]
-        binned = self.rebin_template_batch(z, dwave, trapz=True, use_gpu=True)
-        nnearest_prior = None
-        if n_nearest is not None:
-            nnearest_prior = prior.copy()
-            prior = prior[n_nearest - 1:, ][:, n_nearest - 1:]
-        tdata = {}
-        for hs in dwave:
-            if trans[hs] is not None:
-                binned[hs] = binned[hs] * to_device(np.asarray(trans[hs]))[:, None]
-            a = binned[hs].transpose(0, 1)[:, :, None]
-            if nleg > 0:
-                leg = to_device(legendre[hs]).transpose(0, 1)[None].expand(self._narch, -1, -1)
-                a = torch.cat([a, leg], dim=2)
-            tdata[hs] = a.contiguous()
-        nbasis = next(iter(tdata.values())).shape[2]
-        if per_camera:
-            zzchi2, zzcoeff = per_camera_coeff_with_least_square_batch(
-                target, tdata, weights, flux, wflux, nleg, self._narch, method=solve_method,
-                n_nbh=1, prior=prior, bands=target.bands)
-        else:
-            bounds = np.zeros((2, nbasis))
-            bounds[0][1:] = -np.inf
-            bounds[1] = np.inf
-            zzchi2, zzcoeff = calc_zchi2_batch(target.spectra, tdata, weights, flux, wflux,
-                                               self._narch, nbasis,
-                                               solve_matrices_algorithm=solve_method.upper(),
-                                               solver_args={'bounds': bounds})
-            zzcoeff = to_numpy(zzcoeff)
-        if n_nearest is not None:
-            ncam = len(dwave) if per_camera else 1
-            return self.nearest_neighbour_model(target, weights, flux, wflux, dwave, z,
-                                                n_nearest, zzchi2, trans, per_camera,
-                                                binned=binned, prior=nnearest_prior, ncam=ncam)
-        iBest = np.argmin(zzchi2)
-        return zzchi2[iBest], zzcoeff[iBest], self._full_type[iBest]
+        return self.best_archetypes([(target, z, trans)], per_camera, n_nearest,
+                                    solve_method=solve_method, prior=prior)[0]
 
 
 class All_archetypes:

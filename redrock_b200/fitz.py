@@ -275,9 +275,10 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                 r['zwarn'] |= BAD_MINFIT
             else:
                 raise ValueError('edges must be within input x range')
-            if archetype is not None:
-                _archetype_fit(targets[j], r, zmin, good, template, archetype, use_gpu,
-                               deg_legendre, per_camera, n_nearest, prior_sigma)
+        if archetype is not None:
+            _archetype_fits([(targets[j], r, zmin, good) for (j, r, zmin), good
+                             in zip(pending_final, ok)], template, archetype, use_gpu,
+                            deg_legendre, per_camera, n_nearest, prior_sigma)
 
     out = []
     for j, t in enumerate(targets):
@@ -303,10 +304,12 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     return out
 
 
-def _archetype_fit(target, r, zmin, good, template, archetype, use_gpu, deg_legendre,
-                   per_camera, n_nearest, prior_sigma):
-    """Replace a refined minimum's fit by the best archetype fit at its
-    redshift (fitz.py:263-293, 331-357).  The IGM transmission at the
+def _archetype_fits(pending, template, archetype, use_gpu, deg_legendre, per_camera, n_nearest,
+                    prior_sigma):
+    """Replace each refined minimum's fit by the best archetype fit at its
+    redshift (fitz.py:263-293, 331-357), all minima of the batch in one
+    ``best_archetypes`` call when the archetype set has it (redrock's own
+    Archetype is called per minimum).  The IGM transmission at the
     parabola minimum comes along as redrock computes it (none when the
     template could not be evaluated there).  redrock leaves ``ncamera``
     undefined when prior_sigma is None (a NameError); here it is the number
@@ -315,37 +318,55 @@ def _archetype_fit(target, r, zmin, good, template, archetype, use_gpu, deg_lege
     from .igm import transmission_Lyman
     from .templates import parse_fulltype
     from .zscan import spectral_data
-    spectra = target.spectra
-    dwave = {s.wavehash: s.wave for s in spectra}
-    weights, flux, wflux = spectral_data(spectra)
-    if target.nleg != deg_legendre or getattr(target, "_legendre", None) is None:
-        target.legendre(deg_legendre)
-    trans = {hs: None for hs in dwave}
-    if good:
-        for k in dwave:
-            trans[k] = transmission_Lyman(np.array([zmin]), dwave[k], use_gpu=False,
-                                          always_return_array=False, model=template.igm_model)
-        pca_coeff = np.asarray(r['coeff'])[0, :]
-    else:
-        pca_coeff = np.copy(r['coeff'])
-    ncamera = len(dwave) if per_camera else 1
+    items, extra = [], []
     prior = None
-    if prior_sigma is not None:
-        prior = prior_on_coeffs(1 if n_nearest is None else n_nearest, deg_legendre, prior_sigma,
-                                ncamera)
-    chi2min, coeff, fulltype = archetype.get_best_archetype(
-        target, weights, flux, wflux, dwave, r['z'], per_camera, n_nearest, trans=trans,
-        use_gpu=use_gpu, prior=prior)
-    subtype = parse_fulltype(fulltype)[1]
-    archcoeff, legcoeff = split_archetype_coeff(subtype, coeff, ncamera, deg_legendre)
-    if per_camera:
-        legcoeff = [np.vstack(legcoeff)]
-    prev = dict(r)
-    r.clear()   # redrock's key order for archetype results
-    r.update(z=prev['z'], zerr=prev['zerr'], zwarn=prev['zwarn'], chi2=chi2min, zz=prev['zz'],
-             zzchi2=prev['zzchi2'], coeff=archcoeff, legcoeff=legcoeff, fulltype=fulltype,
-             fitmethod=archetype.method, pca_coeff=pca_coeff,
-             pca_spectype=template._rrtype, pca_subtype=template.sub_type)
+    for target, r, zmin, good in pending:
+        dwave = {s.wavehash: s.wave for s in target.spectra}
+        if target.nleg != deg_legendre or getattr(target, "_legendre", None) is None:
+            target.legendre(deg_legendre)
+        trans = {hs: None for hs in dwave}
+        if good:
+            for k in dwave:
+                trans[k] = transmission_Lyman(np.array([zmin]), dwave[k], use_gpu=False,
+                                              always_return_array=False, model=template.igm_model)
+            pca_coeff = np.asarray(r['coeff'])[0, :]
+        else:
+            pca_coeff = np.copy(r['coeff'])
+        ncamera = len(dwave) if per_camera else 1
+        prior = None
+        if prior_sigma is not None:
+            prior = prior_on_coeffs(1 if n_nearest is None else n_nearest, deg_legendre,
+                                    prior_sigma, ncamera)
+        items.append((target, r['z'], trans))
+        extra.append((r, pca_coeff, ncamera, prior))
+    if not items:
+        return
+    if hasattr(archetype, "best_archetypes") and len({e[3] is None for e in extra}) == 1 \
+            and len({e[2] for e in extra}) == 1:
+        for _, _, trans in items:
+            for hs in trans:
+                if trans[hs] is not None:
+                    trans[hs] = trans[hs][0, :]
+        fits = archetype.best_archetypes(items, per_camera, n_nearest, prior=extra[0][3])
+    else:
+        fits = []
+        for (target, z, trans), (_, _, _, pri) in zip(items, extra):
+            w, f, wf = spectral_data(target.spectra)
+            dwave = {s.wavehash: s.wave for s in target.spectra}
+            fits.append(archetype.get_best_archetype(target, w, f, wf, dwave, z, per_camera,
+                                                     n_nearest, trans=trans, use_gpu=use_gpu,
+                                                     prior=pri))
+    for (chi2min, coeff, fulltype), (r, pca_coeff, ncamera, _) in zip(fits, extra):
+        subtype = parse_fulltype(fulltype)[1]
+        archcoeff, legcoeff = split_archetype_coeff(subtype, coeff, ncamera, deg_legendre)
+        if per_camera:
+            legcoeff = [np.vstack(legcoeff)]
+        prev = dict(r)
+        r.clear()   # redrock's key order for archetype results
+        r.update(z=prev['z'], zerr=prev['zerr'], zwarn=prev['zwarn'], chi2=chi2min,
+                 zz=prev['zz'], zzchi2=prev['zzchi2'], coeff=archcoeff, legcoeff=legcoeff,
+                 fulltype=fulltype, fitmethod=archetype.method, pca_coeff=pca_coeff,
+                 pca_spectype=template._rrtype, pca_subtype=template.sub_type)
 
 
 def fitz(zchi2, redshifts, target, template, nminima=3, archetype=None, use_gpu=False,

@@ -176,3 +176,40 @@ def test_zfind_with_archetypes_vs_redrock(ag, name):
         scale = np.maximum(np.abs(g[k]).reshape(len(g[k]), -1).max(axis=1), 1.0)
         d = np.abs(zfit[k] - g[k]).reshape(len(g[k]), -1).max(axis=1)
         assert np.all(d <= 1e-5 * scale), (k, d.max())
+
+
+@pytest.mark.parametrize("name", ["pc", "nc", "pcnn", "pc0"])
+def test_best_archetypes_batch_vs_oracle(name):
+    """best_archetypes: all targets' fits in one rr_archetype_fit launch (and
+    in groups of two through a small max_bytes) against the oracle's
+    per-target get_best_archetype."""
+    from oracle import oracle as O
+    from redrock_b200 import archetypes as A, fitz, targets as T
+    per_camera, nleg, nn, psig, method = CASES[name]
+    spec, tg = archetype_targets()
+    arch = A.Archetype.from_synth(spec)
+    oarch = O.OArchetype(spec.wave, spec.flux, spec.rrtype, spec.subtype)
+    rt = T.from_synth(tg)
+    items, want = [], []
+    for ts, t in zip(tg, rt):
+        for dz in (0.0, 0.01):
+            z = ts.ztrue + dz
+            t.legendre(nleg)
+            dwave, w, f, wf, trans = _fit_inputs(t, z)
+            items.append((t, z, trans))
+            ncam = len(dwave) if per_camera else 1
+            prior = (None if psig is None else
+                     fitz.prior_on_coeffs(1 if nn is None else nn, nleg, psig, ncam))
+            osp = [O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets)
+                   for s in ts.spectra]
+            otr = {hs: (None if trans[hs] is None else trans[hs][0]) for hs in trans}
+            want.append(O.get_best_archetype(oarch, osp, [s.band for s in ts.spectra],
+                                             O.legendre_dict(dwave, nleg), w, f, wf, dwave, z,
+                                             per_camera, nn, otr, method, prior))
+    for max_bytes in (1 << 31, 2 * arch._narch * 8200 * 8):
+        got = arch.best_archetypes(items, per_camera, nn, solve_method=method, prior=prior,
+                                   max_bytes=max_bytes)
+        for (c2, co, ft), (oc2, oco, oft) in zip(got, want):
+            assert ft == oft
+            np.testing.assert_allclose(c2, oc2, rtol=1e-8)
+            _close_coeff(co, oco)
