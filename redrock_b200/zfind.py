@@ -20,8 +20,9 @@ It returns ``(allresults, allzfit)`` like redrock, except that ``allzfit`` is
 a dict of numpy columns (``astropy.table.Table(allzfit)`` gives redrock's
 table) with redrock's column names and order of rows.  ``priors`` is a
 ``redrock_b200.priors.Priors`` (or redrock's) object, or a prior file name.
-Single-process only (``targets.comm`` None); chi2_scan input is not
-supported.
+``chi2_scan`` names a details file (``redrock_b200.results.write_zscan`` or
+redrock's) whose coarse scans replace the scan.  Single-process only
+(``targets.comm`` None).
 """
 
 from __future__ import annotations
@@ -201,16 +202,18 @@ def _finalise_target(tid, fits, nminima, arch=None):
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
           n_nearest=None, prior_sigma=None, ncamera=None):
-    if chi2_scan is not None:
-        raise NotImplementedError("chi2_scan input (a redrock details file) is not supported "
-                                  "by the GPU zfind driver")
     if priors is not None and not hasattr(priors, 'eval'):
         from .priors import Priors
         priors = Priors(priors)
     if targets.comm is not None and targets.comm.size > 1:
         raise NotImplementedError("use one process per GPU with its own targets (see "
                                   "redrock_b200.shard) instead of an MPI communicator")
-    results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
+    if chi2_scan is None:
+        results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
+    else:
+        # the coarse scans of a details file (zfind.py:298-301)
+        from .results import read_zscan_redrock
+        results = read_zscan_redrock(chi2_scan)
     if priors is not None:
         # redshift prior on the coarse chi2 of every template (zfind.py:318-322)
         for tg in results.keys():

@@ -72,3 +72,35 @@ def test_zfind_with_priors_vs_redrock(name):
     assert np.max(np.abs(d[np.isfinite(d)])) <= 1e-3
     np.testing.assert_array_equal(np.isfinite(zfit["deltachi2"]),
                                   np.isfinite(g[f"prior_{name}_deltachi2"]))
+
+
+def test_zfind_details_file_resume(golden, tmp_path):
+    """zfind -> write_zscan -> zfind(chi2_scan=file): the resumed run reads
+    the float32 coarse scans from the details file instead of scanning and
+    finds the same best redshifts (redrock's --chi2-scan path)."""
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.results import read_zfit, write_zscan
+    from redrock_b200.zfind import zfind
+    ztg = synth.make_targets(5, seed=41, amp=2.0, first_id=5000)
+    sel = {"GALAXY": 23, "QSO": 31, "STAR:::K": 4, "STAR:::M": 4}
+
+    def inputs():
+        dz = T.DistTargetsCopy(T.from_synth(ztg))
+        dts = []
+        for ts in synth.template_set():
+            if ts.full_type in sel:
+                ts.redshifts = ts.redshifts[::sel[ts.full_type]]
+                dts.append(TM.DistTemplate(TM.from_synth(ts), dz.wavegrids()))
+        return dz, dts
+
+    res, zfit = zfind(*inputs(), nminima=3)
+    fn = str(tmp_path / "rrdetails.h5")
+    write_zscan(fn, res, zfit)
+    back = read_zfit(fn)
+    np.testing.assert_array_equal(back['targetid'], zfit['targetid'])
+    _, zfit2 = zfind(*inputs(), nminima=3, chi2_scan=fn)
+    best = zfit['znum'] == 0
+    best2 = zfit2['znum'] == 0
+    np.testing.assert_array_equal(zfit2['targetid'][best2], zfit['targetid'][best])
+    np.testing.assert_array_equal(zfit2['spectype'][best2], zfit['spectype'][best])
+    np.testing.assert_allclose(zfit2['z'][best2], zfit['z'][best], rtol=0, atol=1e-6)
