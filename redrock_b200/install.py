@@ -35,6 +35,11 @@ PATCHES = {
         ("zscan", "per_camera_coeff_with_least_square_batch"),
     ("zscan", "per_camera_coeff_with_least_square_batch"):
         ("zscan", "per_camera_coeff_with_least_square_batch"),
+    ("results", "write_zscan"): ("results", "write_zscan"),
+    ("results", "read_zscan"): ("results", "read_zscan"),
+    ("results", "read_zfit"): ("results", "read_zfit"),
+    ("results", "read_zscan_redrock"): ("results", "read_zscan_redrock"),
+    ("zfind", "read_zscan_redrock"): ("results", "read_zscan_redrock"),
 }
 # methods of redrock classes: (module, class, method) -> (our module, function)
 METHOD_PATCHES = {
