@@ -15,8 +15,8 @@ back to the host for the argmin / argsort.
 
 ``Archetype`` mirrors redrock's class.  It is built from arrays
 (``Archetype(wave=..., flux=..., rrtype=..., subtype=...)`` or
-``Archetype.from_synth``) or, when astropy is importable, from a
-redrock-format archetype file.  redrock's own ``Archetype`` also runs on the
+``Archetype.from_synth``) or from a redrock-format archetype file (read
+with astropy when it is installed, else with ``redrock_b200.fits``).  redrock's own ``Archetype`` also runs on the
 GPU once ``redrock_b200.install`` has rebound its ``trapz_rebin``,
 ``transmission_Lyman``, ``calc_zchi2_batch`` and
 ``per_camera_coeff_with_least_square_batch``.
@@ -72,19 +72,26 @@ def _interp(x, xp, fp):
 
 
 def _read_archetype_file(filename):
+    """(wave, flux, rrtype, subtypes, version) of a redrock archetype file
+    (archetypes.py:35-58): astropy when installed, else the FITS table
+    reader of redrock_b200.fits."""
+    filename = os.path.expandvars(filename)
     try:
         from astropy.io import fits
-    except ImportError as e:
-        raise ImportError("reading a redrock archetype file needs astropy; build the "
-                          "Archetype from arrays instead") from e
-    with fits.open(os.path.expandvars(filename), memmap=False) as h:
-        hdr = h['ARCHETYPES'].header
-        flux = np.asarray(h['ARCHETYPES'].data['ARCHETYPE']).astype('float64')
-        sub = [str(s).strip() for s in h['ARCHETYPES'].data['SUBTYPE']]
-        wave = np.asarray(hdr['CRVAL1'] + hdr['CDELT1'] * np.arange(flux.shape[1]))
-        if hdr['LOGLAM']:
-            wave = 10 ** wave
-        return wave, flux, hdr['RRTYPE'].strip(), sub, hdr['VERSION']
+        with fits.open(filename, memmap=False) as h:
+            hdr = h['ARCHETYPES'].header
+            flux = np.asarray(h['ARCHETYPES'].data['ARCHETYPE']).astype('float64')
+            sub = np.asarray(h['ARCHETYPES'].data['SUBTYPE'])
+    except ImportError:
+        from .fits import read_table
+        hdr, rows = read_table(filename, 'ARCHETYPES')
+        flux = np.asarray(rows['ARCHETYPE']).astype('float64')
+        sub = rows['SUBTYPE']
+    sub = [str(s).strip() for s in np.char.strip(np.asarray(sub).astype(str))]
+    wave = np.asarray(hdr['CRVAL1'] + hdr['CDELT1'] * np.arange(flux.shape[1]))
+    if hdr['LOGLAM']:
+        wave = 10 ** wave
+    return wave, flux, hdr['RRTYPE'].strip(), sub, hdr['VERSION']
 
 
 class Archetype:

@@ -108,3 +108,53 @@ def test_hdf5_large_group_and_empty(tmp_path):
     np.testing.assert_array_equal(f['g/599'], np.arange(4))
     assert f['s'] == 2.5 and f['e'].shape == (0, 3)
     assert 'g/600' not in f
+
+
+REF_ARCH = "/root/reference/py/redrock/test/data/rrarchetype-galaxy-test.fits"
+
+
+@pytest.mark.skipif(not os.path.exists(REF_ARCH), reason="reference test data not present")
+def test_archetype_file_as_redrock_reads_it():
+    """Archetype(filename) without astropy gives the arrays redrock's own
+    Archetype builds from the same file (redrock run here with
+    astropy.io.fits.open served by the FITS reader)."""
+    import sys
+    from redrock_b200 import fits as F
+    from redrock_b200.archetypes import Archetype
+    a = Archetype(REF_ARCH)
+    assert a._narch == 2 and a.flux.shape == (2, 48860)
+    assert a._rrtype == 'GALAXY' and a.version == 'v3.0'
+    assert list(a._subtype) == ['LRG_0', 'ELG_1']
+    assert list(a.full_type) == ['GALAXY:::LRG_0', 'GALAXY:::ELG_1']
+    np.testing.assert_allclose(a.wave[:2], [1228.0701754386, 1228.2701754386])
+    before = set(sys.modules)
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import import_redrock
+
+    class _H:
+        def __init__(self, fn):
+            self.h = {h.header.get('EXTNAME', ''): h for h in F.read_hdus(fn)}
+
+        def __getitem__(self, k):
+            return self.h[k]
+
+        def close(self):
+            pass
+
+    rr = import_redrock()
+    import redrock.archetypes as ra
+    old = sys.modules["astropy.io.fits"].open
+    ra.fits.open = lambda fn, memmap=False: _H(fn)
+    try:
+        ref = ra.Archetype(REF_ARCH)
+    finally:
+        ra.fits.open = old
+        # drop redrock and the astropy stand-ins again
+        for name in set(sys.modules) - before:
+            if name.split(".")[0] in ("redrock", "astropy", "fitsio", "make_golden"):
+                del sys.modules[name]
+    np.testing.assert_array_equal(a.flux, ref.flux)
+    np.testing.assert_array_equal(a.wave, ref.wave)
+    assert list(a._subtype) == list(ref._subtype)
+    assert list(a._full_type) == list(ref._full_type)
+    assert a._rrtype == ref._rrtype and a.version == ref._version
