@@ -3,8 +3,9 @@
 A prior adds a function of (z - z0) / sigma to each target's coarse chi2(z)
 of every template before the fine-grid refinement (zfind.py:318-322).  The
 per-target (z0, sigma) and the function name come from redrock's prior file
-(a FITS table PRIORS with TARGETID, Z, SIGMA, FUNCTION); here they can also
-be given as arrays.
+(a FITS table PRIORS with TARGETID, Z, SIGMA, FUNCTION, read with astropy
+or, without it, with ``redrock_b200.fits``); they can also be given as
+arrays.
 """
 
 from __future__ import annotations
@@ -19,16 +20,21 @@ class Priors:
 
     def __init__(self, filename=None, targetid=None, z=None, sigma=None, function='gaussian'):
         if filename is not None:
+            filename = os.path.expandvars(filename)
             try:
                 from astropy.io import fits
-            except ImportError as e:
-                raise ImportError("reading a redrock prior file needs astropy; build Priors "
-                                  "from arrays instead") from e
-            with fits.open(os.path.expandvars(filename), memmap=False) as h:
-                targetid = h['PRIORS'].data['TARGETID']
-                z = h['PRIORS'].data['Z']
-                sigma = h['PRIORS'].data['SIGMA']
-                function = h['PRIORS'].data['FUNCTION'][0]
+                with fits.open(filename, memmap=False) as h:
+                    rows = h['PRIORS'].data
+                    targetid, z, sigma = rows['TARGETID'], rows['Z'], rows['SIGMA']
+                    function = rows['FUNCTION'][0]
+            except ImportError:
+                from .fits import read_table
+                _, rows = read_table(filename, 'PRIORS')
+                targetid, z, sigma = rows['TARGETID'], rows['Z'], rows['SIGMA']
+                function = rows['FUNCTION'][0]
+            if isinstance(function, bytes):
+                function = function.decode()
+            function = str(function).strip()
         z = np.asarray(z)
         self._param = {targetid[i]: {'Z': z[i], 'SIGMA': sigma[i]} for i in range(z.size)}
         self._type = function
