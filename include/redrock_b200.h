@@ -499,12 +499,16 @@ typedef struct {
   int64_t leg_off;
 } rr_arch_pair;
 
-/* work: device scratch of rr_archetype_fit_work_bytes(npair, njob, m + nl) */
-size_t rr_archetype_fit_work_bytes(int64_t npair, int32_t njob, int32_t nb);
+/* work: device scratch of rr_archetype_fit_work_bytes(npair, njob, m, nl, max_npix),
+ * max_npix >= every pair's npix (R L of each pair's Legendre columns is
+ * built once there and shared by the pair's jobs) */
+size_t rr_archetype_fit_work_bytes(int64_t npair, int32_t njob, int32_t m, int32_t nl,
+                                   int64_t max_npix);
 int rr_archetype_fit(const rr_arch_pair* pairs /* device */, int64_t npair, const double* band,
                      const int64_t* pix_basis, const double* w, const double* wflux,
-                     const double* flux, const double* arch, int32_t narch, const double* leg,
-                     int64_t pix_stride, const int32_t* jobs, int32_t njob, int32_t m,
+                     const double* flux, int64_t max_npix, const double* arch, int32_t narch,
+                     const double* leg, int64_t pix_stride, const int32_t* jobs, int32_t njob,
+                     int32_t m,
                      int32_t nl, const double* prior, int32_t method, const double* bounds,
                      double* chi2, double* coeff, void* work, size_t work_bytes,
                      rr_stream_t stream);

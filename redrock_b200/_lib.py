@@ -153,11 +153,11 @@ _SIGNATURES = {
                             c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "rr_coadd_cosmics": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                  c_double, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
-    "rr_archetype_fit_work_bytes": (c_size_t, [c_int64, c_int32, c_int32]),
+    "rr_archetype_fit_work_bytes": (c_size_t, [c_int64, c_int32, c_int32, c_int32, c_int64]),
     "rr_archetype_fit": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
-                                 c_void_p, c_void_p, c_int32, c_void_p, c_int64, c_void_p,
-                                 c_int32, c_int32, c_int32, c_void_p, c_int32, c_void_p,
-                                 c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+                                 c_void_p, c_int64, c_void_p, c_int32, c_void_p, c_int64,
+                                 c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int32,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "rr_ygemm_kpad": (c_int64, [c_int64]),
     "rr_pack_g": (c_int, [ctypes.POINTER(ScanTargets), c_int64, c_int64, c_int64, c_void_p,
                           c_void_p, c_void_p, c_void_p]),

@@ -296,10 +296,12 @@ class Archetype:
                 raise ValueError(f"prior of shape {np.shape(pri)} for {nb} coefficients")
             dpri = None if pri is None else to_device(np.ascontiguousarray(pri, np.float64))
             hb = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
-            nwork = int(L.rr_archetype_fit_work_bytes(npair, njob, nb))
+            max_npix = max(pt.npix for pt in pts)
+            nwork = int(L.rr_archetype_fit_work_bytes(npair, njob, m, nl, max_npix))
             work = torch.empty(max(nwork, 8), dtype=torch.uint8, device=dev)
             rc = L.rr_archetype_fit(ptr(dpairs), npair, ptr(band), ptr(pixb), ptr(w), ptr(wf),
-                                    ptr(fl), ptr(arch), self._narch, ptr(dleg), layout.pix_stride,
+                                    ptr(fl), max_npix, ptr(arch), self._narch, ptr(dleg),
+                                    layout.pix_stride,
                                     ptr(djobs), njob, m, nl, ptr(dpri), method,
                                     None if hb is None else hb.ctypes.data, ptr(chi2), ptr(co),
                                     ptr(work), work.numel(), stream_handle())
