@@ -293,6 +293,7 @@ def run_ours(args, rank, world, local_rank):
 
     study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
     adj = adjoint_study(rtg, tms, torch) if (args.adjoint and rank == 0) else None
+    arc = archetype_study(tg, rtg, torch) if (args.archetypes and rank == 0) else None
 
     # ---- end to end through the public API, host buffers ------------------
     e2e = None
@@ -410,6 +411,8 @@ def run_ours(args, rank, world, local_rank):
         out["ygemm_study"] = study
     if adj is not None:
         out["adjoint"] = adj
+    if arc is not None:
+        out["archetypes"] = arc
     return out
 
 
@@ -442,6 +445,34 @@ def adjoint_study(rtg, tms, torch):
     return {"pairs": npairs, "ms": ms, "value": npairs / (ms / 1e3),
             "unit": "gradient evals/s (chi2, dchi2/dz, d2chi2/dz2, dchi2/dflux per (target, z))",
             "kernel": "zscan_pairs_kernel<NB, grad> (template rebinned + IGM per pair)"}
+
+
+def archetype_study(tg, rtg, torch, narch=24):
+    """Archetype refits (archetypes.py:295-400) of every target of the
+    workload at its true redshift: per-camera fits with 2 Legendre terms per
+    camera and prior sigma 0.1 against narch synthetic GALAXY archetypes,
+    all targets in one best_archetypes call (rebin x IGM of every archetype
+    at every redshift, then the rr_archetype_fit launches)."""
+    from redrock_b200 import archetypes as A, fitz, synth
+    arch = A.Archetype.from_synth(synth.archetype_set(narch=narch, seed=5))
+    items = []
+    for t, ts in zip(rtg, tg):
+        t.legendre(2)
+        items.append((t, ts.ztrue, None))
+    prior = fitz.prior_on_coeffs(1, 2, 0.1, 3)
+    arch.best_archetypes(items, True, None, prior=prior)   # warm-up
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    arch.best_archetypes(items, True, None, prior=prior)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    nfit = len(items) * narch
+    return {"fits": nfit, "ms": ms, "value": nfit / (ms / 1e3),
+            "unit": "archetype fits/s (one archetype + per-camera Legendre terms at one z)",
+            "kernels": "arch_pair_kernel, arch_gram_kernel, arch_solve_kernel (+ rr_trapz_rebin)"}
 
 
 def ygemm_study(args, step, torch, evals):
@@ -572,6 +603,8 @@ def main():
     ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
                     help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
                          "summed in the FP64 scan (fp64)")
+    ap.add_argument("--archetypes", action="store_true",
+                    help="also time batched archetype refits of every target (24 archetypes)")
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the adjoint pair kernel on 3 redshifts per target and template")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",

@@ -221,15 +221,14 @@ class Archetype:
             if id(t) not in tix:
                 tix[id(t)] = len(tlist)
                 tlist.append(t)
-        pts = [PlainTarget(t.spectra, layout) for t in tlist]
-        offs = np.cumsum([0] + [pt.npix for pt in pts])
-        band = torch.cat([pt.band for pt in pts])
-        pixb = torch.cat([pt.pix_basis for pt in pts])
-        w = torch.cat([pt.w for pt in pts])
-        fl = torch.cat([pt.flux for pt in pts])
-        wf = torch.cat([pt.wflux for pt in pts])
-        for pt in pts:
-            pt._status.check("rr_pack_band_rows")
+        # band rows of every target's spectra in one pack (rows are per pixel)
+        allspec = [sp for t in tlist for sp in t.spectra]
+        pt_all = PlainTarget(allspec, layout)
+        pt_all._status.check("rr_pack_band_rows")
+        npix_t = [sum(len(sp.wave) for sp in t.spectra) for t in tlist]
+        offs = np.cumsum([0] + npix_t)
+        band, pixb, w, fl, wf = (pt_all.band, pt_all.pix_basis, pt_all.w, pt_all.flux,
+                                 pt_all.wflux)
         wsum = [float(np.sum(np.concatenate([s.ivar for s in t.spectra]))) for t in tlist]
         # archetype columns (npair, narch, pix_stride): rebin x IGM
         zs = np.array([float(z) for _, z, _ in items])
@@ -239,17 +238,17 @@ class Archetype:
             wv = next(s.wave for t, _, _ in items for s in t.spectra if s.wavehash == hs)
             n = layout.npix[g]
             b = trapz_rebin(self.wave, self.dflux, wv, myz=zs, use_gpu=True)  # (npair, n, narch)
+            # IGM: given per item, or redrock's transmission_Lyman(z, wave) for
+            # the items without one, all their redshifts in one call
             tr = np.ones((npair, n))
-            for i, (t, z, trans) in enumerate(items):
-                if trans is None:
-                    T = transmission_Lyman(z, wv, use_gpu=False, model=self.igm_model)
-                else:
-                    T = trans.get(hs)
-                    if T is not None:
-                        T = np.asarray(T)
-                        T = T[0] if T.ndim == 2 else T
-                if T is not None:
-                    tr[i] = T
+            need = [i for i, (_, _, trans) in enumerate(items) if trans is None]
+            if need:
+                tr[need] = np.asarray(transmission_Lyman(zs[need], wv, use_gpu=False,
+                                                         model=self.igm_model)).reshape(len(need), n)
+            for i, (_, _, trans) in enumerate(items):
+                if trans is not None and trans.get(hs) is not None:
+                    T = np.asarray(trans[hs])
+                    tr[i] = T[0] if T.ndim == 2 else T
             b = b * to_device(tr)[:, :, None]
             off = layout.pix_offset[g]
             arch[:, :, off:off + n] = b.permute(0, 2, 1)
@@ -285,7 +284,7 @@ class Archetype:
 
         def launch(m, jobs, njob, method, bounds, pri):
             nb = m + nl
-            pairs = [_lib.ArchPair(int(offs[tix[id(t)]]), int(pts[tix[id(t)]].npix),
+            pairs = [_lib.ArchPair(int(offs[tix[id(t)]]), int(npix_t[tix[id(t)]]),
                                    i * self._narch * layout.pix_stride, set_of[i] * leg_stride)
                      for i, (t, _, _) in enumerate(items)]
             dpairs = to_device(struct_bytes(pairs), torch.uint8)
@@ -296,7 +295,7 @@ class Archetype:
                 raise ValueError(f"prior of shape {np.shape(pri)} for {nb} coefficients")
             dpri = None if pri is None else to_device(np.ascontiguousarray(pri, np.float64))
             hb = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float64)
-            max_npix = max(pt.npix for pt in pts)
+            max_npix = max(npix_t)
             nwork = int(L.rr_archetype_fit_work_bytes(npair, njob, m, nl, max_npix))
             work = torch.empty(max(nwork, 8), dtype=torch.uint8, device=dev)
             rc = L.rr_archetype_fit(ptr(dpairs), npair, ptr(band), ptr(pixb), ptr(w), ptr(wf),

@@ -714,13 +714,17 @@ class PlainTarget:
         self.band = torch.empty((self.npix, 2 * _lib.HALF_BAND + 1), dtype=torch.float64,
                                 device=dev)
         dspecs = to_device(struct_bytes(descs), torch.uint8)
-        drdata = to_device(np.concatenate(rdata))
+        # gathered once, straight into pinned memory, for the upload
+        pinned = {}
+        hrdata = _concat(rdata, np.float64, pinned, "rdata")
+        t = pinned.get("rdata")
+        drdata = t.to(dev, non_blocking=True) if t is not None else to_device(hrdata)
         droff = to_device(np.concatenate(roffs), torch.int32)
         st = StatusWord(dev)
         rc = L.rr_pack_band_rows(ptr(dspecs), len(descs), ptr(drdata), ptr(droff), self.npix,
                                  ptr(self.band), st.ptr, stream_handle(stream))
         _lib.check(rc, "rr_pack_band_rows")
-        self._keep = (dspecs, drdata, droff)
+        self._keep = (dspecs, drdata, droff, pinned)
         self._status = st
 
 

@@ -320,6 +320,20 @@ def _archetype_fits(pending, template, archetype, use_gpu, deg_legendre, per_cam
     from .zscan import spectral_data
     items, extra = [], []
     prior = None
+    # transmission_Lyman(zmin, wave) of every good minimum, one call per grid
+    # (None where redrock's always_return_array=False gives None)
+    tgrid = {}
+    if template.igm_model not in ('None', None):
+        for target, r, zmin, good in pending:
+            for s in target.spectra:
+                tgrid.setdefault(s.wavehash, s.wave)
+    zgood = np.array([zmin for _, _, zmin, good in pending if good], dtype=np.float64)
+    tvals = {}
+    if len(zgood):
+        for hs, wv in tgrid.items():
+            tvals[hs] = np.asarray(transmission_Lyman(zgood, wv, use_gpu=False,
+                                                      model=template.igm_model)).reshape(len(zgood), -1)
+    igood = 0
     for target, r, zmin, good in pending:
         dwave = {s.wavehash: s.wave for s in target.spectra}
         if target.nleg != deg_legendre or getattr(target, "_legendre", None) is None:
@@ -327,8 +341,10 @@ def _archetype_fits(pending, template, archetype, use_gpu, deg_legendre, per_cam
         trans = {hs: None for hs in dwave}
         if good:
             for k in dwave:
-                trans[k] = transmission_Lyman(np.array([zmin]), dwave[k], use_gpu=False,
-                                              always_return_array=False, model=template.igm_model)
+                lyman = np.min(dwave[k]) / (1. + zmin) <= 1215.67
+                if k in tvals and lyman:
+                    trans[k] = tvals[k][igood][None, :]
+            igood += 1
             pca_coeff = np.asarray(r['coeff'])[0, :]
         else:
             pca_coeff = np.copy(r['coeff'])
