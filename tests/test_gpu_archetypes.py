@@ -213,3 +213,35 @@ def test_best_archetypes_batch_vs_oracle(name):
             assert ft == oft
             np.testing.assert_allclose(c2, oc2, rtol=1e-8)
             _close_coeff(co, oco)
+
+
+@pytest.mark.parametrize("per_camera,nleg", [(True, 2), (False, 2), (False, 0)])
+def test_archetype_multi_exposure_target_vs_oracle(per_camera, nleg):
+    """redrock's own archetype unit case (test_archetypes.py:55-95): a
+    target with two exposures per camera (util.get_target), bands set to
+    ['b', 'r'], z = 0.5, with and without Legendre terms: coefficient
+    counts 1 + nleg * 2 (per camera) / 1 + nleg, and the fit against the
+    oracle."""
+    from oracle import oracle as O
+    from redrock_b200 import archetypes as A, fitz, targets as T
+    from redrock_b200.zscan import spectral_data
+    spec, _ = archetype_targets()
+    arch = A.Archetype.from_synth(spec)
+    oarch = O.OArchetype(spec.wave, spec.flux, spec.rrtype, spec.subtype)
+    ut = synth.util_target(0.5, seed=23, targetid=123)
+    t = T.from_synth([ut])[0]
+    t.bands = ['b', 'r']
+    t.nleg = nleg
+    dwave = {s.wavehash: s.wave for s in t.spectra}
+    w, f, wf = spectral_data(t.spectra)
+    prior = fitz.prior_on_coeffs(1, nleg, 0.1, len(dwave)) if nleg else None
+    c2, co, ft = arch.get_best_archetype(t, w, f, wf, dwave, 0.5, per_camera, None, trans=None,
+                                         solve_method='bvls', prior=prior)
+    assert len(co) == (1 + nleg * len(t.bands) if per_camera else 1 + nleg)
+    osp = [O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets) for s in ut.spectra]
+    oc2, oco, oft = O.get_best_archetype(oarch, osp, ['b', 'r'], O.legendre_dict(dwave, nleg),
+                                         w, f, wf, dwave, 0.5, per_camera, None, None, 'bvls',
+                                         prior)
+    assert ft == oft
+    np.testing.assert_allclose(c2, oc2, rtol=1e-8)
+    _close_coeff(co, oco)

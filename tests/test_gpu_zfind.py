@@ -98,6 +98,26 @@ def test_zfind_details_file_resume(golden, tmp_path):
     write_zscan(fn, res, zfit)
     back = read_zfit(fn)
     np.testing.assert_array_equal(back['targetid'], zfit['targetid'])
+    # redrock's test_io.py:45-85 checks on the same round trip
+    from redrock_b200.results import read_zscan
+    zfit1 = {k: v for k, v in zfit.items() if k != 'fitmethod'}
+    fn1 = str(tmp_path / "rrdetails1.h5")
+    write_zscan(fn1, res, zfit1)
+    write_zscan(fn1, res, zfit1, clobber=True)
+    zscan2, zfit2 = read_zscan(fn1)
+    assert list(zfit2.keys()) == list(zfit1.keys())
+    assert zfit2['z'].dtype == zfit1['z'].dtype
+    assert zfit2['targetid'].dtype == zfit1['targetid'].dtype
+    for cn in zfit1:
+        d2 = zfit2[cn]
+        np.testing.assert_equal(np.asarray(zfit1[cn]).astype(d2.dtype), d2)
+    for tid in res:
+        for ft in res[tid]:
+            for key in ('redshifts', 'zchi2', 'penalty', 'zcoeff'):
+                d1 = np.asarray(res[tid][ft][key])
+                if key != 'redshifts':
+                    d1 = d1.astype(np.float32)
+                np.testing.assert_equal(d1, zscan2[tid][ft][key])
     _, zfit2 = zfind(*inputs(), nminima=3, chi2_scan=fn)
     best = zfit['znum'] == 0
     best2 = zfit2['znum'] == 0
