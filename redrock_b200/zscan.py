@@ -14,8 +14,8 @@ redrock_b200.templates); outputs are the same numpy arrays with the same
 shapes.  Error conventions follow redrock: all-zero weights give HUGE_CHI2
 rows with zero coefficients; an exactly singular normal matrix gives
 HUGE_CHI2 at that z; an unrecognised solve method gives HUGE_CHI2
-everywhere.  Non-negative / bounded solvers (NMF, NNLS, BVLS) raise
-NotImplementedError instead of silently running on the CPU.
+everywhere.  Non-negative / bounded solvers (NMF, NNLS, BVLS) run on the
+GPU too, through the plain chain's device solvers.
 """
 
 from __future__ import annotations

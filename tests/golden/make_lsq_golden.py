@@ -1,8 +1,8 @@
 """Golden vectors for the bounded solves of redrock's solve_matrices
 (zscan.py:1153-1201), made by running redrock itself: calc_zchi2_batch with
 "NNLS", "BVLS" (active bounds) and "BVLS" (no bounds) for two synthetic
-targets on every 150th GALAXY redshift, and calc_zchi2 with an NMF GALAXY
-template (chi2, coefficients, [OII] penalty).
+targets on every 150th GALAXY redshift, calc_zchi2 with an NMF GALAXY
+template (chi2, coefficients, [OII] penalty), and fitz on that scan.
 
     python tests/golden/make_lsq_golden.py
 """
@@ -61,6 +61,11 @@ def main():
     out["lsq_nmf_zchi2"] = zc
     out["lsq_nmf_zcoeff"] = co
     out["lsq_nmf_penalty"] = pe
+    # fitz on the NMF coarse scan (fitz.py:133-395 with the NNLS solver)
+    for j, t in enumerate(rtg):
+        zf = rr.fitz.fitz(zc[j] + pe[j], zb, t, nmf, nminima=3)
+        for k in ("z", "zerr", "zwarn", "chi2", "coeff", "npixels"):
+            out[f"lsq_nmf_fitz_{j}_{k}"] = np.asarray(zf[k])
     np.savez(os.path.join(HERE, "lsq_golden.npz"), **out)
     print("wrote", len(out), "arrays; NNLS zeros per target:",
           [int((out[f"lsq_nnls_{i}_zcoeff"] == 0).sum()) for i in range(NTARGET)],

@@ -83,3 +83,30 @@ def test_nmf_template_scan_vs_redrock():
         r = res[t.id][tm.full_type]
         _close(r["zchi2"][None], r["zcoeff"][None], g["lsq_nmf_zchi2"][i][None],
                g["lsq_nmf_zcoeff"][i][None])
+
+
+def test_nmf_template_fitz_vs_redrock():
+    """fitz on the NMF template's coarse scan: the fine grids and the fits at
+    the parabola minima through rebin + IGM + the plain chain with NNLS, as
+    redrock's fitz does.  z |dz| <= 1e-7, ZWARN identical, chi2 |d| <= 1e-3,
+    coefficients |dc| <= 1e-5 max|c|."""
+    from redrock_b200 import fitz, targets as T, templates as TM
+    g = np.load(GOLDEN)
+    tg = synth.make_targets(2, seed=11, amp=1.0)
+    gal = synth.template_set()[0]
+    zb = g["lsq_z"]
+    tm = TM.Template(spectype="GALAXY", subtype="NMF", redshifts=zb, wave=gal.wave, flux=gal.flux,
+                     method="NMF", igm_model=gal.igm_model)
+    rt = T.from_synth(tg)
+    chi2 = [g["lsq_nmf_zchi2"][j] + g["lsq_nmf_penalty"][j] for j in range(len(rt))]
+    out = fitz.fitz_targets(chi2, zb, rt, tm, nminima=3)
+    for j, r in enumerate(out):
+        gz = {k: g[f"lsq_nmf_fitz_{j}_{k}"] for k in ("z", "zerr", "zwarn", "chi2", "coeff",
+                                                      "npixels")}
+        np.testing.assert_array_equal(r["zwarn"], gz["zwarn"])
+        np.testing.assert_array_equal(r["npixels"], gz["npixels"])
+        np.testing.assert_allclose(r["z"], gz["z"], rtol=0, atol=1e-7)
+        np.testing.assert_allclose(r["zerr"], gz["zerr"], rtol=1e-5)
+        assert np.max(np.abs(r["chi2"] - gz["chi2"])) <= 1e-3
+        scale = np.maximum(np.abs(gz["coeff"]).max(axis=-1, keepdims=True), 1e-300)
+        assert np.all(np.abs(r["coeff"] - gz["coeff"]) <= 1e-5 * scale)
