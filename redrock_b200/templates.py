@@ -157,8 +157,12 @@ class DistTemplate:
         self.source = TemplateSource.from_template(template)
         self.basis = DeviceBasis.build(self.source, self._layout)
         rank = 0 if comm is None else comm.rank
+        # the lazy host view holds the basis, not self: a closure over self
+        # would make a reference cycle that keeps the device basis (GBs)
+        # alive until the cyclic collector happens to run
+        basis = self.basis
         self._piece = DistTemplatePiece(rank, template.redshifts,
-                                        lambda: self.basis.data_dict(as_numpy=True))
+                                        lambda: basis.data_dict(as_numpy=True))
 
     @property
     def comm(self):

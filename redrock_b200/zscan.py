@@ -181,7 +181,32 @@ def calc_negOII_penalty_sums(oii_sums_dev, coeff_t):
     return out
 
 
+class _NoGC:
+    """Python's cyclic collector paused for the duration of the pipelined
+    scan: a full collection (hundreds of ms with a large heap) in the middle
+    would leave the GPU idle waiting for the next chunk's launches.  The
+    objects made meanwhile are collected afterwards as usual."""
+
+    def __enter__(self):
+        import gc
+        self._was = gc.isenabled()
+        gc.disable()
+
+    def __exit__(self, *exc):
+        import gc
+        if self._was:
+            gc.enable()
+        return False
+
+
 def scan_device(targets, dtemplates, chunk=None, host=False):
+    """Fused scan of every target against every template (see
+    _scan_device), with the cyclic garbage collector paused."""
+    with _NoGC():
+        return _scan_device(targets, dtemplates, chunk=chunk, host=host)
+
+
+def _scan_device(targets, dtemplates, chunk=None, host=False):
     """Fused scan of every target against every template.
 
     Returns a list (one entry per template) of results with zchi2 (T, nz),
