@@ -96,9 +96,11 @@ def _pack(targets, layout):
 # ---------------------------------------------------------------------------
 # fused scan
 # ---------------------------------------------------------------------------
-CHUNK_TARGETS = 128   # targets per pipelined chunk (4 target blocks)
+CHUNK_TARGETS = 224   # targets per pipelined chunk (7 target blocks)
 AUTOTUNE = True       # time the small-basis tile shapes once per workload signature
-FIRST_CHUNK = 32      # a small first chunk gets the GPU started early
+FIRST_CHUNK = 64      # a small first chunk gets the GPU started early
+# (64 / 224 measured best of 32-64 / 128-468 for 500 DESI-like targets:
+# 304.6 ms per end-to-end step against 315.3 ms for 32 / 128)
 
 
 def _bases_for(dtemplates, layout):
