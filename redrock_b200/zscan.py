@@ -183,6 +183,31 @@ def calc_negOII_penalty_sums(oii_sums_dev, coeff_t):
     return out
 
 
+_copy_streams = {}
+
+
+def _pack_overlapped(sub, layout, st, main):
+    """TargetPack of one chunk whose host-to-device copies run on a copy
+    stream, so that they overlap the previous chunk's scan instead of
+    queueing behind it on the main stream; the pack kernel waits for them.
+    The copy stream does not wait for the main stream: its buffers are new
+    allocations, and record_stream keeps them from reuse until the main
+    stream's kernels that read them are done."""
+    d = torch.cuda.current_device()
+    if d not in _copy_streams:
+        _copy_streams[d] = torch.cuda.Stream()
+    cs = _copy_streams[d]
+    batch = TargetBatch(sub, layout)
+    with torch.cuda.stream(cs):
+        dbatch = batch.to_device()
+    for name in ("descs", "segs", "first", "rows", "rdata", "roffs", "ivar", "flux"):
+        getattr(dbatch, name).record_stream(main)
+    ev = torch.cuda.Event()
+    ev.record(cs)
+    main.wait_event(ev)
+    return TargetPack(dbatch, status=st)
+
+
 class _NoGC:
     """Python's cyclic collector paused for the duration of the pipelined
     scan: a full collection (hundreds of ms with a large heap) in the middle
@@ -254,8 +279,7 @@ def _scan_device(targets, dtemplates, chunk=None, host=False):
             pack = _pack(sub, layout)
         else:
             pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
-                                   lambda: TargetPack(TargetBatch(sub, layout).to_device(),
-                                                      status=st))
+                                   lambda: _pack_overlapped(sub, layout, st, main))
         tiles = None
         if AUTOTUNE:
             from . import autotune
