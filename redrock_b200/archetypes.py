@@ -254,6 +254,9 @@ class Archetype:
             arch[:, :, off:off + n] = b.permute(0, 2, 1)
         # Legendre columns, one set per distinct grid order of the targets
         nleg = tlist[0].nleg
+        if any(t.nleg != nleg for t in tlist):
+            raise ValueError("targets with different numbers of Legendre terms in one "
+                             "archetype batch")
         sets, set_of = {}, []
         for t, _, _ in items:
             hs_order = tuple(dict.fromkeys(s.wavehash for s in t.spectra))
