@@ -149,20 +149,32 @@ class DistTemplate:
     """
 
     def __init__(self, template, dwave, mp_procs=1, comm=None, use_gpu=True, gpu_mode=True):
+        from .device import StatusWord
         from .engine import DeviceBasis, GridLayout, TemplateSource
         self._comm = comm
         self._template = template
         self._dwave = dwave
         self._layout = GridLayout.from_dwave(dwave)
         self.source = TemplateSource.from_template(template)
-        self.basis = DeviceBasis.build(self.source, self._layout)
+        # built asynchronously: the device status is checked when the basis
+        # is first read (the scan, or the host view below)
+        status = StatusWord()
+        self._status = status
+        self.basis = DeviceBasis.build(self.source, self._layout, status=status)
         rank = 0 if comm is None else comm.rank
         # the lazy host view holds the basis, not self: a closure over self
         # would make a reference cycle that keeps the device basis (GBs)
         # alive until the cyclic collector happens to run
         basis = self.basis
-        self._piece = DistTemplatePiece(rank, template.redshifts,
-                                        lambda: basis.data_dict(as_numpy=True))
+
+        def host_view():
+            status.check("rr_build_basis")
+            return basis.data_dict(as_numpy=True)
+        self._piece = DistTemplatePiece(rank, template.redshifts, host_view)
+
+    def check(self):
+        """Raise if building the basis on the device reported an error."""
+        self._status.check("rr_build_basis")
 
     @property
     def comm(self):

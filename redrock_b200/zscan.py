@@ -230,7 +230,13 @@ def scan_device(targets, dtemplates, chunk=None, host=False):
     """Fused scan of every target against every template (see
     _scan_device), with the cyclic garbage collector paused."""
     with _NoGC():
-        return _scan_device(targets, dtemplates, chunk=chunk, host=host)
+        out = _scan_device(targets, dtemplates, chunk=chunk, host=host)
+    # bases built asynchronously (DistTemplate) report device errors here
+    for dt in dtemplates:
+        chk = getattr(dt, "check", None)
+        if callable(chk):
+            chk()
+    return out
 
 
 def _scan_device(targets, dtemplates, chunk=None, host=False):
