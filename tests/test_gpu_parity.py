@@ -209,6 +209,30 @@ def test_calc_zchi2_targets_all_templates_one_launch(rr):
             np.testing.assert_allclose(r["penalty"], ope[j], rtol=1e-8, atol=1e-8)
 
 
+def test_empty_and_single_target_inputs(rr):
+    """No targets: calc_zchi2 returns (0, nz) / (0, nz, nbasis) / (0, nz)
+    arrays and calc_zchi2_targets an empty result (zscan.py:846-851, 1008);
+    one target and a one-redshift template run through the same launches."""
+    T, TM = rr["targets"], rr["templates"]
+    tg = synth.make_targets(1, seed=5)
+    dtg = T.DistTargetsCopy(T.from_synth(tg))
+    ts = synth.template_set(zsub=331)[0]
+    dt = TM.DistTemplate(TM.from_synth(ts), dtg.wavegrids())
+    zc, co, pe = rr["zscan"].calc_zchi2([], [], dt)
+    nz, nb = len(ts.redshifts), ts.flux.shape[0]
+    assert zc.shape == (0, nz) and co.shape == (0, nz, nb) and pe.shape == (0, nz)
+    empty = T.DistTargetsCopy([])
+    assert rr["zscan"].calc_zchi2_targets(empty, [dt]) == {}
+    one = TM.from_synth(ts)
+    one._redshifts = np.ascontiguousarray(ts.redshifts[5:6])
+    dt1 = TM.DistTemplate(one, dtg.wavegrids())
+    zc1, co1, _ = rr["zscan"].calc_zchi2([t.id for t in dtg.local()], dtg.local(), dt1)
+    zcf, cof, _ = rr["zscan"].calc_zchi2([t.id for t in dtg.local()], dtg.local(), dt)
+    assert zc1.shape == (1, 1)
+    assert_chi2(zc1[0], zcf[0, 5:6])
+    assert_coeff(co1[0], cof[0, 5:6])
+
+
 def test_util_fixture_two_exposures(rr, golden):
     ut = [synth.util_target(0.2, seed=21, targetid=111),
           synth.util_target(0.25, seed=22, targetid=222)]
