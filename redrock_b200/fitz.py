@@ -187,10 +187,15 @@ class _PlainRefiner:
 
 def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=None,
                  use_gpu=True, deg_legendre=None, zminfit_npoints=15, per_camera=False,
-                 n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=2,
+                 n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=0,
                  refine="parabola"):
     """redrock's fitz for many targets of one template; returns a list of
     per-target result dicts (the same dict-of-arrays fitz returns).
+
+    The first launch evaluates each target's first nminima + batch_extra
+    candidate minima; targets whose candidates fall within max_velo_diff of
+    one another get further launches for the next ones (0 extra measured
+    fastest: most targets need no more than nminima).
 
     refine="parabola" is redrock's minfit through the three fine-grid points
     around the best one.  refine="newton" instead runs safeguarded Newton
