@@ -51,6 +51,14 @@ def prior_on_coeffs(n_nbh, deg_legendre, sigma, ncamera):
     return prior
 
 
+def _vstack(vals):
+    """np.vstack of the values, with a faster path for all-scalar lists
+    (the same (n, 1) array and dtype)."""
+    if all(np.ndim(v) == 0 for v in vals):
+        return np.array(vals).reshape(len(vals), 1)
+    return np.vstack(vals)
+
+
 def get_dv(z, zref):
     """Velocity difference in km/s (fitz.py:28-43)."""
     return C_KMS * (z - zref) / (1.0 + zref)
@@ -362,7 +370,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             r['npixels'] = npix
         tmp = {}
         for k in res[0].keys():
-            tmp[k] = np.vstack([r[k] for r in res])
+            tmp[k] = _vstack([r[k] for r in res])
         out.append(tmp)
     return out
 

@@ -174,3 +174,14 @@ def test_prior_functions():
     t = Priors.tophat(z, 0.0, 0.25)
     assert t[0] == 0 and t[1] == np.inf or t[0] == np.inf
     assert np.isnan(Priors.tophat(z, 5.0, 0.1)).all()
+
+
+def test_fitz_stack_matches_vstack():
+    """fitz's result stacking gives np.vstack's arrays (shape and dtype)."""
+    from redrock_b200.fitz import _vstack
+    cases = [[1.5, np.float64(2.0)], [1, 2, np.int64(3)], ['PCA', 'PCA'], [np.float64(1)],
+             [np.array([1.0, 2.0]), np.array([3.0, 4.0])], [np.zeros((1, 3)), np.ones((1, 3))],
+             ['GALAXY:::ELG_0', 'GALAXY:::BGS_12'], [[np.zeros((3, 2))], [np.ones((3, 2))]]]
+    for c in cases:
+        a, b = _vstack(c), np.vstack(c)
+        assert a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a, b)
