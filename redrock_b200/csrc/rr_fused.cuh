@@ -23,15 +23,25 @@ namespace rr {
 #endif
 
 #ifndef RR_PIX
-#define RR_PIX 3
+#define RR_PIX 4
+#endif
+#ifndef RR_PIX_SMALL
+#define RR_PIX_SMALL RR_PIX
 #endif
 
 constexpr int kQUnroll = RR_Q_UNROLL;
-constexpr int kPix = RR_PIX;  // pixels per step of the pixel loop
+// pixels per step of the pixel loop: RR_PIX for the instantiations whose
+// accumulators fill the register file (NB * ZT > 10), RR_PIX_SMALL for the
+// others
+template <int NB, int ZT>
+constexpr int pix_per_step() {
+  return NB * ZT > 10 ? RR_PIX : RR_PIX_SMALL;
+}
 constexpr int kWarps = RR_SCAN_WARPS;  // redshifts per tile (one per warp)
 constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = RR_CHUNK;
-static_assert(kChunk % kPix == 0, "chunk must hold whole pixel steps");
+static_assert(kChunk % RR_PIX == 0 && kChunk % RR_PIX_SMALL == 0,
+              "chunk must hold whole pixel steps");
 constexpr int kWin = kChunk + 2 * kHalfBand;  // basis rows per chunk window
 constexpr int kStages = RR_SCAN_STAGES;      // copy pipeline depth
 constexpr int kRwChunkDoubles = kChunk * RR_RW * RR_LANES;
@@ -192,6 +202,7 @@ __device__ __forceinline__ bool sweep(const FusedParams& p, const rr_scan_templa
     } else if (any && ok) {
       const double* rws = sb.rw(s) + lane;
       const double* ts = sb.t(s) + warp * ZT * kWin * stride;
+      constexpr int kPix = pix_per_step<NB, ZT>();
       // kPix pixels per step: basis row q + k serves pixel q + i with band
       // index k - i, so each row is read once for all kPix pixels (and the
       // packed rows once for all ZT redshifts)

@@ -54,9 +54,21 @@ def prior_on_coeffs(n_nbh, deg_legendre, sigma, ncamera):
 def _vstack(vals):
     """np.vstack of the values, with a faster path for all-scalar lists
     (the same (n, 1) array and dtype)."""
-    if all(np.ndim(v) == 0 for v in vals):
+    if all(isinstance(v, _SCALARS) for v in vals):
         return np.array(vals).reshape(len(vals), 1)
     return np.vstack(vals)
+
+
+_SCALARS = (float, int, str, np.floating, np.integer, np.str_)
+
+
+def _near_any(z, zprev, maxv):
+    """np.any(np.abs(get_dv(z, np.array(zprev))) < maxv), elementwise in
+    the same operation order, without building arrays."""
+    for zr in zprev:
+        if abs(C_KMS * (z - zr) / (1.0 + zr)) < maxv:
+            return True
+    return False
 
 
 def get_dv(z, zref):
@@ -95,6 +107,52 @@ def minfit(x, y):
         xerr = 1 / np.sqrt(-a)
         zwarn |= BAD_MINFIT
     return (x0, xerr, y0, zwarn)
+
+
+def minfit_batch(x, y):
+    """minfit for K triples at once: x, y (K, 3) -> x0, xerr, y0 (K,) and
+    zwarn (K,) int.
+
+    The parabola through three points is the Newton form
+    y0 + d1 (x - x0) + a (x - x0)(x - x1), a = the second divided
+    difference; its vertex differs from np.polyfit's least-squares fit by
+    rounding only (~1e-10 in z on redrock's fine grids, below the ~1e-9 the
+    FP64 chi2 noise itself moves it).  Triples where that form is not well
+    determined -- non-finite values, repeated x, or a second difference
+    within 1e-9 of the values' scale (flat or constant chi2, e.g.
+    HUGE_CHI2) -- go through minfit, so degenerate cases return exactly
+    what redrock's polyfit returns."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    k = len(x)
+    x0 = np.empty(k)
+    xerr = np.empty(k)
+    y0 = np.empty(k)
+    zwarn = np.zeros(k, dtype=np.int64)
+    if k == 0:
+        return x0, xerr, y0, zwarn
+    with np.errstate(all='ignore'):
+        h0 = x[:, 1] - x[:, 0]
+        h1 = x[:, 2] - x[:, 1]
+        d1 = (y[:, 1] - y[:, 0]) / h0
+        d2 = (y[:, 2] - y[:, 1]) / h1
+        a = (d2 - d1) / (x[:, 2] - x[:, 0])
+        dd = y[:, 0] - 2.0 * y[:, 1] + y[:, 2]
+        scale = np.max(np.abs(y), axis=1)
+        good = (np.all(np.isfinite(x), axis=1) & np.all(np.isfinite(y), axis=1)
+                & (h0 > 0) & (h1 > 0) & (np.abs(dd) > 1e-9 * scale) & (a != 0.0))
+        xv = 0.5 * (x[:, 0] + x[:, 1]) - d1 / (2.0 * a)
+        yv = y[:, 0] + d1 * (xv - x[:, 0]) + a * (xv - x[:, 0]) * (xv - x[:, 1])
+        sig = 1.0 / np.sqrt(np.abs(a))
+    x0[:] = xv
+    y0[:] = yv
+    xerr[:] = sig
+    zwarn[(xv <= np.min(x, axis=1)) | (np.max(x, axis=1) <= xv)] |= BAD_MINFIT
+    zwarn[yv <= 0.0] |= BAD_MINFIT
+    zwarn[~(a > 0.0)] |= BAD_MINFIT
+    for i in np.nonzero(~good)[0]:
+        x0[i], xerr[i], y0[i], zwarn[i] = minfit(x[i], y[i])
+    return x0, xerr, y0, zwarn
 
 
 class _NewtonCtx:
@@ -233,29 +291,41 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     want = nminima + batch_extra
 
     def fetch(tlist, count):
-        tid, zs, key = [], [], []
+        tid, key = [], []
         for j in tlist:
             c = cands[j]
             for imin in c[pos[j]:pos[j] + count]:
-                ilo = max(0, imin - 1)
-                ihi = min(imin + 1, len(redshifts) - 1)
-                zz = np.linspace(redshifts[ilo], redshifts[ihi], nz)
                 tid += [j] * nz
-                zs.append(zz)
-                key.append((j, imin, zz))
+                key.append((j, int(imin)))
             pos[j] = min(len(c), pos[j] + count)
         if not key:
             return
-        chi2, _, pen, ok = ref.scan(tid, np.concatenate(zs))
+        imins = np.array([k[1] for k in key])
+        lo = redshifts[np.maximum(0, imins - 1)]
+        hi = redshifts[np.minimum(imins + 1, len(redshifts) - 1)]
+        if nz > 1 and np.all(hi != lo):
+            # np.linspace over all candidates at once: the same
+            # start + i * ((stop - start) / (nz - 1)) per row, last = stop
+            zzall = np.linspace(lo, hi, nz, axis=1)
+        else:
+            zzall = np.stack([np.linspace(a, b, nz) for a, b in zip(lo, hi)])
+        chi2, _, pen, ok = ref.scan(tid, zzall.reshape(-1))
         if not np.all(ok):
             raise ValueError('edges must be within input x range')
-        off = 0
-        for j, imin, zz in key:
-            zzchi2 = chi2[off:off + nz].copy()
-            if has_oii:
-                zzchi2 += pen[off:off + nz]
-            fine[j][imin] = (zz, zzchi2)
-            off += nz
+        c2all = chi2.reshape(len(key), nz).copy()
+        if has_oii:
+            c2all += pen.reshape(len(key), nz)
+        fits = [None] * len(key)
+        if refine != "newton" and nz >= 3:
+            # the parabola of every candidate in one pass (the replay below
+            # only picks the ones it reaches)
+            ib = np.clip(np.argmin(c2all, axis=1), 1, nz - 2)
+            cols = ib[:, None] + np.arange(-1, 2)[None, :]
+            rows = np.arange(len(key))[:, None]
+            fx0, ferr, fy0, fzw = minfit_batch(zzall[rows, cols], c2all[rows, cols])
+            fits = list(zip(fx0.tolist(), ferr.tolist(), fy0.tolist(), fzw.tolist()))
+        for n_, (j, imin) in enumerate(key):
+            fine[j][imin] = (zzall[n_], c2all[n_], fits[n_])
 
     newton_ctx = {}
 
@@ -295,14 +365,15 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                 if imin not in fine[j]:
                     break        # not fetched yet
                 st['ci'] += 1
-                zprev = np.array([tmp['z'] for tmp in results[j]])
-                dv = get_dv(z=redshifts[imin], zref=zprev)
-                if np.any(np.abs(dv) < maxv):
+                zprev = [tmp['z'] for tmp in results[j]]
+                if _near_any(redshifts[imin], zprev, maxv):
                     continue
-                zz, zzchi2 = fine[j][imin]
+                zz, zzchi2, fit = fine[j][imin]
                 i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
                 if refine == "newton":
                     zmin, sigma, chi2min, zwarn = newton_min(j, zz[i - 1:i + 2], zzchi2[i])
+                elif fit is not None:
+                    zmin, sigma, chi2min, zwarn = fit
                 else:
                     zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])
                 zbest = zmin
@@ -316,9 +387,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                     zwarn |= Z_FITLIMIT
                 if zmin < redshifts[1] or zmin > redshifts[-2]:
                     zwarn |= Z_FITLIMIT
-                zprev = np.array([tmp['z'] for tmp in results[j]])
-                dv = get_dv(z=zbest, zref=zprev)
-                if np.any(np.abs(dv) < maxv):
+                if _near_any(zbest, zprev, maxv):
                     continue
                 r = dict(z=zbest, zerr=zerr, zwarn=zwarn, chi2=chi2min, zz=zz, zzchi2=zzchi2,
                          coeff=None, fitmethod=template.method)

@@ -56,6 +56,9 @@ def calc_deltachi2(chi2, z, zwarn, dvlimit=MAX_VELO_DIFF):
     okfit = (zwarn & BADFIT_MASK) == 0
     if np.isscalar(dvlimit):
         dvlimit = np.full(nz, dvlimit)
+    if all(np.asarray(v).dtype == np.float64 and np.all(np.isfinite(v))
+           for v in (chi2, z, dvlimit)):
+        return _deltachi2_f64(chi2, z, okfit, dvlimit)
     for i in range(len(chi2) - 1):
         dv = _fitz.get_dv(z[i + 1:], z[i])
         ii = (np.abs(dv) > np.minimum(dvlimit[i], dvlimit[i + 1:])) & okfit[i + 1:]
@@ -72,6 +75,32 @@ def calc_deltachi2(chi2, z, zwarn, dvlimit=MAX_VELO_DIFF):
         alldvlimit = np.minimum(dvlimit[i], dvlimit[noti])
         if np.any(okfit[noti] & (alldeltachi2 < MIN_DELTACHI2) & (alldv >= alldvlimit)):
             setzwarn[i] = True
+    return deltachi2, setzwarn
+
+
+def _deltachi2_f64(chi2, z, okfit, dvlimit):
+    """calc_deltachi2 on float64 inputs with Python floats: the same IEEE
+    operations in the same order per pair (a target has a handful of
+    fits, where numpy's per-call cost dominates)."""
+    c, zz, ok, dl = chi2.tolist(), z.tolist(), okfit.tolist(), dvlimit.tolist()
+    nz = len(c)
+    deltachi2 = np.zeros(nz)
+    for i in range(nz - 1):
+        best = None
+        for j in range(i + 1, nz):
+            if ok[j] and abs(_fitz.C_KMS * (zz[j] - zz[i]) / (1.0 + zz[i])) > min(dl[i], dl[j]):
+                d = c[j] - c[i]
+                if best is None or d < best:
+                    best = d
+        if best is not None:
+            deltachi2[i] = best
+    setzwarn = np.zeros(nz, dtype=bool)
+    for i in range(nz):
+        for j in range(nz):
+            if j != i and ok[j] and abs(c[j] - c[i]) < MIN_DELTACHI2 and \
+                    abs(_fitz.C_KMS * (zz[j] - zz[i]) / (1.0 + zz[i])) >= min(dl[i], dl[j]):
+                setzwarn[i] = True
+                break
     return deltachi2, setzwarn
 
 

@@ -145,6 +145,34 @@ def test_calc_deltachi2_known_answers():
     assert np.all(dchi2 == np.array([3, 2, 0.0, 0.0]))
 
 
+def test_deltachi2_fast_path_matches_numpy_loop():
+    """calc_deltachi2's float64 path (Python floats) gives the numpy loop's
+    bits on random fit sets with close pairs, bad fits and both limits."""
+    from redrock_b200 import zfind as Z
+    rng = np.random.default_rng(3)
+    for it in range(500):
+        n = int(rng.integers(1, 12))
+        chi2 = rng.uniform(0, 30, n)
+        z = rng.uniform(0, 3, n) if it % 2 else np.round(rng.uniform(0, 0.01, n), 4)
+        zw = rng.choice([0, 0, 0, 4, 1024, 32], n)
+        dl = rng.choice([100.0, 1000.0], n)
+        ok = (zw & Z.BADFIT_MASK) == 0
+        d2 = np.zeros(n)
+        for i in range(n - 1):
+            dv = Z._fitz.get_dv(z[i + 1:], z[i])
+            ii = (np.abs(dv) > np.minimum(dl[i], dl[i + 1:])) & ok[i + 1:]
+            if np.any(ii):
+                d2[i] = np.min((chi2[i + 1:] - chi2[i])[ii])
+        sz = np.zeros(n, dtype=bool)
+        for i in range(n):
+            m = np.arange(n) != i
+            sz[i] = np.any(ok[m] & (np.abs(chi2[m] - chi2[i]) < Z.MIN_DELTACHI2)
+                           & (np.abs(Z._fitz.get_dv(z[m], z[i])) >= np.minimum(dl[i], dl[m])))
+        got = Z.calc_deltachi2(chi2, z, zw, dvlimit=dl)
+        np.testing.assert_array_equal(got[0], d2)
+        np.testing.assert_array_equal(got[1], sz)
+
+
 def test_find_minima_and_minfit():
     from redrock_b200.fitz import find_minima, minfit
     assert list(find_minima([1, 1, 1, 2, 2, 2])) == [0, 1, 2, 4, 5]
@@ -154,6 +182,50 @@ def test_find_minima_and_minfit():
     assert abs(x0 - 0.21) < 1e-12 and abs(xerr - 0.05) < 1e-12 and abs(y0 - 2.0) < 1e-9
     assert zw == 0
     assert minfit(x[:2], x[:2])[3] == 2 ** 10
+
+
+def test_minfit_batch_matches_minfit():
+    """The batched parabola agrees with redrock's polyfit-based minfit on
+    fine-grid triples (vertex within 1e-9 in z, same ZWARN bits; chi2 at the
+    vertex within polyfit's own cancellation error), and
+    degenerate triples (flat, constant HUGE_CHI2, NaN, repeated x) give
+    exactly minfit's answer."""
+    from redrock_b200.fitz import minfit, minfit_batch
+    rng = np.random.default_rng(11)
+    xs, ys = [], []
+    for it in range(400):
+        # fine-grid spacings of the z grids: 2 coarse steps over 14 intervals
+        # (STAR: linspace(-0.002, 0.002, 100); GALAXY / QSO: 3e-4 / 5e-4 in ln(1 + z))
+        if it % 5 == 0:
+            z1 = rng.uniform(-0.002, 0.002)
+            h = 2 * 0.004 / 99 / 14
+        else:
+            z1 = rng.uniform(0.0, 6.0)
+            h = 2 * (1 + z1) * rng.uniform(3e-4, 5e-4) / 14
+        x = np.array([z1 - h, z1, z1 + h])
+        a = rng.uniform(1e5, 1e11) * rng.choice([1, 1, 1, -1])
+        zt = z1 + rng.uniform(-1.5, 1.5) * h
+        xs.append(x)
+        ys.append(rng.uniform(-50, 2e4) + a * (x - zt) ** 2)
+    x = np.array([0.5, 0.5 + 4e-5, 0.5 + 8e-5])
+    deg = [(x, np.full(3, 9999999.0)), (x, np.array([5.0, 5.0, 5.0])),
+           (x, np.array([1.0, np.nan, 2.0])), (np.array([0.5, 0.5, 0.6]), np.array([3.0, 2.0, 4.0])),
+           (x, 1.0 + 1e3 * (x - x[0]))]
+    for xx, yy in deg:
+        xs.append(xx)
+        ys.append(yy)
+    x0, xerr, y0, zw = minfit_batch(np.array(xs), np.array(ys))
+    for i, (xx, yy) in enumerate(zip(xs, ys)):
+        r = minfit(xx, yy)
+        if i >= 400:
+            np.testing.assert_array_equal([x0[i], xerr[i], y0[i], zw[i]], r, err_msg=str(i))
+            continue
+        assert zw[i] == r[3], i
+        assert abs(x0[i] - r[0]) <= 1e-9 * max(1.0, abs(r[0])), i
+        assert abs(xerr[i] - r[1]) <= 1e-5 * r[1], i
+        # polyfit's y0 = c - b^2/4a cancels terms of size a x0^2
+        assert abs(y0[i] - r[2]) <= 1e-14 * x0[i] ** 2 / xerr[i] ** 2 + 1e-9 * abs(r[2]), i
+    assert all(len(v) == 0 for v in minfit_batch(np.zeros((0, 3)), np.zeros((0, 3))))
 
 
 def test_prior_functions():
