@@ -218,12 +218,15 @@ typedef struct {
   int64_t npix_block;
 } rr_scan_targets;
 
-/* tile_counter: four device ints of scratch (reset by the call); on
- * return tile_counter[2] counts the tiles that were swept a second time to
- * sum chi2 as the direct residual (ill-conditioned fits) and
- * tile_counter[3] the (target, z) pairs re-evaluated that way.  Templates with
- * nbasis 4, 5 or 10 run in one persistent launch, any others in a second
- * one. */
+/* tile_counter: RR_FUSED_COUNTERS device ints of scratch (reset by the
+ * call); on return tile_counter[2] counts the tiles that were swept a second
+ * time to sum chi2 as the direct residual (ill-conditioned fits) and
+ * tile_counter[3] the (target, z) pairs re-evaluated that way.  Each nbasis
+ * group (10, 4, 5, any other) runs as one persistent launch with its own
+ * instantiation; the launches follow one another in the stream, each after
+ * the first as a programmatic dependent launch, so it starts on the SMs the
+ * previous one's last tiles leave idle. */
+#define RR_FUSED_COUNTERS 12
 int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                    int ntemplate, int* tile_counter, int* status, rr_stream_t stream);
 

@@ -25,6 +25,7 @@ RW = 12
 CHUNK = 24   # default; chunk() returns the loaded library's value
 MAX_TEMPLATES = 16
 MAX_NBASIS = 10
+FUSED_COUNTERS = 12   # RR_FUSED_COUNTERS: tile_counter ints of rr_zscan_fused
 
 IGM_CODES = {None: RR_IGM_NONE, "None": RR_IGM_NONE, "Calura12": RR_IGM_CALURA12,
              "Kamble20": RR_IGM_KAMBLE20, "Inoue14": RR_IGM_INOUE14}

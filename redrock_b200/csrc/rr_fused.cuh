@@ -374,6 +374,9 @@ __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_k
     fence_mbar_init();
   }
   __syncthreads();
+  // the next group's launch (programmatic dependent launch) may start now:
+  // its CTAs take the SMs this grid's CTAs leave in its last tile wave
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   Uses uses;
   bool failed = false;
   const int64_t ntiles = p.tile_start[p.ntemplate];
@@ -407,6 +410,10 @@ __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_k
     if (failed) break;  // uniform across the CTA
     __syncthreads();
   }
+  // a grid launched as a dependent completes only after the grid before it
+  // (no-op otherwise), so stream order still holds for whatever follows the
+  // last launch
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 inline size_t fused_smem_bytes(int max_stride, int zt) {
@@ -415,11 +422,14 @@ inline size_t fused_smem_bytes(int max_stride, int zt) {
 }
 
 // Launch one instantiation of the fused kernel over the templates selected
-// by `pick` (indices into templates), using counter as its tile counter.
+// by `pick` (indices into templates), using counter (zeroed by the caller) as
+// its tile counter.  overlap: launch as a programmatic dependent of the
+// previous kernel in the stream (the previous fused launch, whose tiles are
+// independent of these).
 template <int GROUP, bool EXTY, int ZT>
 int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
                         const int* pick, int npick, int* counter, int* resweep, int* status,
-                        cudaStream_t stream) {
+                        bool overlap, cudaStream_t stream) {
   constexpr int kZt = ZT;
   FusedParams p;
   memset(&p, 0, sizeof(p));
@@ -453,14 +463,24 @@ int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templat
   int dev = 0, nsm = 0;
   RR_CUDA_TRY(cudaGetDevice(&dev));
   RR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  RR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), stream));
   int per_sm = 1;
   RR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, zscan_fused_kernel<GROUP, EXTY, ZT>,
                                                             kThreads, smem));
   if (per_sm < 1) per_sm = 1;
   const int64_t slots = (int64_t)nsm * per_sm;
   const int64_t grid = ntiles < slots ? ntiles : slots;
-  zscan_fused_kernel<GROUP, EXTY, ZT><<<(unsigned)grid, kThreads, smem, stream>>>(p);
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = overlap ? 1 : 0;
+  RR_CUDA_TRY(cudaLaunchKernelEx(&cfg, zscan_fused_kernel<GROUP, EXTY, ZT>, p));
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
@@ -469,20 +489,21 @@ int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templat
 template <int GROUP, bool EXTY>
 int launch_group(int zt, const rr_scan_targets* targets, const rr_scan_template* templates,
                         const int* pick, int npick, int* counter, int* resweep, int* status,
-                        cudaStream_t stream) {
+                        bool overlap, cudaStream_t stream) {
   if (zt < 1 || zt > kMaxZt[GROUP]) return RR_EINVAL;
   if constexpr (kMaxZt[GROUP] >= 3)
-    if (zt == 3) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 3 ? 3 : 1)>(targets, templates, pick, npick, counter, resweep, status, stream);
+    if (zt == 3) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 3 ? 3 : 1)>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
   if constexpr (kMaxZt[GROUP] >= 2)
-    if (zt == 2) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 2 ? 2 : 1)>(targets, templates, pick, npick, counter, resweep, status, stream);
-  return launch_fused<GROUP, EXTY, 1>(targets, templates, pick, npick, counter, resweep, status, stream);
+    if (zt == 2) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 2 ? 2 : 1)>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
+  return launch_fused<GROUP, EXTY, 1>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
 }
 
 // one entry per group translation unit
 #define RR_FUSED_GROUP_DECL(G)                                                                   \
   int fused_group_##G(bool exty, int zt, const rr_scan_targets* targets,                         \
                       const rr_scan_template* templates, const int* pick, int npick,             \
-                      int* counter, int* resweep, int* status, cudaStream_t stream);
+                      int* counter, int* resweep, int* status, bool overlap,            \
+                      cudaStream_t stream);
 RR_FUSED_GROUP_DECL(0)
 RR_FUSED_GROUP_DECL(1)
 RR_FUSED_GROUP_DECL(2)

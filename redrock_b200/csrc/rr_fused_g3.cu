@@ -5,11 +5,11 @@ namespace rr {
 
 int fused_group_3(bool exty, int zt, const rr_scan_targets* targets,
                    const rr_scan_template* templates, const int* pick, int npick, int* counter,
-                   int* resweep, int* status, cudaStream_t stream) {
+                   int* resweep, int* status, bool overlap, cudaStream_t stream) {
   return exty ? launch_group<3, true>(zt, targets, templates, pick, npick, counter, resweep,
-                                        status, stream)
+                                        status, overlap, stream)
               : launch_group<3, false>(zt, targets, templates, pick, npick, counter, resweep,
-                                         status, stream);
+                                         status, overlap, stream);
 }
 
 }  // namespace rr

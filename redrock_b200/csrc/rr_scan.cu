@@ -407,19 +407,24 @@ static int zscan_fused(const rr_scan_targets* targets, const rr_scan_template* t
     group[gi][ng[gi]++] = t;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  RR_CUDA_TRY(cudaMemsetAsync(tile_counter + 2, 0, 2 * sizeof(int), st));
-  // each launch resets its counter first (stream order), so the launches
-  // share tile_counter[0]
+  // one zeroing of every counter before the first launch, so the launches
+  // follow one another directly in the stream and each one after the first
+  // can start on the SMs its predecessor's last tile wave leaves idle
+  // (tile_counter[4 + g] hands out the tiles of launch g)
+  RR_CUDA_TRY(cudaMemsetAsync(tile_counter, 0, RR_FUSED_COUNTERS * sizeof(int), st));
   int* resweep = tile_counter + 2;
   int rc = RR_OK;
-  if (!rc && ng[0]) rc = fused_group_0(false, zt[0], targets, templates, group[0], ng[0], tile_counter, resweep, status, st);
-  if (!rc && ng[1]) rc = fused_group_1(false, zt[1], targets, templates, group[1], ng[1], tile_counter, resweep, status, st);
-  if (!rc && ng[2]) rc = fused_group_2(false, zt[2], targets, templates, group[2], ng[2], tile_counter, resweep, status, st);
-  if (!rc && ng[3]) rc = fused_group_3(false, zt[3], targets, templates, group[3], ng[3], tile_counter, resweep, status, st);
-  if (!rc && ng[4]) rc = fused_group_0(true, zt[0], targets, templates, group[4], ng[4], tile_counter, resweep, status, st);
-  if (!rc && ng[5]) rc = fused_group_1(true, zt[1], targets, templates, group[5], ng[5], tile_counter, resweep, status, st);
-  if (!rc && ng[6]) rc = fused_group_2(true, zt[2], targets, templates, group[6], ng[6], tile_counter, resweep, status, st);
-  if (!rc && ng[7]) rc = fused_group_3(true, zt[3], targets, templates, group[7], ng[7], tile_counter, resweep, status, st);
+  bool overlap = false;
+  typedef int (*group_fn)(bool, int, const rr_scan_targets*, const rr_scan_template*, const int*,
+                          int, int*, int*, int*, bool, cudaStream_t);
+  const group_fn fns[kNGroups] = {fused_group_0, fused_group_1, fused_group_2, fused_group_3};
+  for (int gi = 0; gi < 2 * kNGroups && !rc; ++gi) {
+    if (!ng[gi]) continue;
+    const int g = gi % kNGroups;
+    rc = fns[g](gi >= kNGroups, zt[g], targets, templates, group[gi], ng[gi], tile_counter + 4 + gi,
+                resweep, status, overlap, st);
+    overlap = true;
+  }
   return rc;
 }
 

@@ -518,7 +518,7 @@ def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=N
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
     tgs = pack.scan_targets_struct()
-    counter = torch.zeros(4, dtype=torch.int32, device=dev)
+    counter = torch.zeros(_lib.FUSED_COUNTERS, dtype=torch.int32, device=dev)
     st = status or StatusWord(dev)
     ygemm = resolve_y(ygemm, pack.layout)
     yg = None if ygemm == "fp64" else YGemm(pack, ygemm, stream=stream, status=st)

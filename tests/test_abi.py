@@ -48,3 +48,10 @@ def test_argument_errors_without_gpu():
     assert L.rr_igm_transmission(7, None, 1, None, 1, None, None) == _lib.RR_EINVAL
     assert L.rr_zscan_fused(None, None, 0, None, None, None) == _lib.RR_EINVAL
     assert L.rr_zchi2_batch_plain_workspace_bytes(100, 10, 4) > 100 * 10 * 4 * 8
+
+
+def test_header_constants_match_binding():
+    src = open(os.path.join(ROOT, "include", "redrock_b200.h")).read()
+    consts = dict(re.findall(r"#define\s+(RR_[A-Z0-9_]+)\s+(\d+)\b", src))
+    assert int(consts["RR_FUSED_COUNTERS"]) == _lib.FUSED_COUNTERS
+    assert int(consts["RR_CHUNK"]) == _lib.CHUNK
