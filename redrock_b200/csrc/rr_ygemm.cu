@@ -386,7 +386,10 @@ constexpr int kKt = 32;                    // pixels per stage = one MMA K step
 constexpr int kNkg = kKt / 16;             // 2 core matrices along K
 constexpr int kSbo = kNkg * 128;           // 256 B between 8-row groups
 constexpr int kN = 64;                     // MMA N: 7 accumulators x 64 columns <= 512
-constexpr int kStages = 4;
+#ifndef RR_I8_STAGES
+#define RR_I8_STAGES 4
+#endif
+constexpr int kStages = RR_I8_STAGES;  // copy pipeline depth (43 KB per stage)
 constexpr int kASlice = kTileM * kKt;      // bytes of one digit plane of a G block
 constexpr int kBSlice = kN * kKt;
 constexpr int kABlock = kDigits * kASlice;  // 28672 B per (target tile, chunk)
