@@ -299,8 +299,7 @@ def run_ours(args, rank, world, local_rank):
     e2e = None
     if not args.no_e2e:
         def e2e_step():
-            zscan._pack_cache.clear()
-            zscan._basis_cache.clear()
+            zscan.clear_caches()
             dtg = T.DistTargetsCopy(rtg)
             dwave = dtg.wavegrids()
             dts = [TM.DistTemplate(tm, dwave) for tm in tms]

@@ -325,6 +325,8 @@ int rr_pack_band_rows(const rr_spectrum_desc* specs /* device */, int64_t nspec,
                       const double* rdata, const int32_t* roffsets, int64_t npix_total,
                       double* band, int* status, rr_stream_t stream);
 
+/* Workspace bytes of one call; SIZE_MAX when the count overflows (every
+ * size check against it then fails with RR_EINVAL / RR_ESCRATCH). */
 size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz, int32_t nbasis);
 
 /* rr_zchi2_batch_plain with the bounds of RR_SOLVE_BVLS: a host array
@@ -332,7 +334,10 @@ size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz, int3
  * (-inf, inf) -- redrock's solver_args['bounds'].  For RR_SOLVE_NNLS and
  * RR_SOLVE_BVLS chi2 is the direct residual sum w (f - Tb c)^2 (as for
  * every method of this path); a failed bounded solve (singular free set,
- * iteration limit) gives HUGE_CHI2 like redrock's caught exception. */
+ * iteration limit) gives HUGE_CHI2 like redrock's caught exception.
+ * status (optional): RR_EINVAL when a pix_basis entry puts its 11-row band
+ * outside the basis rows [0, pix_stride) (those pixels read nothing and
+ * count as zero model); check it before trusting the outputs. */
 int rr_zchi2_batch_plain_ex(const double* band, const double* w, const double* wflux,
                             const double* flux, const int64_t* pix_basis, int64_t npix_total,
                             const double* basis, int64_t pix_stride, int32_t nz, int32_t nbasis,
@@ -358,8 +363,9 @@ int rr_zchi2_batch_plain(const double* band, const double* w, const double* wflu
  * rr_zchi2_batch_plain_workspace_bytes(npix_total, nz, nbasis) >
  * RR_NOALLOC_SCRATCH_BYTES return RR_ESCRATCH.  All calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.
- * The first call on a device looks up the array's address; make it before
- * any stream capture.
+ * The first call on a device looks up the array's address and caches it;
+ * make it before any stream capture, and do not use this entry point again
+ * after cudaDeviceReset on that device (the cached address is stale).
  * ---------------------------------------------------------------------- */
 #define RR_NOALLOC_SCRATCH_BYTES (16u << 20)
 

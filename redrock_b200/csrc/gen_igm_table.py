@@ -11,6 +11,7 @@ same doubles.
 Usage (needs the reference checkout):
     python gen_igm_table.py /path/to/redrock/py/redrock/data > rr_igm_table.h
 """
+import os
 import sys
 import numpy as np
 
@@ -45,4 +46,8 @@ def main(datadir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/py/redrock/data")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REDROCK_DATA")
+    if not src:
+        sys.exit("usage: gen_igm_table.py <redrock data directory holding LAFcoeff.txt and "
+                 "DLAcoeff.txt> (or set REDROCK_DATA)")
+    main(src)

@@ -31,7 +31,9 @@
 // solves the n x n system in registers (LDL^T, no pivoting; an exactly zero
 // pivot is redrock's singular case) and writes chi2, coefficients and the
 // penalty.
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -158,7 +160,7 @@ __global__ void pack_band_rows_kernel(const rr_spectrum_desc* __restrict__ specs
 // Tb[z][p][b] = sum_k band[p][k] basis[z][pix_basis[p] + k - 5][b]
 __global__ void plain_rt_kernel(const double* __restrict__ band, const int64_t* __restrict__ pix_basis,
                                 int64_t npix, const double* __restrict__ basis, int64_t pix_stride,
-                                int nz, int nb, int stride, double* __restrict__ tb) {
+                                int nz, int nb, int stride, double* __restrict__ tb, int* status) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t total = (int64_t)nz * npix * nb;
   if (i >= total) return;
@@ -166,7 +168,14 @@ __global__ void plain_rt_kernel(const double* __restrict__ band, const int64_t* 
   const int64_t pz = i / nb;
   const int64_t p = pz % npix;
   const int64_t z = pz / npix;
-  const double* t = basis + (z * pix_stride + pix_basis[p] - kHalfBand) * stride + b;
+  const int64_t pb = pix_basis[p];
+  // the 11 basis rows of the band must lie inside this redshift's rows
+  if (pb < kHalfBand || pb + kHalfBand >= pix_stride) {
+    set_status(status, RR_EINVAL);
+    tb[i] = 0.0;
+    return;
+  }
+  const double* t = basis + (z * pix_stride + pb - kHalfBand) * stride + b;
   const double* r = band + p * kBand;
   double acc = 0.0;
 #pragma unroll
@@ -482,11 +491,17 @@ extern "C" int rr_pack_band_rows(const rr_spectrum_desc* specs, int64_t nspec, c
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// SIZE_MAX for sizes whose byte count does not fit (or negative sizes), so
+// that every size check against it fails
 extern "C" size_t rr_zchi2_batch_plain_workspace_bytes(int64_t npix_total, int32_t nz,
                                                        int32_t nbasis) {
+  if (npix_total < 0 || nz < 0 || nbasis < 0) return SIZE_MAX;
   const size_t tri = (size_t)nbasis * (nbasis + 1) / 2;
-  return align256((size_t)nz * npix_total * nbasis * sizeof(double)) +
-         align256((size_t)nz * tri * sizeof(double)) +
+  size_t tb = 0;
+  if (__builtin_mul_overflow((size_t)nz, (size_t)npix_total, &tb) ||
+      __builtin_mul_overflow(tb, (size_t)nbasis * sizeof(double), &tb) || tb > SIZE_MAX / 2)
+    return SIZE_MAX;
+  return align256(tb) + align256((size_t)nz * tri * sizeof(double)) +
          align256((size_t)nz * nbasis * sizeof(double)) + align256((size_t)nz);
 }
 
@@ -495,7 +510,8 @@ static int plain_launch(const double* band, const double* w, const double* wflux
                         const double* flux, const int64_t* pix_basis, int64_t npix,
                         const double* basis, int64_t pix_stride, int nz, int stride,
                         const double* prior, int method, const SolveBounds& bounds,
-                        double* zchi2, double* zcoeff, unsigned char* ws, cudaStream_t st) {
+                        double* zchi2, double* zcoeff, unsigned char* ws, int* status,
+                        cudaStream_t st) {
   constexpr int kTri = NB * (NB + 1) / 2;
   double* tb = reinterpret_cast<double*>(ws);
   double* mtri = reinterpret_cast<double*>(ws + align256((size_t)nz * npix * NB * sizeof(double)));
@@ -504,8 +520,10 @@ static int plain_launch(const double* band, const double* w, const double* wflux
   unsigned char* bad =
       reinterpret_cast<unsigned char*>(yv) + align256((size_t)nz * NB * sizeof(double));
   const int64_t total = (int64_t)nz * npix * NB;
+  if ((total + 255) / 256 > (int64_t)INT32_MAX) return RR_EINVAL;
   plain_rt_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(band, pix_basis, npix, basis,
-                                                                    pix_stride, nz, NB, stride, tb);
+                                                                    pix_stride, nz, NB, stride, tb,
+                                                                    status);
   RR_CHECK_LAUNCH();
   plain_gram_kernel<NB><<<nz, 128, 0, st>>>(tb, w, wflux, npix, mtri, yv);
   RR_CHECK_LAUNCH();
@@ -528,7 +546,6 @@ static int plain_entry(const double* band, const double* w, const double* wflux,
                                     const double* prior, int32_t method, double* zchi2,
                                     double* zcoeff, void* workspace, size_t workspace_bytes,
                                     int* status, rr_stream_t stream, const double* bounds) {
-  (void)status;
   SolveBounds sb;
   for (int i = 0; i < RR_MAX_NBASIS; ++i) {
     sb.lo[i] = -INFINITY;
@@ -552,7 +569,7 @@ static int plain_entry(const double* band, const double* w, const double* wflux,
 #define RR_PLAIN_CASE(N)                                                                          \
   case N:                                                                                         \
     return plain_launch<N>(band, w, wflux, flux, pix_basis, npix_total, basis, pix_stride, nz,    \
-                           basis_stride, prior, method, sb, zchi2, zcoeff, ws, st);
+                           basis_stride, prior, method, sb, zchi2, zcoeff, ws, status, st);
   switch (nbasis) {
     RR_PLAIN_CASE(1)
     RR_PLAIN_CASE(2)
@@ -613,7 +630,10 @@ extern "C" int rr_zchi2_batch_plain_ex(const double* band, const double* w, cons
 //   caller.
 // * The first call on each device looks up the array's device address
 //   (cudaGetSymbolAddress) with that device current and caches it; make
-//   that first call before any stream capture.
+//   that first call before any stream capture.  The cached address belongs
+//   to that device's context: after cudaDeviceReset (or any teardown of
+//   the primary context) it is stale, so do not call this entry point in a
+//   process that resets a device it has already used it on.
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char rr_noalloc_scratch[RR_NOALLOC_SCRATCH_BYTES];
 

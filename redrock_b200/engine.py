@@ -764,6 +764,12 @@ def run_plain(pt, basis, prior=None, method=_lib.RR_SOLVE_PCA, stream=None, boun
 # small LRU caches keyed by object identity
 # ---------------------------------------------------------------------------
 class IdCache:
+    """LRU cache whose entries are valid while the same objects (by
+    identity) are passed again.  Identity says nothing about contents: a
+    caller that changes a cached object's arrays in place (a target's flux
+    or ivar, say) must clear the cache (``redrock_b200.zscan.clear_caches``)
+    before the next call, or it gets the results of the old contents."""
+
     def __init__(self, size=8):
         self.size = size
         self.d = OrderedDict()

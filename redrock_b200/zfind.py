@@ -56,26 +56,8 @@ def calc_deltachi2(chi2, z, zwarn, dvlimit=MAX_VELO_DIFF):
     okfit = (zwarn & BADFIT_MASK) == 0
     if np.isscalar(dvlimit):
         dvlimit = np.full(nz, dvlimit)
-    if all(np.asarray(v).dtype == np.float64 and np.all(np.isfinite(v))
-           for v in (chi2, z, dvlimit)):
-        return _deltachi2_f64(chi2, z, okfit, dvlimit)
-    for i in range(len(chi2) - 1):
-        dv = _fitz.get_dv(z[i + 1:], z[i])
-        ii = (np.abs(dv) > np.minimum(dvlimit[i], dvlimit[i + 1:])) & okfit[i + 1:]
-        if np.any(ii):
-            dchi2 = chi2[i + 1:] - chi2[i]
-            deltachi2[i] = np.min(dchi2[ii])
-    noti = np.ones(nz, dtype=bool)
-    setzwarn = np.zeros(nz, dtype=bool)
-    for i in range(nz):
-        noti[:] = True
-        noti[i] = False
-        alldeltachi2 = np.absolute(chi2[noti] - chi2[i])
-        alldv = np.absolute(_fitz.get_dv(z=z[noti], zref=z[i]))
-        alldvlimit = np.minimum(dvlimit[i], dvlimit[noti])
-        if np.any(okfit[noti] & (alldeltachi2 < MIN_DELTACHI2) & (alldv >= alldvlimit)):
-            setzwarn[i] = True
-    return deltachi2, setzwarn
+    return _deltachi2_f64(np.asarray(chi2, dtype=np.float64), np.asarray(z, dtype=np.float64),
+                          okfit, np.asarray(dvlimit, dtype=np.float64))
 
 
 def _deltachi2_f64(chi2, z, okfit, dvlimit):
@@ -90,7 +72,8 @@ def _deltachi2_f64(chi2, z, okfit, dvlimit):
         for j in range(i + 1, nz):
             if ok[j] and abs(_fitz.C_KMS * (zz[j] - zz[i]) / (1.0 + zz[i])) > min(dl[i], dl[j]):
                 d = c[j] - c[i]
-                if best is None or d < best:
+                # a NaN difference sticks, as in numpy's min
+                if best is None or d < best or d != d:
                     best = d
         if best is not None:
             deltachi2[i] = best

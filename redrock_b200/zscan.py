@@ -11,7 +11,9 @@
 
 Inputs are redrock's own objects (or the mirrors in redrock_b200.targets /
 redrock_b200.templates); outputs are the same numpy arrays with the same
-shapes.  Error conventions follow redrock: all-zero weights give HUGE_CHI2
+shapes.  Device copies of packed targets and template bases are cached by
+the identity of the objects they came from; after changing a Target's or a
+DistTemplate's arrays in place, call ``clear_caches()``.  Error conventions follow redrock: all-zero weights give HUGE_CHI2
 rows with zero coefficients; an exactly singular normal matrix gives
 HUGE_CHI2 at that z; an unrecognised solve method gives HUGE_CHI2
 everywhere.  Non-negative / bounded solvers (NMF, NNLS, BVLS) run on the
@@ -35,6 +37,13 @@ HUGE_CHI2 = 9999999.0
 
 _pack_cache = IdCache(64)
 _basis_cache = IdCache(32)
+
+
+def clear_caches():
+    """Drop the device copies of packed targets and template bases (needed
+    after a caller modifies those objects' arrays in place)."""
+    _pack_cache.clear()
+    _basis_cache.clear()
 
 
 def spectral_data(spectra):

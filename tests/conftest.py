@@ -11,6 +11,22 @@ if ROOT not in sys.path:
 GOLDEN = os.path.join(ROOT, "tests", "golden", "redrock_golden.npz")
 
 
+def redrock_dir():
+    """Directory holding an unmodified redrock package, or None: the
+    reference install at baseline/_ref (pip --target), else $REDROCK_PY."""
+    for d in (os.path.join(ROOT, "baseline", "_ref"), os.environ.get("REDROCK_PY")):
+        if d and os.path.exists(os.path.join(d, "redrock", "zscan.py")):
+            return d
+    return None
+
+
+def redrock_test_data(name):
+    """Path of a file in redrock's own test data, or None when absent."""
+    d = redrock_dir()
+    p = None if d is None else os.path.join(d, "redrock", "test", "data", name)
+    return p if p and os.path.exists(p) else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 

@@ -17,7 +17,7 @@ camera, prior 0.1; with and without 2 nearest archetypes).
 redrock calls calc_zchi2_batch without a solve method there
 (archetypes.py:287) and solve_matrices fails on None.)
 
-    python tests/golden/make_archetype_golden.py
+    REDROCK_PY=<dir> python tests/golden/make_archetype_golden.py
 """
 
 import os

@@ -8,7 +8,7 @@ SHA-256 checksums (plus their sums, for diagnosis).  The cosmic-ray cases
 coadd synth.multi_exposure_targets(4, seed=62, cosmics=4) (four hits per
 exposure) with cosmics_nsig = 4 and 2.5.
 
-    python tests/golden/make_coadd_golden.py
+    REDROCK_PY=<dir> python tests/golden/make_coadd_golden.py
 """
 
 import os

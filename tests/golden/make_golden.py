@@ -1,17 +1,17 @@
 """Generate the golden fixtures in this directory by running redrock itself.
 
-Run in a checkout that has redrock's source at REDROCK_PY (default
-/root/reference/py); astropy and fitsio are stubbed because redrock only uses
-them for file I/O.  The fixtures hold redrock's outputs (and checksums of the
-generated inputs) for seeded synthetic inputs from redrock_b200.synth, so the
-tests can regenerate the inputs without redrock.
+Run with REDROCK_PY set to the directory that holds redrock's ``redrock``
+package (a source checkout's ``py/`` directory, or an install target);
+astropy and fitsio are stubbed because redrock only uses them for file I/O
+(tests/redrock_ref.py).  The fixtures hold redrock's outputs (and checksums
+of the generated inputs) for seeded synthetic inputs from
+redrock_b200.synth, so the tests can regenerate the inputs without redrock.
 
-    python tests/golden/make_golden.py
+    REDROCK_PY=<dir> python tests/golden/make_golden.py
 """
 
 import os
 import sys
-import types
 
 import numpy as np
 
@@ -20,84 +20,10 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
 
 from redrock_b200 import synth  # noqa: E402
-
-REDROCK_PY = os.environ.get("REDROCK_PY", "/root/reference/py")
-
-
-def import_redrock():
-    for name in ["astropy", "astropy.io", "astropy.io.fits", "astropy.table", "fitsio"]:
-        sys.modules.setdefault(name, types.ModuleType(name))
-    sys.modules["astropy.io.fits"].open = None
-    sys.modules["astropy.table"].Table = None
-    sys.modules["fitsio"].FITS = None
-    sys.modules["astropy"].io = sys.modules["astropy.io"]
-    sys.modules["astropy"].table = sys.modules["astropy.table"]
-    sys.modules["astropy.io"].fits = sys.modules["astropy.io.fits"]
-    sys.path.insert(0, REDROCK_PY)
-    import redrock.zscan
-    import redrock.rebin
-    import redrock.igm
-    import redrock.templates
-    import redrock.targets
-    import redrock.fitz
-    return redrock
-
-
-class _Column(np.ndarray):
-    """Stand-in for astropy.table.Column (array with a name)."""
-
-    def __new__(cls, data, name=None, dtype=None):
-        obj = np.asarray(data, dtype=dtype).view(cls)
-        obj.name = name
-        return obj
-
-
-class _Table(dict):
-    """Minimal stand-in for astropy.table.Table as zfind uses it (dict of
-    columns; the redrock numbers are untouched)."""
-
-    def __init__(self, cols=None):
-        super().__init__()
-        for k, v in (cols or {}).items():
-            self[k] = np.asarray(v)
-
-    @property
-    def colnames(self):
-        return list(self.keys())
-
-    @property
-    def columns(self):
-        return self
-
-    def move_to_end(self, key, last=True):
-        v = self.pop(key)
-        if last:
-            self[key] = v
-        else:
-            items = list(self.items())
-            self.clear()
-            self[key] = v
-            for k, x in items:
-                self[k] = x
-
-    def add_column(self, col):
-        self[col.name] = np.asarray(col)
-
-    def replace_column(self, name, col):
-        self[name] = np.asarray(col)
-
-
-def _vstack(tables):
-    out = _Table()
-    for k in tables[0].keys():
-        out[k] = np.concatenate([np.asarray(t[k]) for t in tables], axis=0)
-    return out
-
+from tests.redrock_ref import import_redrock, install_table_stubs  # noqa: E402,F401
 
 rr = import_redrock()
-sys.modules["astropy.table"].Table = _Table
-sys.modules["astropy.table"].vstack = _vstack
-sys.modules["astropy.table"].Column = _Column
+install_table_stubs()
 import redrock.zfind  # noqa: E402
 import scipy.sparse  # noqa: E402
 

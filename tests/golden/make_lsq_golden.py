@@ -4,7 +4,7 @@
 targets on every 150th GALAXY redshift, calc_zchi2 with an NMF GALAXY
 template (chi2, coefficients, [OII] penalty), and fitz on that scan.
 
-    python tests/golden/make_lsq_golden.py
+    REDROCK_PY=<dir> python tests/golden/make_lsq_golden.py
 """
 
 import os

@@ -6,7 +6,7 @@ tests/prior_cases.py: Gaussian and top-hat, the last target without a
 prior.  redrock's Priors reads a FITS file; the object is built directly
 and handed to zfind in place of the file.
 
-    python tests/golden/make_prior_golden.py
+    REDROCK_PY=<dir> python tests/golden/make_prior_golden.py
 """
 
 import os

@@ -48,6 +48,14 @@ def test_argument_errors_without_gpu():
     assert L.rr_igm_transmission(7, None, 1, None, 1, None, None) == _lib.RR_EINVAL
     assert L.rr_zscan_fused(None, None, 0, None, None, None) == _lib.RR_EINVAL
     assert L.rr_zchi2_batch_plain_workspace_bytes(100, 10, 4) > 100 * 10 * 4 * 8
+    # a byte count that overflows (or a negative size) reads as SIZE_MAX, so
+    # no workspace or scratch size check can pass it
+    size_max = 2 ** (8 * ctypes.sizeof(ctypes.c_size_t)) - 1
+    assert L.rr_zchi2_batch_plain_workspace_bytes(2 ** 62, 2 ** 30, 10) == size_max
+    assert L.rr_zchi2_batch_plain_workspace_bytes(-1, 10, 4) == size_max
+    assert L.rr_zchi2_batch_plain_noalloc(None, None, None, None, None, 2 ** 62, None, 8000,
+                                          2 ** 30, 10, 10, None, 0, None, None, None,
+                                          None) == _lib.RR_ESCRATCH
 
 
 def test_header_constants_match_binding():

@@ -1,15 +1,17 @@
 """Details-file I/O (redrock results.py) through redrock_b200.hdf5: the
-reader against a file that redrock itself wrote with h5py (when the
-reference checkout is present), and write -> read round trips."""
+reader against a file that redrock itself wrote with h5py (when redrock's
+test data is present: its install at baseline/_ref, or $REDROCK_PY), and write -> read round trips."""
 import os
 
 import numpy as np
 import pytest
 
-REF_H5 = "/root/reference/py/redrock/test/data/rrdetails-test.h5"
+from tests.conftest import redrock_test_data
+
+REF_H5 = redrock_test_data("rrdetails-test.h5")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_H5), reason="reference test data not present")
+@pytest.mark.skipif(REF_H5 is None, reason="redrock's test data not present")
 def test_read_redrock_written_details_file():
     from redrock_b200 import hdf5
     from redrock_b200.results import read_zfit, read_zscan, read_zscan_redrock
@@ -110,10 +112,10 @@ def test_hdf5_large_group_and_empty(tmp_path):
     assert 'g/600' not in f
 
 
-REF_ARCH = "/root/reference/py/redrock/test/data/rrarchetype-galaxy-test.fits"
+REF_ARCH = redrock_test_data("rrarchetype-galaxy-test.fits")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_ARCH), reason="reference test data not present")
+@pytest.mark.skipif(REF_ARCH is None, reason="redrock's test data not present")
 def test_archetype_file_as_redrock_reads_it():
     """Archetype(filename) without astropy gives the arrays redrock's own
     Archetype builds from the same file (redrock run here with
@@ -128,8 +130,7 @@ def test_archetype_file_as_redrock_reads_it():
     assert list(a.full_type) == ['GALAXY:::LRG_0', 'GALAXY:::ELG_1']
     np.testing.assert_allclose(a.wave[:2], [1228.0701754386, 1228.2701754386])
     before = set(sys.modules)
-    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
-    from make_golden import import_redrock
+    from tests.redrock_ref import import_redrock
 
     class _H:
         def __init__(self, fn):
@@ -141,7 +142,8 @@ def test_archetype_file_as_redrock_reads_it():
         def close(self):
             pass
 
-    rr = import_redrock()
+    from tests.conftest import redrock_dir
+    rr = import_redrock(redrock_dir())
     import redrock.archetypes as ra
     old = sys.modules["astropy.io.fits"].open
     ra.fits.open = lambda fn, memmap=False: _H(fn)
@@ -151,7 +153,7 @@ def test_archetype_file_as_redrock_reads_it():
         ra.fits.open = old
         # drop redrock and the astropy stand-ins again
         for name in set(sys.modules) - before:
-            if name.split(".")[0] in ("redrock", "astropy", "fitsio", "make_golden"):
+            if name.split(".")[0] in ("redrock", "astropy", "fitsio"):
                 del sys.modules[name]
     np.testing.assert_array_equal(a.flux, ref.flux)
     np.testing.assert_array_equal(a.wave, ref.wave)

@@ -13,8 +13,6 @@ This file is collected last so a stop-at-first-failure run has already run
 every other test; it needs nothing from them.
 """
 
-import ctypes
-
 import numpy as np
 import pytest
 
@@ -86,8 +84,9 @@ def test_noalloc_rejects_oversized_request():
     cap = 16 << 20
     # 3311 redshifts x 7958 pixels x 10 bases needs ~2 GB of scratch
     assert L.rr_zchi2_batch_plain_workspace_bytes(7958, 3311, 10) > cap
-    dummy = ctypes.c_void_p(1)
-    rc = L.rr_zchi2_batch_plain_noalloc(dummy, dummy, dummy, dummy, dummy, 7958, dummy, 8000,
-                                        3311, 10, 10, None, 0, dummy, dummy, None, None)
+    # null pointers: the size check answers first; were it ever to let the
+    # request through, the null checks would refuse it before any launch
+    rc = L.rr_zchi2_batch_plain_noalloc(None, None, None, None, None, 7958, None, 8000,
+                                        3311, 10, 10, None, 0, None, None, None, None)
     assert rc == _lib.RR_ESCRATCH
     assert "scratch" in _lib.status_string(rc)
