@@ -1,19 +1,24 @@
 """Throughput benchmark: chi2 evaluations per second (target x z x template).
 
-Workload (one "step"): 500 synthetic DESI-like targets (cameras b/r/z,
-P = 7958 pixels, 11-diagonal resolution, 5 % masked pixels) scanned against
-the full template set -- GALAXY (10 bases, 3311 z), QSO (4 bases, 3794 z,
-Inoue14 IGM) and 5 STAR subtypes (5 bases, 100 z) -- i.e. 7605 chi2
-evaluations per target, 3.8025 M per step.  A step runs the whole hot path:
-rebin + IGM bases for every template, target packing, and the fused scan
-(chi2, coefficients and [OII] penalty for every target, template and z).
+Workload (one "step", default ``uneven5000``): 5000 synthetic DESI-like
+targets (cameras b/r/z, P = 7958 pixels, 11-diagonal resolution with its
+width varying per camera, 0-40 % of pixels masked per target, 10 % of the
+targets with one camera dropped) scanned against the full template set --
+GALAXY (10 bases, 3311 z), QSO (4 bases, 3794 z, Inoue14 IGM) and 5 STAR
+subtypes (5 bases, 100 z) -- i.e. 7605 chi2 evaluations per target, 38.0 M
+per step.  A step runs the whole hot path: rebin + IGM bases for every
+template, target packing, the tensor-core y GEMM and the fused scan (chi2,
+coefficients and [OII] penalty for every target, template and z).  The
+500-target batch (``desi500``, 5 % masked) is reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU (torchrun, one process per GPU): every rank scans its own 500
-targets (weak scaling, no collective in the data path); the step time is the
-max over ranks.  ``--impl reference`` times the CPU restatement of redrock's
-scan (oracle/) on the host cores instead.
+Multi-GPU (torchrun, one process per GPU): every rank scans its own targets
+(weak scaling, no collective in the data path); the step time is the max
+over ranks.  ``--impl reference`` times redrock's own CPU path (the
+unmodified install at baseline/_ref: DistTemplate construction, then
+calc_zchi2_targets with one process per host core) on a sample of the same
+workload, or the CPU restatement in oracle/ when that install is absent.
 """
 
 from __future__ import annotations
@@ -33,7 +38,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 D_BAND = 11
-WORKLOAD = "zscan-desi-500x(GALAXY3311+QSO3794+5xSTAR100)"
+WORKLOAD_NAMES = {
+    "desi500": "zscan-desi-500x(GALAXY3311+QSO3794+5xSTAR100)",
+    "uneven5000": "zscan-uneven-5000x(GALAXY3311+QSO3794+5xSTAR100): 0-40% masked, "
+                  "10% one camera dropped, resolution width per camera",
+    "stress20000": "zscan-stress-20000x(GALAXY3311+QSO3794+5xSTAR100): 60% QSO-like z<=6 "
+                   "with Inoue14, S/N 0.5-50",
+}
+DEFAULT_WORKLOAD = "uneven5000"
+METRIC = "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3"
 
 
 def flops_per_eval(nb, npix):
@@ -112,21 +125,28 @@ WORKLOADS = {
 }
 
 
-def make_workload(ntarget, seed, zsub=None, workload="desi500"):
+def synth_targets(workload, n, seed, transmission=None):
+    """Seeded synthetic targets of a workload (plain numpy)."""
+    from redrock_b200 import synth
+    spec = dict(WORKLOADS[workload])
+    spec.pop("ntarget", None)
+    if "qso_frac" in spec:
+        return synth.make_population(n, seed=seed, transmission=transmission, **spec)
+    return synth.make_targets(n, seed=seed, **spec)
+
+
+def make_workload(ntarget, seed, zsub=None, workload=DEFAULT_WORKLOAD):
     from redrock_b200 import synth
     from redrock_b200 import targets as T
     from redrock_b200 import templates as TM
-    spec = dict(WORKLOADS[workload])
-    n = ntarget or spec.pop("ntarget")
-    spec.pop("ntarget", None)
-    if "qso_frac" in spec:
+    n = ntarget or WORKLOADS[workload]["ntarget"]
+    tr = None
+    if "qso_frac" in WORKLOADS[workload]:
         from redrock_b200.igm import transmission_Lyman
 
         def tr(z, w):
             return transmission_Lyman(np.array([z]), w, model="Inoue14")[0]
-        tg = synth.make_population(n, seed=seed, transmission=tr, **spec)
-    else:
-        tg = synth.make_targets(n, seed=seed, **spec)
+    tg = synth_targets(workload, n, seed, transmission=tr)
     tset = synth.template_set(zsub=zsub)
     rtg = T.from_synth(tg)
     tms = [TM.from_synth(ts) for ts in tset]
@@ -202,6 +222,9 @@ def run_ours(args, rank, world, local_rank):
     layout = GridLayout.from_dwave(synth.camera_grids())
     srcs = [TemplateSource.from_template(tm) for tm in tms]
     dbatch = TargetBatch(rtg, layout).to_device()
+    bases_gb = sum(len(tm.redshifts) * layout.pix_stride * (tm.nbasis + tm.nbasis % 2) * 8
+                   for tm in tms) / 1e9
+    pack_gb = dbatch.batch.nblock * dbatch.batch.npix_block * _lib.RW * _lib.LANES * 8 / 1e9
     st = StatusWord()
     ev_fused = []
 
@@ -315,12 +338,13 @@ def run_ours(args, rank, world, local_rank):
                 dist.barrier()
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
+            n_e2e = max(1, min(args.steps, args.e2e_steps))
             a.record()
-            for _ in range(args.steps):
+            for _ in range(n_e2e):
                 e2e_step()
             b.record()
         torch.cuda.synchronize()
-        e2e_ms = a.elapsed_time(b) / args.steps
+        e2e_ms = a.elapsed_time(b) / n_e2e
         if world > 1:
             v = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
             dist.all_reduce(v, op=dist.ReduceOp.MAX)
@@ -330,7 +354,7 @@ def run_ours(args, rank, world, local_rank):
             2 * 8 * (n + 1) for n in layout.npix)
         d2h = sum(len(rtg) * len(tm.redshifts) * (2 + tm.nbasis) * 8 for tm in tms)
         e2e = {"value": world * evals / (e2e_ms / 1e3), "unit": "chi2 evals/s",
-               "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(h2d),
+               "ms_per_step": e2e_ms, "steps": n_e2e, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "path": "redrock_b200.zscan.calc_zchi2_targets(DistTargetsCopy, [DistTemplate x7])"
                        " from host numpy arrays"}
@@ -367,19 +391,20 @@ def run_ours(args, rank, world, local_rank):
     fused_flops = flops - (y_flops if y_on_tc else 0.0)
     achieved = fused_flops / (kernel_ms / 1e3) / 1e12
     out = {
-        "metric": "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3",
+        "metric": METRIC,
         "value": value, "unit": "chi2 evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded DESI-like targets and "
         "templates, redrock_b200/synth.py)",
-        "config": {"workload": (WORKLOAD if args.workload == "desi500" else args.workload)
+        "config": {"workload": WORKLOAD_NAMES[args.workload]
                    if not args.ntargets and not args.zsub else
                    f"reduced {args.workload}: {len(rtg)} targets, zsub={args.zsub}",
                    "targets_per_gpu": len(rtg),
                    "templates": [tm.full_type for tm in tms],
                    "evals_per_step_per_gpu": evals,
                    "pixels_per_target": "7958 (fewer with a dropped camera)",
-                   "l2": "inputs larger than L2 (bases 3.2 GB + packed targets 0.4 GB per step)",
+                   "l2": (f"inputs larger than L2 (bases {bases_gb:.1f} GB + packed targets "
+                          f"{pack_gb:.2f} GB per step; L2 126 MB)"),
                    "parallelism": f"targets sharded {world}-way, no collective",
                    "cuda_graph": bool(args.graph),
                    "y_term": args.ygemm,
@@ -519,8 +544,106 @@ def ygemm_study(args, step, torch, evals):
 
 
 # ---------------------------------------------------------------------------
-# CPU restatement of redrock's scan (oracle), all host cores
+# CPU baseline: redrock's own CPU path (the unmodified install at
+# baseline/_ref), or the oracle restatement when that install is absent
 # ---------------------------------------------------------------------------
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def reference_available():
+    return os.path.exists(os.path.join(REF_DIR, "redrock", "zscan.py"))
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _import_reference():
+    """redrock from baseline/_ref, unmodified.  astropy and fitsio are not
+    installed; redrock uses them only for file I/O and zfind's output table,
+    so empty stand-in modules satisfy its imports."""
+    import types
+    for name in ("astropy", "astropy.io", "astropy.io.fits", "astropy.table", "fitsio"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules["astropy"].io = sys.modules["astropy.io"]
+    sys.modules["astropy"].table = sys.modules["astropy.table"]
+    sys.modules["astropy.io"].fits = sys.modules["astropy.io.fits"]
+    sys.modules["astropy.io.fits"].open = None
+    sys.modules["astropy.table"].Table = None
+    sys.modules["fitsio"].FITS = None
+    sys.path.insert(0, REF_DIR)
+    import redrock.igm  # noqa: F401
+    import redrock.rebin  # noqa: F401
+    import redrock.targets  # noqa: F401
+    import redrock.templates  # noqa: F401
+    import redrock.zscan  # noqa: F401
+    return sys.modules["redrock"]
+
+
+def _reference_samples(workload, per_core, zsub, seed, ncores, nsample):
+    """nsample samples of the workload through redrock's own CPU path, in
+    this (torch-free) process: per sample, DistTemplate of every template
+    on every zsub-th redshift (one process, as redrock does without MPI),
+    then calc_zchi2_targets(mp_procs=ncores) over ncores * per_core
+    targets.  Each sample is extrapolated to the whole workload: template
+    builds scale with the redshifts per template, the scan with the
+    evaluations."""
+    import contextlib
+    import io
+
+    import scipy.sparse
+    rr = _import_reference()
+    from redrock_b200 import synth
+    tr = None
+    if "qso_frac" in WORKLOADS[workload]:
+        def tr(z, w):
+            return rr.igm.transmission_Lyman(np.array([z]), w, model="Inoue14")[0]
+    full_nz = [len(ts.redshifts) for ts in synth.template_set()]
+    tset = synth.template_set(zsub=zsub)
+    # the rebin's numba JIT compiles before anything is timed
+    rr.rebin.trapz_rebin(np.arange(10.), np.ones((1, 10)), edges=[1., 2., 3.],
+                         myz=np.array([0.0]))
+    ntarget_full = WORKLOADS[workload]["ntarget"]
+    out = []
+    for k in range(nsample):
+        tg = synth_targets(workload, ncores * per_core, seed + k, transmission=tr)
+        targets = []
+        for t in tg:
+            sp = [rr.targets.Spectrum(s.wave, s.flux.copy(), s.ivar.copy(),
+                                      scipy.sparse.dia_matrix((s.rdata, s.roffsets),
+                                                              shape=(len(s.wave),) * 2),
+                                      band=s.band) for s in t.spectra]
+            targets.append(rr.targets.Target(t.targetid, sp))
+        tms = [rr.templates.Template(spectype=ts.spectype, subtype=ts.subtype,
+                                     redshifts=ts.redshifts, wave=ts.wave, flux=ts.flux,
+                                     method=ts.method, igm_model=ts.igm_model) for ts in tset]
+        dtg = rr.targets.DistTargetsCopy(targets)
+        dwave = dtg.wavegrids()
+        build = []
+        with contextlib.redirect_stdout(io.StringIO()):
+            dts = []
+            for tm in tms:
+                t0 = time.perf_counter()
+                dts.append(rr.templates.DistTemplate(tm, dwave))
+                build.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            rr.zscan.calc_zchi2_targets(dtg, dts, mp_procs=ncores)
+            scan = time.perf_counter() - t0
+        evals = len(targets) * sum(len(ts.redshifts) for ts in tset)
+        evals_full = ntarget_full * sum(full_nz)
+        build_full = sum(b * nf / len(ts.redshifts) for b, nf, ts in zip(build, full_nz, tset))
+        scan_full = scan * evals_full / evals
+        out.append({"version": getattr(rr, "__version__", "unknown"),
+                    "evals": evals, "build_s": sum(build), "scan_s": scan,
+                    "value": evals_full / (build_full + scan_full),
+                    "scan_value": evals / scan, "build_full_s": build_full,
+                    "scan_full_s": scan_full, "targets": len(targets)})
+    return out
+
+
 def _cpu_worker(args):
     seed, ntarget, zsub, barrier = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
@@ -546,8 +669,9 @@ def _cpu_worker(args):
     return evals, time.perf_counter() - t0
 
 
-def cpu_scan_sample(nproc, per_worker, zsub, seed=1):
-    """(evals/s, cores, sample description) of the oracle on host cores."""
+def port_scan_sample(nproc, per_worker, zsub, seed=1):
+    """(evals/s, cores, sample description) of the oracle restatement of
+    redrock's scan on host cores (bases built before timing)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Manager() as mgr:
@@ -557,30 +681,78 @@ def cpu_scan_sample(nproc, per_worker, zsub, seed=1):
                                          for i in range(nproc)])
     evals = sum(r[0] for r in res)
     wall = max(r[1] for r in res)
-    sample = (f"{nproc} processes x {per_worker} targets x all 7 templates at every "
-              f"{zsub}th redshift ({evals} evals, {wall:.1f} s); bases built before timing")
+    sample = (f"oracle restatement (redrock install absent): {nproc} processes x {per_worker} "
+              f"targets x all 7 templates at every {zsub}th redshift ({evals} evals, "
+              f"{wall:.1f} s); bases built before timing")
     return evals / wall, nproc, sample
+
+
+def reference_cpu(workload, per_core, zsub, seed, nsample):
+    """Samples of redrock's own CPU path, each run in a fresh interpreter
+    (no CUDA context in the processes redrock forks).  Returns (samples,
+    cores, description) or None when baseline/_ref is absent."""
+    if not reference_available():
+        return None
+    ncores = host_cores()
+    env = dict(os.environ)
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMBA_NUM_THREADS"):
+        env[k] = "1"
+    cmd = [sys.executable, os.path.abspath(__file__), "--reference-worker",
+           json.dumps({"workload": workload, "per_core": per_core, "zsub": zsub, "seed": seed,
+                       "ncores": ncores, "nsample": nsample})]
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference worker failed: {r.stderr[-2000:]}")
+    samples = json.loads(r.stdout.strip().splitlines()[-1])
+    s0 = samples[-1]
+    ver = s0["version"]
+    desc = (f"redrock {ver} (unmodified, baseline/_ref) on {ncores} host cores: per sample "
+            f"{s0['targets']} targets x 7 templates at every {zsub}th redshift "
+            f"({s0['evals']} evals); DistTemplate builds {s0['build_s']:.2f} s (one process, "
+            f"as redrock without MPI), calc_zchi2_targets(mp_procs={ncores}) "
+            f"{s0['scan_s']:.2f} s; extrapolated to {WORKLOADS[workload]['ntarget']} targets on "
+            f"the full z grids (builds x redshifts, scan x evals): "
+            f"{s0['build_full_s']:.1f} s + {s0['scan_full_s']:.1f} s")
+    return samples, ncores, desc
+
+
+def cpu_baseline_entry(workload, args):
+    """The cpu_baseline object of our arm's line (one bounded sample)."""
+    ref = reference_cpu(workload, args.ref_per_core, args.ref_zsub, seed=100, nsample=1)
+    if ref is not None:
+        samples, cores, desc = ref
+        return {"value": samples[0]["value"], "unit": "chi2 evals/s", "cores": cores,
+                "kind": "reference", "sample": desc,
+                "scan_only_value": samples[0]["scan_value"]}
+    v, cores, sample = port_scan_sample(host_cores(), 4, 5)
+    return {"value": v, "unit": "chi2 evals/s", "cores": cores, "kind": "port", "sample": sample}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    ncpu = os.cpu_count() or 1
-    vals = []
-    for i in range(args.warmup + args.steps):
-        v, cores, sample = cpu_scan_sample(ncpu, args.ref_targets, args.ref_zsub, seed=100 + i)
-        if i >= args.warmup:
-            vals.append(v)
+    ref = reference_cpu(args.workload, args.ref_per_core, args.ref_step_zsub, seed=100,
+                        nsample=args.warmup + args.steps)
+    if ref is not None:
+        samples, cores, desc = ref
+        vals = [x["value"] for x in samples[args.warmup:]]
+        kind = "reference"
+    else:
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, cores, desc = port_scan_sample(host_cores(), 4, 5, seed=100 + i)
+            if i >= args.warmup:
+                vals.append(v)
+        kind = "port"
     value = float(np.median(vals))
     return {
-        "metric": "chi2 evals/s (target x z x template) on 1 B200, fused vs plain, |dchi2|<=1e-3",
-        "impl": "reference", "value": value, "unit": "chi2 evals/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded DESI-like targets and templates)",
-        "config": {"workload": WORKLOAD if args.workload == "desi500" else args.workload},
-        "cpu_baseline": {"value": value, "unit": "chi2 evals/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "chi2 evals/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded DESI-like targets and templates, redrock_b200/synth.py)",
+        "config": {"workload": WORKLOAD_NAMES[args.workload]},
+        "cpu_baseline": {"value": value, "unit": "chi2 evals/s", "cores": cores, "kind": kind,
+                         "sample": desc},
         "e2e": {"value": value, "unit": "chi2 evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -592,13 +764,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="desi500", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--ntargets", type=int, default=None,
                     help="override the workload's number of targets")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--zsub", type=int, default=None,
                     help="keep every zsub-th redshift (small profiling cases only)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=8,
+                    help="end-to-end steps timed (at most --steps)")
     ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
                     help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
                          "summed in the FP64 scan (fp64)")
@@ -612,32 +786,56 @@ def main():
                     help="also time every y variant once and report its chi2/coeff error")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the desi500 line reported beside the main workload")
     ap.add_argument("--graph", action="store_true",
                     help="capture the device step as a CUDA graph and replay it")
     ap.add_argument("--plain-targets", type=int, default=8)
-    ap.add_argument("--ref-zsub", type=int, default=5)
-    ap.add_argument("--ref-targets", type=int, default=4)
+    ap.add_argument("--ref-zsub", type=int, default=10,
+                    help="redshift subsampling of the cpu_baseline sample")
+    ap.add_argument("--ref-step-zsub", type=int, default=20,
+                    help="redshift subsampling of each --impl reference step")
+    ap.add_argument("--ref-per-core", type=int, default=2,
+                    help="targets per host core in a reference sample")
+    ap.add_argument("--reference-worker", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.reference_worker is not None:
+        # child process of reference_cpu: redrock's CPU path, no torch
+        kw = json.loads(args.reference_worker)
+        print(json.dumps(_reference_samples(**kw)))
+        return
     rank, world, local_rank = env_rank()
+    if args.impl == "reference":
+        # rank 0 alone times the CPU path; the other ranks have no work
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
     if world > 1:
         import datetime
 
         import torch
         import torch.distributed as dist
-        if args.impl == "ours":
-            torch.cuda.set_device(local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        else:
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-    if args.impl == "reference":
-        out = run_reference(args, rank, world)
-    else:
-        out = run_ours(args, rank, world, local_rank)
-        if out is not None and world == 1 and not args.no_cpu_baseline:
-            v, cores, sample = cpu_scan_sample(os.cpu_count() or 1, args.ref_targets,
-                                               args.ref_zsub)
-            out["cpu_baseline"] = {"value": v, "unit": "chi2 evals/s", "cores": cores,
-                                   "kind": "port", "sample": sample}
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, local_rank)
+    if out is not None and world == 1 and not args.no_extra and args.workload != "desi500" \
+            and not args.ntargets and not args.zsub:
+        # the 500-target batch beside the main workload (fewer steps)
+        ex = argparse.Namespace(**vars(args))
+        ex.workload = "desi500"
+        ex.steps, ex.warmup = min(args.steps, 5), min(args.warmup, 3)
+        ex.e2e_steps = min(args.e2e_steps, 5)
+        ex.no_plain = False
+        ex.plain_targets = args.plain_targets
+        ex.ygemm_study = ex.adjoint = ex.archetypes = False
+        import torch
+        torch.cuda.empty_cache()
+        d = run_ours(ex, rank, world, local_rank)
+        out["desi500"] = {k: d[k] for k in ("value", "ms_per_step", "e2e", "plain", "roofline",
+                                            "config", "clocks", "gpu_launches")}
+    if out is not None and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_entry(args.workload, args)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

@@ -19,5 +19,5 @@ __version__ = "0.1.0"
 
 
 def install(redrock_pkg=None, **kw):
-    from .install import install as _install
+    from .installer import install as _install
     return _install(redrock_pkg, **kw)

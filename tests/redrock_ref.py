@@ -95,3 +95,26 @@ def install_table_stubs():
     sys.modules["astropy.table"].Table = _Table
     sys.modules["astropy.table"].vstack = _vstack
     sys.modules["astropy.table"].Column = _Column
+
+
+def ref_targets(rr, specs):
+    """redrock Target objects (its own Spectrum with a scipy DIA R) from
+    synthetic target specs."""
+    import scipy.sparse
+    out = []
+    for t in specs:
+        spectra = []
+        for s in t.spectra:
+            npix = len(s.wave)
+            R = scipy.sparse.dia_matrix((s.rdata, s.roffsets), shape=(npix, npix))
+            spectra.append(rr.targets.Spectrum(s.wave, s.flux.copy(), s.ivar.copy(), R,
+                                               band=s.band))
+        out.append(rr.targets.Target(t.targetid, spectra))
+    return out
+
+
+def ref_template(rr, ts):
+    """redrock Template from a synthetic template spec."""
+    return rr.templates.Template(spectype=ts.spectype, subtype=ts.subtype,
+                                 redshifts=ts.redshifts, wave=ts.wave, flux=ts.flux,
+                                 method=ts.method, igm_model=ts.igm_model)

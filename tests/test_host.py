@@ -7,7 +7,7 @@ import pytest
 
 from redrock_b200 import _lib, synth
 from redrock_b200.engine import GridLayout, TargetBatch, centers2edges, round_up
-from redrock_b200.install import PATCHES, install
+from redrock_b200.installer import PATCHES, install
 from redrock_b200.targets import DistTargetsCopy, distribute_work, from_synth
 
 
@@ -122,6 +122,37 @@ def test_installer_rebinds_every_import_site():
         assert callable(getattr(mods[sub], attr))
     assert mods["fitz"].calc_zchi2_batch.__module__ == "redrock_b200.zscan"
     assert mods["templates"].DistTemplate.__module__ == "redrock_b200.templates"
+
+
+def test_installer_on_unmodified_redrock():
+    """install() on the real redrock package (its install at baseline/_ref,
+    or $REDROCK_PY) rebinds every listed name in redrock's own modules."""
+    import sys
+    from tests.conftest import redrock_dir
+    from redrock_b200.installer import FUSED_TARGETS, METHOD_PATCHES
+    d = redrock_dir()
+    if d is None:
+        pytest.skip("redrock not installed at baseline/_ref and REDROCK_PY unset")
+    before = set(sys.modules)
+    path0 = list(sys.path)
+    try:
+        from tests.redrock_ref import import_redrock, install_table_stubs
+        rr = import_redrock(d)
+        install_table_stubs()
+        import redrock.zfind  # noqa: F401
+        own_batch = rr.fitz.calc_zchi2_batch
+        done = install(rr)
+        assert len(done) == len(PATCHES) + len(FUSED_TARGETS) + len(METHOD_PATCHES)
+        assert rr.fitz.calc_zchi2_batch is not own_batch
+        assert rr.fitz.calc_zchi2_batch.__module__ == "redrock_b200.zscan"
+        assert rr.templates.rebin_template.__module__ == "redrock_b200.rebin"
+        assert rr.zfind.calc_zchi2_targets.__module__ == "redrock_b200.zscan"
+        assert rr.targets.Target.compute_coadd.__module__ == "redrock_b200.coadd"
+    finally:
+        for name in set(sys.modules) - before:
+            if name.split(".")[0] in ("redrock", "astropy", "fitsio"):
+                del sys.modules[name]
+        sys.path[:] = path0
 
 
 def test_flop_model():
