@@ -316,41 +316,43 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
         if has_oii:
             c2all += pen.reshape(len(key), nz)
         fits = [None] * len(key)
-        if refine != "newton" and nz >= 3:
-            # the parabola of every candidate in one pass (the replay below
-            # only picks the ones it reaches)
+        if nz >= 3:
+            # every candidate's refinement in one pass (the replay below only
+            # picks the ones it reaches): the parabola through the three
+            # fine-grid points around the best one, or Newton steps inside
+            # that cell for all candidates in one batch of pair launches
             ib = np.clip(np.argmin(c2all, axis=1), 1, nz - 2)
             cols = ib[:, None] + np.arange(-1, 2)[None, :]
             rows = np.arange(len(key))[:, None]
-            fx0, ferr, fy0, fzw = minfit_batch(zzall[rows, cols], c2all[rows, cols])
+            if refine == "newton":
+                fx0, ferr, fy0, fzw = newton_batch([k[0] for k in key], zzall[rows, cols])
+            else:
+                fx0, ferr, fy0, fzw = minfit_batch(zzall[rows, cols], c2all[rows, cols])
             fits = list(zip(fx0.tolist(), ferr.tolist(), fy0.tolist(), fzw.tolist()))
         for n_, (j, imin) in enumerate(key):
             fine[j][imin] = (zzall[n_], c2all[n_], fits[n_])
 
     newton_ctx = {}
 
-    def newton_min(j, z3, chi2_mid):
-        # safeguarded Newton in [z3[0], z3[2]] from z3[1]
+    def newton_batch(tj, z3):
+        # safeguarded Newton in [z3[:, 0], z3[:, 2]] from z3[:, 1], all
+        # candidates together: one pair-gradient launch per Newton iteration
         from .adjoint import refine_newton
         ctx = newton_ctx.get("ctx")
         if ctx is None:
             ctx = newton_ctx["ctx"] = _NewtonCtx(ref)
-        z, c2, co, g, h, _ = refine_newton(ctx, np.array([j], dtype=np.int32),
-                                           np.array([z3[1]]), np.array([z3[0]]),
-                                           np.array([z3[2]]))
-        zwarn = 0
-        if h[0] > 0:
-            sigma = np.sqrt(2.0 / h[0])
-        else:
-            sigma = -1.0
-            zwarn |= BAD_MINFIT
-        if not (z3[0] < z[0] < z3[2]):
-            zwarn |= BAD_MINFIT
-        pen = 0.0
+        z, c2, co, g, h, _ = refine_newton(ctx, np.asarray(tj, dtype=np.int32), z3[:, 1],
+                                           z3[:, 0], z3[:, 2])
+        zwarn = np.zeros(len(z), dtype=np.int64)
+        pos_h = h > 0
+        sigma = np.where(pos_h, np.sqrt(2.0 / np.where(pos_h, h, 1.0)), -1.0)
+        zwarn[~pos_h] |= BAD_MINFIT
+        zwarn[~((z3[:, 0] < z) & (z < z3[:, 2]))] |= BAD_MINFIT
+        pen = np.zeros(len(z))
         if has_oii:
-            s_ = float(np.dot(co[0], ref.src.oii))
-            pen = -s_ if s_ < 0 else 0.0
-        return z[0], sigma, c2[0] + pen, zwarn
+            s_ = co @ np.asarray(ref.src.oii, dtype=np.float64)
+            pen = np.where(s_ < 0, -s_, 0.0)
+        return z, sigma, c2 + pen, zwarn
 
     pending_final = []   # (target, result dict, zmin)
     active = list(range(ntg))
@@ -370,9 +372,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                     continue
                 zz, zzchi2, fit = fine[j][imin]
                 i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
-                if refine == "newton":
-                    zmin, sigma, chi2min, zwarn = newton_min(j, zz[i - 1:i + 2], zzchi2[i])
-                elif fit is not None:
+                if fit is not None:
                     zmin, sigma, chi2min, zwarn = fit
                 else:
                     zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])

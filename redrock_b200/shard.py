@@ -16,6 +16,46 @@ import torch.distributed as dist
 from .targets import distribute_work
 
 
+class TorchComm:
+    """The mpi4py-style communicator redrock's distributed objects expect
+    (``rank``, ``size``, ``bcast``, ``allgather``, ``gather``, ``barrier``)
+    over a torch.distributed process group.  Python objects travel through
+    a gloo group (host memory), made from the default group's ranks unless
+    one is given, so large result dicts never pass through GPU buffers."""
+
+    def __init__(self, group=None):
+        if group is None:
+            group = dist.new_group(backend="gloo") \
+                if dist.get_backend() != "gloo" else dist.group.WORLD
+        self.group = group
+
+    @property
+    def rank(self):
+        return dist.get_rank(self.group)
+
+    @property
+    def size(self):
+        return dist.get_world_size(self.group)
+
+    def bcast(self, obj, root=0):
+        buf = [obj]
+        dist.broadcast_object_list(buf, src=root, group=self.group)
+        return buf[0]
+
+    def allgather(self, obj):
+        out = [None] * self.size
+        dist.all_gather_object(out, obj, group=self.group)
+        return out
+
+    def gather(self, obj, root=0):
+        out = [None] * self.size if self.rank == root else None
+        dist.gather_object(obj, out, dst=root, group=self.group)
+        return out
+
+    def barrier(self):
+        dist.barrier(group=self.group)
+
+
 def rank_world():
     if dist.is_available() and dist.is_initialized():
         return dist.get_rank(), dist.get_world_size()

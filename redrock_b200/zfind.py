@@ -21,8 +21,15 @@ a dict of numpy columns (``astropy.table.Table(allzfit)`` gives redrock's
 table) with redrock's column names and order of rows.  ``priors`` is a
 ``redrock_b200.priors.Priors`` (or redrock's) object, or a prior file name.
 ``chi2_scan`` names a details file (``redrock_b200.results.write_zscan`` or
-redrock's) whose coarse scans replace the scan.  Single-process only
-(``targets.comm`` None).
+redrock's) whose coarse scans replace the scan.
+
+Several processes (one per GPU): give the targets an mpi4py-style
+communicator (``rank``, ``size``, ``bcast``, ``allgather``, ``gather``,
+``barrier``; ``redrock_b200.shard.TorchComm`` wraps a torch.distributed
+group).  Each rank scans and refines its own targets against every redshift
+of every template (redrock's GPU mode, templates.py:558-563); the per-target
+results are then gathered on rank 0 (zfind.py:416-456), which finalises and
+returns them, while the other ranks return ``(None, None)``.
 """
 
 from __future__ import annotations
@@ -213,13 +220,11 @@ def _finalise_target(tid, fits, nminima, arch=None):
 
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
-          n_nearest=None, prior_sigma=None, ncamera=None):
+          n_nearest=None, prior_sigma=None, ncamera=None, refine="parabola"):
     if priors is not None and not hasattr(priors, 'eval'):
         from .priors import Priors
         priors = Priors(priors)
-    if targets.comm is not None and targets.comm.size > 1:
-        raise NotImplementedError("use one process per GPU with its own targets (see "
-                                  "redrock_b200.shard) instead of an MPI communicator")
+    comm = targets.comm
     if chi2_scan is None:
         results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
     else:
@@ -234,7 +239,10 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
     local = list(targets.local())
     # the targets' packed rows for the fine-grid pair scans do not depend on
     # the template: pack them once for every template's refinement
-    layout = GridLayout.from_dwave(targets.wavegrids()) if local else None
+    # wavegrids() is collective when the targets have a communicator: every
+    # rank calls it, with or without local targets
+    dwave = targets.wavegrids()
+    layout = GridLayout.from_dwave(dwave) if local else None
     rowpack = RowPack.from_targets(local, layout) if local else None
     sort = np.array([t.template.full_type for t in templates]).argsort()
     arch = None
@@ -245,7 +253,7 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
                 all_spectypes.append(t.template.template_type)
         arch = dict(spectypes=list(archetypes.keys()), all_spectypes=all_spectypes,
                     n_nearest=n_nearest)
-    for t in np.array(list(templates), dtype=object)[sort]:
+    for t in np.array(list(templates), dtype=object)[sort] if local else []:
         ft = t.template.full_type
         archetype = archetypes.get(t.template._rrtype) if archetypes else None
         chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
@@ -253,12 +261,23 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
                                   nminima=nminima, archetype=archetype, use_gpu=use_gpu,
                                   deg_legendre=deg_legendre, zminfit_npoints=zminfit_npoints,
                                   per_camera=per_camera, n_nearest=n_nearest,
-                                  prior_sigma=prior_sigma, layout=layout, rowpack=rowpack)
+                                  prior_sigma=prior_sigma, layout=layout, rowpack=rowpack,
+                                  refine=refine)
         for tg, zf in zip(local, fits):
             results[tg.id][ft]['zfit'] = zf
     for tg in local:
         results[tg.id]['meta'] = tg.meta
-    allresults = results
+    if comm is not None and comm.size > 1:
+        # every rank's results on rank 0, rank order kept (zfind.py:416-456)
+        parts = comm.gather(results, root=0)
+        comm.barrier()
+        if comm.rank != 0:
+            return None, None
+        allresults = {}
+        for part in parts:
+            allresults.update(part)
+    else:
+        allresults = results
     rows = []
     for tid in targets.all_target_ids:
         fits = [(ft, allresults[tid][ft]['zfit']) for ft in allresults[tid] if ft != 'meta']

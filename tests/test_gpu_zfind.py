@@ -124,3 +124,36 @@ def test_zfind_details_file_resume(golden, tmp_path):
     np.testing.assert_array_equal(zfit2['targetid'][best2], zfit['targetid'][best])
     np.testing.assert_array_equal(zfit2['spectype'][best2], zfit['spectype'][best])
     np.testing.assert_allclose(zfit2['z'][best2], zfit['z'][best], rtol=0, atol=1e-6)
+
+
+def test_zfind_newton_refinement(golden):
+    """zfind(refine="newton"): every template's minima refined by batched
+    Newton steps on chi2(z) (one pair-gradient launch per iteration for all
+    candidates) instead of the parabola.  Same targets and row structure as
+    the parabola path; each good redshift within a fine-grid step of the
+    parabola's, with a chi2 (a real evaluation at that z) no higher than the
+    best fine-grid point it started from."""
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.zfind import zfind
+    ztg = synth.make_targets(5, seed=41, amp=2.0, first_id=5000)
+    dz = T.DistTargetsCopy(T.from_synth(ztg))
+    sel = {"GALAXY": 23, "QSO": 31, "STAR:::K": 4, "STAR:::M": 4}
+    dts = []
+    for ts in synth.template_set():
+        if ts.full_type in sel:
+            ts.redshifts = ts.redshifts[::sel[ts.full_type]]
+            dts.append(TM.DistTemplate(TM.from_synth(ts), dz.wavegrids()))
+    _, par = zfind(dz, dts, nminima=3)
+    _, new = zfind(dz, dts, nminima=3, refine="newton")
+    assert list(new.keys()) == list(par.keys())
+    np.testing.assert_array_equal(new["targetid"], par["targetid"])
+    best = new["znum"] == 0
+    np.testing.assert_array_equal(new["spectype"][best], par["spectype"][best])
+    good = (new["zwarn"] == 0) & (par["zwarn"] == 0) & (new["spectype"] == par["spectype"])
+    assert good.sum() >= 5
+    for st, step in (("GALAXY", 23 * 3e-4), ("QSO", 31 * 5e-4), ("STAR", 4 * 4e-5)):
+        m = good & (new["spectype"] == st)
+        # a fine-grid step: the 15-point grid spans two coarse steps
+        assert np.all(np.abs(np.log1p(new["z"][m]) - np.log1p(par["z"][m])) <= step * 2 / 14
+                      + 1e-12)
+    assert np.all(new["zerr"][good] > 0)
