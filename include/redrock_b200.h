@@ -315,6 +315,25 @@ int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_segment* seg
                         double* dchi2_dflux, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * fitz candidates on the device: replaces the host steps of redrock's fitz
+ * between the coarse scan and the fine-grid evaluations --
+ * find_minima (fitz.py:46-67: local minima with <= comparisons, edges
+ * included, sorted by value) and the fine grids
+ * zz = np.linspace(z[i-1], z[i+1], nfine) (fitz.py:226-240, indices clipped)
+ * -- so that the scan and the fine-grid pair scans (rr_zscan_pairs on
+ * pair_t / pair_z) run without a host round trip.  Per target row of
+ * zchi2 + penalty ([ntarget][nz]; penalty may be NULL): the K (<= 8)
+ * smallest minima in cand[ntarget][K] (-1 past count[t]), tie[t] = 1 when
+ * equal values make redrock's (unstable) sort order undetermined -- sort
+ * those rows on the host -- and pair_z / pair_t [ntarget][K][nfine], the
+ * fine grid of each candidate (slots past count repeat candidate 0).
+ * ---------------------------------------------------------------------- */
+int rr_fitz_candidates(const double* zchi2, const double* penalty, int64_t ntarget, int64_t nz,
+                       const double* redshifts, int32_t K, int32_t nfine, int32_t* cand,
+                       int32_t* count, int8_t* tie, double* pair_z, int32_t* pair_t,
+                       rr_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Plain per-target path (the structure of redrock's own GPU branch: R.T for
  * all z into a workspace, then M and y, then the solve, then the model and
  * chi2).  First pack the target's spectra into band rows:

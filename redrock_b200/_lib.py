@@ -131,6 +131,9 @@ _SIGNATURES = {
     "rr_zscan_pairs": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment), c_int,
                                c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
                                c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "rr_fitz_candidates": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int32,
+                                   c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_void_p]),
     "rr_pack_band_rows": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_int64, c_void_p,
                                   c_void_p, c_void_p]),
     "rr_zchi2_batch_plain_workspace_bytes": (c_size_t, [c_int64, c_int32, c_int32]),

@@ -506,7 +506,7 @@ def _record(ev, stream):
 
 
 def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=None,
-              tiles=None):
+              tiles=None, external_events=False):
     """One persistent launch over every (target, template, z).  ygemm:
     None (DEFAULT_Y), "fp64", "int8x7", "bf16x3" or "tf32x3"; other than
     "fp64", y is computed on the tensor cores first (YGemm).  kernel_events:
@@ -539,8 +539,10 @@ def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=N
                                          ptr(r.y_ext) if yg is not None else None))
         arr = (_lib.ScanTemplate * len(tms))(*tms)
         if kernel_events is not None:
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            # external events become event-record nodes when the launches
+            # are captured in a CUDA graph, so each replay times them
+            e0 = torch.cuda.Event(enable_timing=True, external=external_events)
+            e1 = torch.cuda.Event(enable_timing=True, external=external_events)
             _record(e0, stream)
         if tiles:
             opt = _lib.ScanOptions(int(tiles.get(4, 0)), int(tiles.get(5, 0)))
@@ -641,6 +643,54 @@ def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
         torch.cuda.current_stream().synchronize()
         st.check("rr_zscan_pairs")
     return chi2, coeff, pen
+
+
+def run_pairs_device(rowpack, src, pair_target, pair_z, status, stream=None):
+    """run_pairs for pairs already on the device (int32 target indices and
+    float64 redshifts, both CUDA tensors); stays asynchronous (the caller's
+    status word reports kernel errors), so it can be captured in a graph."""
+    L = _lib.lib()
+    dev = device()
+    n = int(pair_z.numel())
+    nb = src.nbasis
+    chi2 = torch.empty(n, dtype=torch.float64, device=dev)
+    coeff = torch.empty((n, nb), dtype=torch.float64, device=dev)
+    pen = torch.zeros(n, dtype=torch.float64, device=dev)
+    if n == 0:
+        return chi2, coeff, pen
+    prior = getattr(src, "prior_dev", None)
+    tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0,
+                           ptr(prior), ptr(src.oii_dev))
+    segs = (_lib.PairSegment * len(rowpack.segments))(*rowpack.segments)
+    rc = L.rr_zscan_pairs(ctypes.byref(tm), segs, len(rowpack.segments), ptr(rowpack.rows),
+                          ptr(rowpack.fwf), ptr(rowpack.wsum), rowpack.npix_row, ptr(pair_target),
+                          ptr(pair_z), n, ptr(chi2), ptr(coeff), ptr(pen), status.ptr,
+                          stream_handle(stream))
+    _lib.check(rc, "rr_zscan_pairs")
+    return chi2, coeff, pen
+
+
+class FitzCandidates:
+    """The K lowest local minima of every target's coarse chi2 (plus
+    penalty) and their fine redshift grids, found on the device
+    (rr_fitz_candidates): cand [T][K] (-1 past count), count [T], tie [T]
+    (rows whose order must come from a host sort), and the pairs
+    pair_t / pair_z [T * K * nfine] of every candidate's fine grid."""
+
+    def __init__(self, zchi2, penalty, redshifts, K, nfine, stream=None):
+        L = _lib.lib()
+        dev = zchi2.device
+        T, nz = zchi2.shape
+        self.K, self.nfine = K, nfine
+        self.cand = torch.empty((T, K), dtype=torch.int32, device=dev)
+        self.count = torch.empty(T, dtype=torch.int32, device=dev)
+        self.tie = torch.empty(T, dtype=torch.int8, device=dev)
+        self.pair_z = torch.empty(T * K * nfine, dtype=torch.float64, device=dev)
+        self.pair_t = torch.empty(T * K * nfine, dtype=torch.int32, device=dev)
+        rc = L.rr_fitz_candidates(ptr(zchi2), ptr(penalty), T, nz, ptr(redshifts), K, nfine,
+                                  ptr(self.cand), ptr(self.count), ptr(self.tie),
+                                  ptr(self.pair_z), ptr(self.pair_t), stream_handle(stream))
+        _lib.check(rc, "rr_fitz_candidates")
 
 
 def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=None, status=None):

@@ -251,12 +251,34 @@ class _PlainRefiner:
         return chi2, coeff, pen, ok
 
 
+class PrecomputedFine:
+    """Host copies of device-evaluated fitz candidates for one template
+    (rr_fitz_candidates + one rr_zscan_pairs launch over their fine grids):
+    cand [T][K], count [T], tie [T], zz [T][K][nfine] and c2 [T][K][nfine]
+    (chi2, plus the [OII] penalty when the template has one)."""
+
+    def __init__(self, cand, count, tie, zz, c2):
+        self.cand = np.asarray(cand)
+        self.count = np.asarray(count)
+        self.tie = np.asarray(tie).astype(bool)
+        self.K = self.cand.shape[1]
+        self.zz = np.asarray(zz)
+        self.c2 = np.asarray(c2)
+
+
 def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=None,
                  use_gpu=True, deg_legendre=None, zminfit_npoints=15, per_camera=False,
                  n_nearest=None, prior_sigma=None, layout=None, rowpack=None, batch_extra=0,
-                 refine="parabola"):
+                 refine="parabola", pre=None):
     """redrock's fitz for many targets of one template; returns a list of
     per-target result dicts (the same dict-of-arrays fitz returns).
+
+    ``pre`` (optional): candidates and fine grids already evaluated on the
+    device for every target (``PrecomputedFine``: the K lowest minima of
+    each row from rr_fitz_candidates and the chi2 of their fine grids from
+    one pair launch).  Rows it covers skip the host find_minima and the
+    first launch; a row flagged as tied, or one that needs more than K
+    candidates, continues on the host exactly as without ``pre``.
 
     The first launch evaluates each target's first nminima + batch_extra
     candidate minima; targets whose candidates fall within max_velo_diff of
@@ -282,17 +304,33 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     has_oii = ref.oii is not None
 
     ntg = len(targets)
-    cands = [find_minima(np.asarray(z)) for z in zchi2_list]
-    pos = [0] * ntg           # next candidate to evaluate
+    use_pre = [pre is not None and not pre.tie[j] for j in range(ntg)]
+    # device candidate lists are the first K entries of find_minima's order
+    # (rows without ties); partial rows get the full host list when the
+    # replay needs more of them
+    cands = [pre.cand[j, :pre.count[j]] if use_pre[j] else find_minima(np.asarray(z))
+             for j, z in enumerate(zchi2_list)]
+    partial = [use_pre[j] and pre.count[j] == pre.K for j in range(ntg)]
+    pos = [int(pre.count[j]) if use_pre[j] else 0 for j in range(ntg)]
     fine = [dict() for _ in range(ntg)]   # imin -> (zz, zzchi2)
     results = [list() for _ in range(ntg)]
     state = [dict(ci=0) for _ in range(ntg)]   # replay cursor per target
     done = [False] * ntg
     want = nminima + batch_extra
 
+    def refine_fits(tj, zz3, c23):
+        if refine == "newton":
+            fx0, ferr, fy0, fzw = newton_batch(tj, zz3)
+        else:
+            fx0, ferr, fy0, fzw = minfit_batch(zz3, c23)
+        return list(zip(fx0.tolist(), ferr.tolist(), fy0.tolist(), fzw.tolist()))
+
     def fetch(tlist, count):
         tid, key = [], []
         for j in tlist:
+            if partial[j] and pos[j] >= len(cands[j]):
+                cands[j] = find_minima(np.asarray(zchi2_list[j]))
+                partial[j] = False
             c = cands[j]
             for imin in c[pos[j]:pos[j] + count]:
                 tid += [j] * nz
@@ -324,11 +362,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             ib = np.clip(np.argmin(c2all, axis=1), 1, nz - 2)
             cols = ib[:, None] + np.arange(-1, 2)[None, :]
             rows = np.arange(len(key))[:, None]
-            if refine == "newton":
-                fx0, ferr, fy0, fzw = newton_batch([k[0] for k in key], zzall[rows, cols])
-            else:
-                fx0, ferr, fy0, fzw = minfit_batch(zzall[rows, cols], c2all[rows, cols])
-            fits = list(zip(fx0.tolist(), ferr.tolist(), fy0.tolist(), fzw.tolist()))
+            fits = refine_fits([k[0] for k in key], zzall[rows, cols], c2all[rows, cols])
         for n_, (j, imin) in enumerate(key):
             fine[j][imin] = (zzall[n_], c2all[n_], fits[n_])
 
@@ -354,9 +388,27 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             pen = np.where(s_ < 0, -s_, 0.0)
         return z, sigma, c2 + pen, zwarn
 
+    if pre is not None and any(use_pre):
+        # the device-evaluated candidates: their fine grids and one batch of
+        # refinements, as fetch() would have made them
+        key = [(j, int(pre.cand[j, k])) for j in range(ntg) if use_pre[j]
+               for k in range(int(pre.count[j]))]
+        jj = np.array([k[0] for k in key])
+        kk = np.concatenate([np.arange(int(pre.count[j])) for j in range(ntg) if use_pre[j]])
+        zzp = pre.zz[jj, kk]
+        c2p = pre.c2[jj, kk]
+        fits = [None] * len(key)
+        if nz >= 3:
+            ib = np.clip(np.argmin(c2p, axis=1), 1, nz - 2)
+            cols = ib[:, None] + np.arange(-1, 2)[None, :]
+            rows = np.arange(len(key))[:, None]
+            fits = refine_fits(jj.tolist(), zzp[rows, cols], c2p[rows, cols])
+        for n_, (j, imin) in enumerate(key):
+            fine[j][imin] = (zzp[n_], c2p[n_], fits[n_])
+
     pending_final = []   # (target, result dict, zmin)
     active = list(range(ntg))
-    fetch(active, want)
+    fetch([j for j in active if not use_pre[j]], want)
     while active:
         need_more = []
         for j in active:
@@ -393,7 +445,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                          coeff=None, fitmethod=template.method)
                 results[j].append(r)
                 pending_final.append((j, r, zmin))
-            if len(results[j]) < nminima and st['ci'] < len(c):
+            if len(results[j]) < nminima and (st['ci'] < len(c) or partial[j]):
                 need_more.append(j)
         if need_more:
             fetch(need_more, want)

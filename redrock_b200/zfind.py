@@ -23,6 +23,16 @@ table) with redrock's column names and order of rows.  ``priors`` is a
 ``chi2_scan`` names a details file (``redrock_b200.results.write_zscan`` or
 redrock's) whose coarse scans replace the scan.
 
+``graph=True`` runs the device part for the whole local batch -- target
+packing, the fused scan, the K lowest minima of every (target, template) and
+the chi2 of their fine redshift grids (``DeviceFitzPlan``) -- as one
+captured CUDA graph, so no host round trip sits between the coarse scan and
+the fine grids; the host then replays redrock's candidate logic on those
+values exactly as the eager path does (rows with tied minima, and targets
+that need more than K candidates, continue on the host), so the outputs are
+the eager path's bit for bit.  ``refine="newton"`` replaces the parabola
+through the three fine-grid points by batched Newton steps on chi2(z).
+
 Several processes (one per GPU): give the targets an mpi4py-style
 communicator (``rank``, ``size``, ``bcast``, ``allgather``, ``gather``,
 ``barrier``; ``redrock_b200.shard.TorchComm`` wraps a torch.distributed
@@ -37,7 +47,8 @@ from __future__ import annotations
 import numpy as np
 
 from . import fitz as _fitz
-from .templates import parse_fulltype
+from . import _lib
+from .templates import parse_fulltype, solve_code
 from .engine import GridLayout, RowPack
 from .zscan import calc_zchi2_targets
 
@@ -218,14 +229,122 @@ def _finalise_target(tid, fits, nminima, arch=None):
     return out
 
 
+# candidates per target and template evaluated on the device in the graph
+# path (rr_fitz_candidates): nminima plus two spares for candidates that
+# fall within max_velo_diff of a better one
+DEVICE_CANDIDATES_EXTRA = 2
+
+
+class DeviceFitzPlan:
+    """The device part of zfind for one target batch -- target packing, the
+    fused coarse scan of every template, the K lowest chi2 minima of every
+    (target, template) and the chi2 of their fine redshift grids -- as one
+    stream of launches with no host round trip, optionally captured as a
+    CUDA graph and replayed.  ``run()`` returns the coarse-scan results in
+    calc_zchi2_targets' form and one ``fitz.PrecomputedFine`` per template.
+
+    Lazy one-time set-up (kernel attributes, constant tables, the tile
+    autotuner) happens in an eager warm-up on the first target block before
+    any capture."""
+
+    def __init__(self, local, templates, layout, nminima=3, nfine=15, graph=True):
+        import torch
+        from . import autotune
+        from .device import StatusWord, to_device
+        from .engine import TargetBatch, TargetPack, TemplateSource
+        from .zscan import _bases_for
+        self.local = local
+        self.templates = list(templates)
+        self.layout = layout
+        self.K = min(8, nminima + DEVICE_CANDIDATES_EXTRA)
+        self.nfine = nfine
+        self.status = StatusWord()
+        self.bases = _bases_for(self.templates, layout)
+        self.srcs = [TemplateSource.from_template(t.template) for t in self.templates]
+        self.zdev = [to_device(np.asarray(t.template.redshifts, dtype=np.float64))
+                     for t in self.templates]
+        self.dbatch = TargetBatch(local, layout).to_device()
+        self.rowpack = RowPack(self.dbatch)
+        pack0 = TargetPack(self.dbatch, status=self.status)
+        self.tiles = autotune.tiles_of(autotune.choice(pack0, self.bases)
+                                       or autotune.tune(pack0, self.bases))
+        del pack0
+        # warm-up on the first 32 targets: every kernel's lazy set-up
+        small = local[:32]
+        wb = TargetBatch(small, layout).to_device()
+        self._body(wb, RowPack(wb))
+        torch.cuda.synchronize()
+        self.status.check("zfind warm-up")
+        self.graph = None
+        if graph:
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self.outs = self._body(self.dbatch, self.rowpack)
+        else:
+            self.outs = None
+
+    def _body(self, dbatch, rowpack):
+        from .engine import FitzCandidates, TargetPack, run_fused, run_pairs_device
+        pack = TargetPack(dbatch, status=self.status)
+        res, _ = run_fused(pack, self.bases, status=self.status, tiles=self.tiles)
+        outs = []
+        for b, r, src, zd in zip(self.bases, res, self.srcs, self.zdev):
+            fc = FitzCandidates(r.zchi2, r.penalty if b.oii is not None else None, zd, self.K,
+                                self.nfine)
+            c2, _, pen = run_pairs_device(rowpack, src, fc.pair_t, fc.pair_z, self.status)
+            outs.append((r, fc, c2, pen))
+        return outs
+
+    def run(self):
+        import torch
+        if self.graph is not None:
+            self.graph.replay()
+            outs = self.outs
+        else:
+            outs = self._body(self.dbatch, self.rowpack)
+        torch.cuda.synchronize()
+        self.status.check("zfind device plan")
+        results = {t.id: {} for t in self.local}
+        pres = []
+        for t, b, (r, fc, c2, pen) in zip(self.templates, self.bases, outs):
+            ft = t.template.full_type
+            zc, co, pe = r.zchi2.cpu().numpy(), r.zcoeff.cpu().numpy(), r.penalty.cpu().numpy()
+            for i, tg in enumerate(self.local):
+                results[tg.id][ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i],
+                                          penalty=pe[i], zcoeff=co[i])
+            T = len(self.local)
+            shape = (T, self.K, self.nfine)
+            c2h = c2.cpu().numpy().reshape(shape)
+            if b.oii is not None:
+                c2h = c2h + pen.cpu().numpy().reshape(shape)
+            pres.append(_fitz.PrecomputedFine(fc.cand.cpu().numpy(), fc.count.cpu().numpy(),
+                                              fc.tie.cpu().numpy(),
+                                              fc.pair_z.cpu().numpy().reshape(shape), c2h))
+        return results, pres
+
+
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
-          n_nearest=None, prior_sigma=None, ncamera=None, refine="parabola"):
+          n_nearest=None, prior_sigma=None, ncamera=None, refine="parabola", graph=False):
     if priors is not None and not hasattr(priors, 'eval'):
         from .priors import Priors
         priors = Priors(priors)
     comm = targets.comm
-    if chi2_scan is None:
+    local = list(targets.local())
+    # wavegrids() is collective when the targets have a communicator: every
+    # rank calls it, with or without local targets
+    dwave = targets.wavegrids()
+    layout = GridLayout.from_dwave(dwave) if local else None
+    pres = None
+    if graph and chi2_scan is None and priors is None and local \
+            and not archetypes \
+            and all(solve_code(t.template) == _lib.RR_SOLVE_PCA for t in templates):
+        # scan, candidates and fine grids on the device in one graph
+        nfine = 15 if zminfit_npoints is None else zminfit_npoints
+        plan = DeviceFitzPlan(local, templates, layout, nminima=nminima, nfine=nfine)
+        results, plist = plan.run()
+        pres = {t.template.full_type: p for t, p in zip(templates, plist)}
+    elif chi2_scan is None:
         results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
     else:
         # the coarse scans of a details file (zfind.py:298-301)
@@ -236,13 +355,8 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
         for tg in results.keys():
             for ft in results[tg].keys():
                 results[tg][ft]['zchi2'] += priors.eval(tg, results[tg][ft]['redshifts'])
-    local = list(targets.local())
     # the targets' packed rows for the fine-grid pair scans do not depend on
     # the template: pack them once for every template's refinement
-    # wavegrids() is collective when the targets have a communicator: every
-    # rank calls it, with or without local targets
-    dwave = targets.wavegrids()
-    layout = GridLayout.from_dwave(dwave) if local else None
     rowpack = RowPack.from_targets(local, layout) if local else None
     sort = np.array([t.template.full_type for t in templates]).argsort()
     arch = None
@@ -262,7 +376,7 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
                                   deg_legendre=deg_legendre, zminfit_npoints=zminfit_npoints,
                                   per_camera=per_camera, n_nearest=n_nearest,
                                   prior_sigma=prior_sigma, layout=layout, rowpack=rowpack,
-                                  refine=refine)
+                                  refine=refine, pre=None if pres is None else pres.get(ft))
         for tg, zf in zip(local, fits):
             results[tg.id][ft]['zfit'] = zf
     for tg in local:

@@ -149,11 +149,88 @@ def test_zfind_newton_refinement(golden):
     np.testing.assert_array_equal(new["targetid"], par["targetid"])
     best = new["znum"] == 0
     np.testing.assert_array_equal(new["spectype"][best], par["spectype"][best])
-    good = (new["zwarn"] == 0) & (par["zwarn"] == 0) & (new["spectype"] == par["spectype"])
-    assert good.sum() >= 5
-    for st, step in (("GALAXY", 23 * 3e-4), ("QSO", 31 * 5e-4), ("STAR", 4 * 4e-5)):
-        m = good & (new["spectype"] == st)
+    # rows are ranked by chi2, which the two refinements give slightly
+    # differently: match each good Newton minimum to the parabola minima of
+    # the same target and spectral type
+    steps = {"GALAXY": 23 * 3e-4, "QSO": 31 * 5e-4, "STAR": 4 * 4e-5}
+    good = np.nonzero(new["zwarn"] == 0)[0]
+    assert len(good) >= 5
+    for r in good:
+        same = (par["targetid"] == new["targetid"][r]) & (par["spectype"] == new["spectype"][r])
+        dz = np.abs(np.log1p(par["z"][same]) - np.log1p(new["z"][r]))
         # a fine-grid step: the 15-point grid spans two coarse steps
-        assert np.all(np.abs(np.log1p(new["z"][m]) - np.log1p(par["z"][m])) <= step * 2 / 14
-                      + 1e-12)
-    assert np.all(new["zerr"][good] > 0)
+        assert dz.min() <= steps[new["spectype"][r]] * 2 / 14 + 1e-12
+        assert new["zerr"][r] > 0
+
+
+def test_fitz_candidates_kernel_vs_find_minima():
+    """rr_fitz_candidates against find_minima + np.linspace on rows with
+    plateaus, edge minima, exact ties and a constant (all-masked) row:
+    identical candidates and grids where the order is determined, the tie
+    flag where numpy's unstable sort decides it."""
+    import torch
+    from redrock_b200.engine import FitzCandidates
+    from redrock_b200.fitz import find_minima
+    rng = np.random.default_rng(3)
+    nz, K, nfine = 200, 5, 15
+    z = np.sort(rng.uniform(0.0, 2.0, nz))
+    rows = [rng.uniform(0, 100, nz) for _ in range(20)]
+    r = rng.uniform(0, 100, nz)
+    r[0] = -1.0                      # edge minimum
+    rows.append(r)
+    r = np.round(rng.uniform(0, 5, nz))   # many exact ties
+    rows.append(r)
+    rows.append(np.full(nz, 9999999.0))   # HUGE_CHI2 row
+    r = np.linspace(10, 0, nz)       # monotone: only the last index
+    rows.append(r)
+    zc = np.stack(rows)
+    pen = np.where(rng.uniform(size=zc.shape) < 0.1, rng.uniform(0, 3, zc.shape), 0.0)
+    pen[-1] = 0.0
+    fc = FitzCandidates(torch.tensor(zc, device="cuda"), torch.tensor(pen, device="cuda"),
+                        torch.tensor(z, device="cuda"), K, nfine)
+    torch.cuda.synchronize()
+    cand, count, tie = fc.cand.cpu().numpy(), fc.count.cpu().numpy(), fc.tie.cpu().numpy()
+    pz = fc.pair_z.cpu().numpy().reshape(len(rows), K, nfine)
+    for j in range(len(rows)):
+        eff = zc[j] + pen[j]
+        ref = find_minima(eff)
+        assert count[j] == min(K, len(ref))
+        vals = eff[ref[:count[j] + 1]]
+        determined = len(np.unique(vals)) == len(vals)
+        if not determined:
+            assert tie[j] == 1
+            continue
+        assert tie[j] == 0
+        np.testing.assert_array_equal(cand[j, :count[j]], ref[:count[j]])
+        for k, im in enumerate(ref[:count[j]]):
+            lo, hi = z[max(0, im - 1)], z[min(im + 1, nz - 1)]
+            np.testing.assert_array_equal(pz[j, k], np.linspace(lo, hi, nfine))
+    assert tie[len(rows) - 2] == 1 and count[-1] == 1
+
+
+def test_zfind_graph_equals_eager():
+    """zfind(graph=True) -- scan, candidates and fine-grid scans of the whole
+    batch captured as one CUDA graph -- gives the eager zfind's table bit
+    for bit, with masked, dropped-camera and all-masked targets in two
+    target blocks."""
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.zfind import zfind
+    tg = synth.make_targets(40, seed=47, amp=1.5, mask_range=(0.0, 0.4), drop_camera_frac=0.15,
+                            first_id=9000)
+    for s in tg[7].spectra:
+        s.ivar[:] = 0.0
+    dz = T.DistTargetsCopy(T.from_synth(tg))
+    sel = {"GALAXY": 11, "QSO": 13, "STAR:::K": 2, "STAR:::A": 2}
+    dts = []
+    for ts in synth.template_set():
+        if ts.full_type in sel:
+            ts.redshifts = ts.redshifts[::sel[ts.full_type]]
+            dts.append(TM.DistTemplate(TM.from_synth(ts), dz.wavegrids()))
+    res_e, eager = zfind(dz, dts, nminima=3)
+    res_g, graph = zfind(dz, dts, nminima=3, graph=True)
+    assert list(graph.keys()) == list(eager.keys())
+    for k in eager:
+        np.testing.assert_array_equal(graph[k], eager[k], err_msg=k)
+    for tid in res_e:
+        for ft in res_e[tid]:
+            np.testing.assert_array_equal(res_g[tid][ft]["zchi2"], res_e[tid][ft]["zchi2"])
