@@ -336,6 +336,7 @@ def run_ours(args, rank, world, local_rank):
 
     study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
     adj = adjoint_study(rtg, tms, torch) if (args.adjoint and rank == 0) else None
+    zst = zfind_study(rtg, tms, torch) if (args.zfind and rank == 0) else None
     arc = archetype_study(tg, rtg, torch) if (args.archetypes and rank == 0) else None
 
     # ---- end to end through the public API, host buffers ------------------
@@ -456,9 +457,71 @@ def run_ours(args, rank, world, local_rank):
         out["ygemm_study"] = study
     if adj is not None:
         out["adjoint"] = adj
+    if zst is not None:
+        out["zfind"] = zst
     if arc is not None:
         out["archetypes"] = arc
     return out
+
+
+def zfind_study(rtg, tms, torch, ntarget=500):
+    """zfind on the first ntarget targets of the workload against all 7
+    templates (3 minima each, config 2's 500 x 7 x 3): wall time of the
+    eager path, of the CUDA-graph path (scan + candidates + fine grids as one
+    graph) and of batched Newton refinement; and, for every target's best
+    GALAXY minimum with ZWARN 0, the distance of the parabola and Newton
+    redshifts to the minimum of a dense FP64 scan (401 points spanning two
+    fine-grid steps around it, rr_zscan_pairs)."""
+    from redrock_b200 import targets as T, templates as TM
+    from redrock_b200.engine import RowPack, TemplateSource, run_pairs
+    from redrock_b200.zfind import zfind
+    sub = rtg[:ntarget]
+    dz = T.DistTargetsCopy(sub)
+    dts = [TM.DistTemplate(tm, dz.wavegrids()) for tm in tms]
+
+    def timed(**kw):
+        with contextlib.redirect_stdout(sys.stderr):
+            zfind(dz, dts, nminima=3, **kw)     # warm-up (autotuner, graph set-up)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = zfind(dz, dts, nminima=3, **kw)
+            torch.cuda.synchronize()
+        return time.perf_counter() - t0, out[1]
+    t_eager, par = timed()
+    t_graph, gra = timed(graph=True)
+    t_newton, new = timed(refine="newton")
+    same = all(np.array_equal(np.asarray(gra[k]), np.asarray(par[k])) for k in par)
+    # dense FP64 scans around each target's best GALAXY minimum
+    gal = tms[0]
+    src = TemplateSource.from_template(gal)
+    rows = RowPack.from_targets(sub, dts[0].basis.layout)
+    zgrid = np.asarray(gal.redshifts)
+    fine = 2.0 * np.median(np.diff(np.log1p(zgrid))) / 14
+    err_p, err_n = [], []
+    idx = {t.id: i for i, t in enumerate(sub)}
+    for tab, errs in ((par, err_p), (new, err_n)):
+        m = (tab["znum"] == 0) & (tab["spectype"] == "GALAXY") & (tab["zwarn"] == 0)
+        tids = tab["targetid"][m]
+        zs = tab["z"][m]
+        if len(zs) == 0:
+            continue
+        off = np.linspace(-fine, fine, 401)
+        zd = (np.exp(np.log1p(zs)[:, None] + off[None, :]) - 1.0)
+        pt = np.repeat([idx[t] for t in tids], 401).astype(np.int32)
+        c2, _, pen = run_pairs(rows, src, pt, zd.ravel())
+        c2 = (c2 + pen).cpu().numpy().reshape(len(zs), 401)
+        zbest = zd[np.arange(len(zs)), np.argmin(c2, axis=1)]
+        errs.extend(np.abs(np.log1p(zs) - np.log1p(zbest)).tolist())
+    return {"targets": len(sub), "templates": len(tms), "nminima": 3,
+            "eager_s": t_eager, "graph_s": t_graph, "newton_s": t_newton,
+            "graph_equals_eager": bool(same),
+            "dense_grid_check": {
+                "cases": len(err_n), "grid": "401 points over +-1 fine-grid step (FP64)",
+                "max_dlnz_parabola": float(max(err_p)) if err_p else None,
+                "max_dlnz_newton": float(max(err_n)) if err_n else None,
+                "median_dlnz_parabola": float(np.median(err_p)) if err_p else None,
+                "median_dlnz_newton": float(np.median(err_n)) if err_n else None,
+                "dense_grid_step_dlnz": float(2 * fine / 400)}}
 
 
 def adjoint_study(rtg, tms, torch):
@@ -801,6 +864,9 @@ def main():
                     help="also time batched archetype refits of every target (24 archetypes)")
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the adjoint pair kernel on 3 redshifts per target and template")
+    ap.add_argument("--zfind", action="store_true",
+                    help="also time zfind (eager, CUDA graph, Newton) on 500 targets and check "
+                         "the refined redshifts against dense FP64 scans")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="use the default tile shapes instead of timing them before the run")
     ap.add_argument("--ygemm-study", action="store_true",
