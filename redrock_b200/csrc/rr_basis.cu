@@ -9,11 +9,10 @@
 //   CaluraKamble        igm.py:321-364
 //   DistTemplate        templates.py:584-597 (rebin, then data *= T)
 //
-// Design: one thread per (z, kBasisPix consecutive output bins) computes
-// every basis of those bins.  The first input sample beyond the first bin's
-// lower edge is found by binary search on the redshifted grid, and the
-// thread walks forward from it for its next bins (the reference walks the
-// grid sequentially; all land on the first j with x[j](1+z) > edge).  All arithmetic of the rebin
+// Design: one thread per (z, output bin) computes every basis of that bin.
+// The first input sample beyond the bin's lower edge is found by binary
+// search on the redshifted grid (the reference walks it sequentially; both
+// land on the first j with x[j](1+z) > edge).  All arithmetic of the rebin
 // uses explicitly rounded operations in the reference's order, so results
 // are bit-identical to redrock's CPU path.  The IGM factor of the bin's
 // centre wavelength is computed in the same thread and multiplied in.
@@ -53,8 +52,6 @@ __global__ void trapz_rebin_kernel(const double* __restrict__ x, int64_t nx,
 // Threads cover the padded pixel range [pix_offset - 5, pix_offset +
 // npix_pad + 5); pixels outside [pix_offset, pix_offset + npix) and basis
 // columns >= nb are written as 0 so the scan's halo reads see zeros.
-constexpr int kBasisPix = 4;  // consecutive output bins per thread
-
 __global__ void build_basis_kernel(const double* __restrict__ x, int64_t nx,
                                    const double* __restrict__ y, int nb,
                                    const double* __restrict__ z, int64_t nz,
@@ -64,35 +61,29 @@ __global__ void build_basis_kernel(const double* __restrict__ x, int64_t nx,
                                    double* __restrict__ basis, int64_t pix_stride,
                                    int basis_stride, int* status) {
   const int64_t span = npix_pad + 2 * kHalfBand;
-  const int64_t i0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * kBasisPix;
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // 0..span-1
   const int64_t iz = blockIdx.y;
-  if (i0 >= span || iz >= nz) return;
+  if (i >= span || iz >= nz) return;
+  const int64_t ipix = i - kHalfBand;  // pixel index within the grid
+  double* o = basis + (iz * pix_stride + pix_offset + ipix) * basis_stride;
+  if (ipix < 0 || ipix >= npix) {
+    for (int b = 0; b < basis_stride; ++b) o[b] = 0.0;
+    return;
+  }
   const double zz = z[iz];
   const double zp1 = dadd(1.0, zz);
-  int64_t cursor = -1;
-  for (int q = 0; q < kBasisPix; ++q) {
-    const int64_t i = i0 + q;  // 0..span-1
-    if (i >= span) break;
-    const int64_t ipix = i - kHalfBand;  // pixel index within the grid
-    double* o = basis + (iz * pix_stride + pix_offset + ipix) * basis_stride;
-    if (ipix < 0 || ipix >= npix) {
-      for (int b = 0; b < basis_stride; ++b) o[b] = 0.0;
-      continue;
-    }
-    double res[kMaxRebinBasis];
-    if (!rebin_bin(x, nx, y, nb, zp1, edges[ipix], edges[ipix + 1], res, &cursor)) {
-      set_status(status, RR_ERANGE);
-      for (int b = 0; b < basis_stride; ++b) o[b] = nan("");
-      cursor = -1;
-      continue;
-    }
-    if (apply_igm) {
-      const double t = transmission(igm_model, zz, wave[ipix]);
-      for (int b = 0; b < nb; ++b) res[b] = dmul(res[b], t);
-    }
-    for (int b = 0; b < nb; ++b) o[b] = res[b];
-    for (int b = nb; b < basis_stride; ++b) o[b] = 0.0;
+  double res[kMaxRebinBasis];
+  if (!rebin_bin(x, nx, y, nb, zp1, edges[ipix], edges[ipix + 1], res)) {
+    set_status(status, RR_ERANGE);
+    for (int b = 0; b < basis_stride; ++b) o[b] = nan("");
+    return;
   }
+  if (apply_igm) {
+    const double t = transmission(igm_model, zz, wave[ipix]);
+    for (int b = 0; b < nb; ++b) res[b] = dmul(res[b], t);
+  }
+  for (int b = 0; b < nb; ++b) o[b] = res[b];
+  for (int b = nb; b < basis_stride; ++b) o[b] = 0.0;
 }
 
 }  // namespace rr
@@ -155,9 +146,8 @@ extern "C" int rr_build_basis(const double* x, int64_t nx, const double* y, int6
   for (int g = 0; g < ngrid; ++g) {
     const rr_grid_desc& gd = grids[g];
     const int64_t span = gd.npix_pad + 2 * kHalfBand;
-    const int64_t nthr = (span + kBasisPix - 1) / kBasisPix;
     dim3 block(128);
-    dim3 grid((unsigned)((nthr + block.x - 1) / block.x), (unsigned)nz);
+    dim3 grid((unsigned)((span + block.x - 1) / block.x), (unsigned)nz);
     build_basis_kernel<<<grid, block, 0, (cudaStream_t)stream>>>(
         x, nx, y, (int)nbasis, z, nz, gd.edges, gd.wave, gd.npix, gd.npix_pad, gd.pix_offset,
         igm_model, gd.apply_igm && igm_model != RR_IGM_NONE, basis, pix_stride, basis_stride,

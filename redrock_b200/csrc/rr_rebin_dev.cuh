@@ -216,32 +216,19 @@ constexpr int kMaxRebinBasis = 16;
 // where y(e) is the redshifted interpolant at the bin edges -- the edge
 // values the trapezoid sum already forms.  (T itself is unchanged, bit for
 // bit, by the extra output.)
-//
-// cursor (optional): the first-sample index of an earlier bin of the same
-// redshift with a lower edge <= e_lo (or < 0 for none).  The first j with
-// x[j] (1+z) > e_lo is then found by walking forward from it instead of by
-// binary search -- the same j either way -- and the cursor is updated.
 template <bool DZ = false>
 __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, int64_t nx,
                                                   const double* __restrict__ y, int64_t ystride,
                                                   int nb, double zp1, double e_lo, double e_hi,
-                                                  double* res, double* dres = nullptr,
-                                                  int64_t* cursor = nullptr) {
+                                                  double* res, double* dres = nullptr) {
   double ylo_e[DZ ? kMaxRebinBasis : 1], yhi_e[DZ ? kMaxRebinBasis : 1];
   // first j with x[j] (1+z) > e_lo
-  int64_t j;
-  if (cursor && *cursor >= 0) {
-    j = *cursor;
-    while (j < nx && dmul(x[j], zp1) <= e_lo) ++j;
-  } else {
-    int64_t lo = 0, hi = nx;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (dmul(x[mid], zp1) <= e_lo) lo = mid + 1; else hi = mid;
-    }
-    j = lo;
+  int64_t lo = 0, hi = nx;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (dmul(x[mid], zp1) <= e_lo) lo = mid + 1; else hi = mid;
   }
-  if (cursor) *cursor = j;
+  int64_t j = lo;
   if (j < 1 || j >= nx) return false;
   double xj = dmul(x[j], zp1);
   const double xjm1 = dmul(x[j - 1], zp1);
@@ -302,9 +289,8 @@ __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, 
 
 __device__ __forceinline__ bool rebin_bin(const double* __restrict__ x, int64_t nx,
                                           const double* __restrict__ y, int nb, double zp1,
-                                          double e_lo, double e_hi, double* res,
-                                          int64_t* cursor = nullptr) {
-  return rebin_bin_strided(x, nx, y, nx, nb, zp1, e_lo, e_hi, res, nullptr, cursor);
+                                          double e_lo, double e_hi, double* res) {
+  return rebin_bin_strided(x, nx, y, nx, nb, zp1, e_lo, e_hi, res);
 }
 
 }  // namespace rr
