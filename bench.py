@@ -232,7 +232,10 @@ def run_ours(args, rank, world, local_rank):
 
     tiles = None
     tuned = None
-    if args.autotune:
+    if args.tiles:
+        # a fixed tile choice (e.g. the one an earlier run's autotuner made)
+        tiles = {(int(k) if k.isdigit() else k): int(v) for k, v in json.loads(args.tiles).items()}
+    elif args.autotune:
         # tile shapes picked by the autotuner before anything is timed
         from redrock_b200 import autotune
         bases0 = [DeviceBasis.build(s, layout, status=st) for s in srcs]
@@ -267,9 +270,8 @@ def run_ours(args, rank, world, local_rank):
         # nodes, so every replay re-times the scan stage and the fused
         # launches (the values read after the timed region are the last
         # replay's)
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            step(True, external=True)
+        from redrock_b200.device import capture_graph
+        graph, _ = capture_graph(lambda: step(True, external=True))
         graph.replay()
         torch.cuda.synchronize()
         st.check("graph replay")
@@ -434,7 +436,7 @@ def run_ours(args, rank, world, local_rank):
                             "chosen_by": ("autotuner (kernel time per candidate, ms: "
                                           + str({k: v for k, v in tuned.items()
                                                  if not isinstance(k, int)}) + ")")
-                            if tuned else "defaults"}},
+                            if tuned else ("--tiles" if args.tiles else "defaults")}},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(args.workload,
                                                                   bool(args.ntargets or args.zsub)),
@@ -511,17 +513,21 @@ def zfind_study(rtg, tms, torch, ntarget=500):
         c2, _, pen = run_pairs(rows, src, pt, zd.ravel())
         c2 = (c2 + pen).cpu().numpy().reshape(len(zs), 401)
         zbest = zd[np.arange(len(zs)), np.argmin(c2, axis=1)]
-        errs.extend(np.abs(np.log1p(zs) - np.log1p(zbest)).tolist())
+        # (|dln(1+z)| to the dense minimum, chi2 at the reported z minus the
+        # dense minimum's chi2)
+        errs.extend(zip(np.abs(np.log1p(zs) - np.log1p(zbest)).tolist(),
+                        (c2[:, 200] - c2.min(axis=1)).tolist()))
     return {"targets": len(sub), "templates": len(tms), "nminima": 3,
             "eager_s": t_eager, "graph_s": t_graph, "newton_s": t_newton,
             "graph_equals_eager": bool(same),
-            "dense_grid_check": {
-                "cases": len(err_n), "grid": "401 points over +-1 fine-grid step (FP64)",
-                "max_dlnz_parabola": float(max(err_p)) if err_p else None,
-                "max_dlnz_newton": float(max(err_n)) if err_n else None,
-                "median_dlnz_parabola": float(np.median(err_p)) if err_p else None,
-                "median_dlnz_newton": float(np.median(err_n)) if err_n else None,
-                "dense_grid_step_dlnz": float(2 * fine / 400)}}
+            "dense_grid_check": dict(
+                cases=len(err_n), grid="401 points over +-1 fine-grid step (FP64)",
+                dense_grid_step_dlnz=float(2 * fine / 400),
+                **{f"{k}_{name}": (float(f(np.asarray(e)[:, col])) if e else None)
+                   for name, e in (("parabola", err_p), ("newton", err_n))
+                   for k, f, col in (("max_dlnz", np.max, 0), ("median_dlnz", np.median, 0),
+                                     ("max_dchi2_over_dense_min", np.max, 1),
+                                     ("median_dchi2_over_dense_min", np.median, 1))})}
 
 
 def adjoint_study(rtg, tms, torch):
@@ -867,6 +873,9 @@ def main():
     ap.add_argument("--zfind", action="store_true",
                     help="also time zfind (eager, CUDA graph, Newton) on 500 targets and check "
                          "the refined redshifts against dense FP64 scans")
+    ap.add_argument("--tiles", default=None,
+                    help='fixed tile choice as JSON, e.g. \'{"4": 3, "5": 2, "block_group": 4}\' '
+                         "(skips the autotuner)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="use the default tile shapes instead of timing them before the run")
     ap.add_argument("--ygemm-study", action="store_true",

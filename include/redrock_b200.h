@@ -233,11 +233,17 @@ int rr_zscan_fused(const rr_scan_targets* targets, const rr_scan_template* templ
 /* Tile shape of the fused scan: a tile is 32 targets (one per lane) x 8 ZT
  * redshifts (ZT per thread, 8 warps) x 24-pixel stages.  nbasis 10 and the
  * uncommon sizes run at ZT = 1; nbasis 4 may run at ZT = 1-3 and nbasis 5
- * at ZT = 1-2 (0 = the default, 2).  rr_zscan_fused uses the defaults; the
- * host autotuner (redrock_b200/autotune.py) times the choices. */
+ * at ZT = 1-2 (0 = the default, 2).  block_group sets the order in which
+ * the persistent CTAs take tiles: 0 = target blocks fastest (tiles running
+ * at one time share basis windows); G > 0 = all redshift tiles of G target
+ * blocks before the next G (their packed rows are reused while in L2).
+ * Results do not depend on either choice.  rr_zscan_fused uses the
+ * defaults; the host autotuner (redrock_b200/autotune.py) times the
+ * choices. */
 typedef struct {
   int32_t zt_nbasis4;
   int32_t zt_nbasis5;
+  int32_t block_group;
 } rr_scan_options;
 
 int rr_zscan_fused_opt(const rr_scan_targets* targets, const rr_scan_template* templates,

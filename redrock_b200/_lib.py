@@ -72,7 +72,7 @@ class CoaddGroup(ctypes.Structure):
 
 
 class ScanOptions(ctypes.Structure):
-    _fields_ = [("zt_nbasis4", c_int32), ("zt_nbasis5", c_int32)]
+    _fields_ = [("zt_nbasis4", c_int32), ("zt_nbasis5", c_int32), ("block_group", c_int32)]
 
 
 class ScanTargets(ctypes.Structure):

@@ -61,6 +61,8 @@ struct FusedParams {
   int64_t tile_start[RR_MAX_TEMPLATES + 1];
   int64_t chunks_total;  // pixel chunks per block (over all segments)
   int max_stride;        // largest basis_stride
+  int block_group;       // tile order: 0 = target blocks fastest; G > 0 = all z tiles of
+                         // G blocks before the next G (their packed rows stay in L2)
   int* tile_counter;
   int* resweep_counter;  // [0] tiles swept a second time for the direct residual,
                          // [1] (target, z) lanes re-evaluated there
@@ -347,6 +349,34 @@ __device__ void scan_tile(const FusedParams& p, const rr_scan_template& tm, int 
   }
 }
 
+// (block, z tile) of tile `local` of a template with nzt z tiles.  G <= 0
+// (or >= nblock): target blocks fastest, so the tiles running at one time
+// share z tiles (basis windows) across blocks.  G > 0: the blocks form
+// groups of G; all z tiles of one group come before the next group, blocks
+// fastest within it, so a group's packed rows are reused by many z tiles
+// while they sit in L2 (the last group may be smaller).
+__device__ __forceinline__ void tile_coords(int64_t local, int64_t nzt, int nblock, int G,
+                                            int& block, int64_t& zt) {
+  if (G <= 0 || G >= nblock) {
+    block = (int)(local % nblock);
+    zt = local / nblock;
+    return;
+  }
+  const int64_t full = nblock / G;
+  const int64_t per = (int64_t)G * nzt;
+  const int64_t g = local / per;
+  if (g < full) {
+    const int64_t r = local - g * per;
+    block = (int)(g * G + r % G);
+    zt = r / G;
+  } else {
+    const int gr = nblock - (int)full * G;
+    const int64_t r = local - full * per;
+    block = (int)(full * G + r % gr);
+    zt = r / gr;
+  }
+}
+
 // Launch groups of the fused kernel, one instantiation per (group,
 // redshifts per thread ZT), so a group's register allocation does not
 // depend on the others: nbasis 10 (GALAXY; ZT 1), 4 (QSO; ZT 1-3), 5
@@ -390,8 +420,11 @@ __global__ void __launch_bounds__(kThreads, (kWarps <= 4 ? 2 : 1)) zscan_fused_k
     while (t + 1 < p.ntemplate && tile >= p.tile_start[t + 1]) ++t;
     const rr_scan_template& tm = p.tm[t];
     const int64_t local = tile - p.tile_start[t];
-    const int block = (int)(local % p.tg.nblock);
-    const int z0 = (int)(local / p.tg.nblock) * kWarps * ZT;
+    const int64_t nzt = (p.tile_start[t + 1] - p.tile_start[t]) / p.tg.nblock;
+    int block;
+    int64_t ztile;
+    tile_coords(local, nzt, p.tg.nblock, p.block_group, block, ztile);
+    const int z0 = (int)ztile * kWarps * ZT;
 #define RR_TILE_CASE(N)                                                   \
   case N:                                                                 \
     if constexpr (group_of(N) == GROUP) {                                 \
@@ -428,8 +461,8 @@ inline size_t fused_smem_bytes(int max_stride, int zt) {
 // independent of these).
 template <int GROUP, bool EXTY, int ZT>
 int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templates,
-                        const int* pick, int npick, int* counter, int* resweep, int* status,
-                        bool overlap, cudaStream_t stream) {
+                        const int* pick, int npick, int bgroup, int* counter, int* resweep,
+                        int* status, bool overlap, cudaStream_t stream) {
   constexpr int kZt = ZT;
   FusedParams p;
   memset(&p, 0, sizeof(p));
@@ -452,6 +485,7 @@ int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templat
     max_stride = tm.basis_stride > max_stride ? tm.basis_stride : max_stride;
   }
   p.max_stride = max_stride;
+  p.block_group = bgroup;
   p.tile_counter = counter;
   p.resweep_counter = resweep;
   p.status = status;
@@ -487,20 +521,25 @@ int launch_fused(const rr_scan_targets* targets, const rr_scan_template* templat
 
 // launch with the runtime ZT of a group (one of its compiled values)
 template <int GROUP, bool EXTY>
-int launch_group(int zt, const rr_scan_targets* targets, const rr_scan_template* templates,
-                        const int* pick, int npick, int* counter, int* resweep, int* status,
-                        bool overlap, cudaStream_t stream) {
+int launch_group(int zt, int bgroup, const rr_scan_targets* targets,
+                 const rr_scan_template* templates, const int* pick, int npick, int* counter,
+                 int* resweep, int* status, bool overlap, cudaStream_t stream) {
   if (zt < 1 || zt > kMaxZt[GROUP]) return RR_EINVAL;
   if constexpr (kMaxZt[GROUP] >= 3)
-    if (zt == 3) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 3 ? 3 : 1)>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
+    if (zt == 3)
+      return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 3 ? 3 : 1)>(
+          targets, templates, pick, npick, bgroup, counter, resweep, status, overlap, stream);
   if constexpr (kMaxZt[GROUP] >= 2)
-    if (zt == 2) return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 2 ? 2 : 1)>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
-  return launch_fused<GROUP, EXTY, 1>(targets, templates, pick, npick, counter, resweep, status, overlap, stream);
+    if (zt == 2)
+      return launch_fused<GROUP, EXTY, (kMaxZt[GROUP] >= 2 ? 2 : 1)>(
+          targets, templates, pick, npick, bgroup, counter, resweep, status, overlap, stream);
+  return launch_fused<GROUP, EXTY, 1>(targets, templates, pick, npick, bgroup, counter, resweep,
+                                      status, overlap, stream);
 }
 
 // one entry per group translation unit
 #define RR_FUSED_GROUP_DECL(G)                                                                   \
-  int fused_group_##G(bool exty, int zt, const rr_scan_targets* targets,                         \
+  int fused_group_##G(bool exty, int zt, int bgroup, const rr_scan_targets* targets,             \
                       const rr_scan_template* templates, const int* pick, int npick,             \
                       int* counter, int* resweep, int* status, bool overlap,            \
                       cudaStream_t stream);

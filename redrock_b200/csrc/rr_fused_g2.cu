@@ -3,12 +3,12 @@
 
 namespace rr {
 
-int fused_group_2(bool exty, int zt, const rr_scan_targets* targets,
+int fused_group_2(bool exty, int zt, int bgroup, const rr_scan_targets* targets,
                    const rr_scan_template* templates, const int* pick, int npick, int* counter,
                    int* resweep, int* status, bool overlap, cudaStream_t stream) {
-  return exty ? launch_group<2, true>(zt, targets, templates, pick, npick, counter, resweep,
+  return exty ? launch_group<2, true>(zt, bgroup, targets, templates, pick, npick, counter, resweep,
                                         status, overlap, stream)
-              : launch_group<2, false>(zt, targets, templates, pick, npick, counter, resweep,
+              : launch_group<2, false>(zt, bgroup, targets, templates, pick, npick, counter, resweep,
                                          status, overlap, stream);
 }
 

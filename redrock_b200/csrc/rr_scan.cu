@@ -391,7 +391,10 @@ static int zscan_fused(const rr_scan_targets* targets, const rr_scan_template* t
   if (rw_end > targets->npix_block) return RR_EINVAL;
   int zt[kNGroups];
   for (int g = 0; g < kNGroups; ++g) zt[g] = kDefaultZt[g];
+  int bgroup = 0;
   if (opt) {
+    if (opt->block_group < 0) return RR_EINVAL;
+    bgroup = opt->block_group;
     if (opt->zt_nbasis4 < 0 || opt->zt_nbasis4 > kMaxZt[1] || opt->zt_nbasis5 < 0 ||
         opt->zt_nbasis5 > kMaxZt[2])
       return RR_EINVAL;
@@ -422,16 +425,25 @@ static int zscan_fused(const rr_scan_targets* targets, const rr_scan_template* t
   // (tile_counter[4 + g] hands out the tiles of launch g)
   RR_CUDA_TRY(cudaMemsetAsync(tile_counter, 0, RR_FUSED_COUNTERS * sizeof(int), st));
   int* resweep = tile_counter + 2;
+  // Invariant of the programmatic dependent launches below: the group
+  // launches are independent of one another -- each reads only the packed
+  // targets, its own bases and y, all written before the first launch, and
+  // writes only its own templates' outputs and its own tile counter (the
+  // re-sweep counters are atomics).  That is why a dependent launch may
+  // start before its predecessor finishes, and why each CTA can leave its
+  // griddepcontrol.wait to the very end (it only orders completion for the
+  // work after the last launch).  A change that makes one group read what
+  // another writes must move that wait ahead of the read.
   int rc = RR_OK;
   bool overlap = false;
-  typedef int (*group_fn)(bool, int, const rr_scan_targets*, const rr_scan_template*, const int*,
-                          int, int*, int*, int*, bool, cudaStream_t);
+  typedef int (*group_fn)(bool, int, int, const rr_scan_targets*, const rr_scan_template*,
+                          const int*, int, int*, int*, int*, bool, cudaStream_t);
   const group_fn fns[kNGroups] = {fused_group_0, fused_group_1, fused_group_2, fused_group_3};
   for (int gi = 0; gi < 2 * kNGroups && !rc; ++gi) {
     if (!ng[gi]) continue;
     const int g = gi % kNGroups;
-    rc = fns[g](gi >= kNGroups, zt[g], targets, templates, group[gi], ng[gi], tile_counter + 4 + gi,
-                resweep, status, overlap, st);
+    rc = fns[g](gi >= kNGroups, zt[g], bgroup, targets, templates, group[gi], ng[gi],
+                tile_counter + 4 + gi, resweep, status, overlap, st);
     overlap = true;
   }
   return rc;

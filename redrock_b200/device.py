@@ -49,6 +49,26 @@ def to_device(a, dtype=torch.float64, dev=None):
     return t.to(dev, non_blocking=True)
 
 
+def capture_graph(fn):
+    """Capture fn()'s launches as a CUDA graph on a side stream and return
+    (graph, fn's result).  Unlike torch.cuda.graph, this leaves torch's
+    device and pinned-host caches alone (no empty_cache before the capture),
+    so pinned buffers and cached blocks stay warm for the work around the
+    graph; allocations inside fn come from the graph's private pool and
+    live as long as the graph."""
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        g.capture_begin()
+        try:
+            out = fn()
+        finally:
+            g.capture_end()
+    torch.cuda.current_stream().wait_stream(side)
+    return g, out
+
+
 def to_numpy(t):
     if isinstance(t, torch.Tensor):
         return t.detach().cpu().numpy()

@@ -512,8 +512,8 @@ def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=N
     "fp64", y is computed on the tensor cores first (YGemm).  kernel_events:
     a list that gets a (start, end) CUDA event pair around the scan launches
     alone (timing).  tiles: redshifts per thread {nbasis: ZT} for the small
-    bases (nbasis 4: 1-3, nbasis 5: 1-2; rr_scan_options), else the
-    defaults."""
+    bases (nbasis 4: 1-3, nbasis 5: 1-2; rr_scan_options) and optionally
+    "block_group" (the tile order), else the defaults."""
     L = _lib.lib()
     dev = device()
     results = [ScanResult(pack.ntarget, b, dev) for b in bases]
@@ -545,7 +545,8 @@ def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=N
             e1 = torch.cuda.Event(enable_timing=True, external=external_events)
             _record(e0, stream)
         if tiles:
-            opt = _lib.ScanOptions(int(tiles.get(4, 0)), int(tiles.get(5, 0)))
+            opt = _lib.ScanOptions(int(tiles.get(4, 0)), int(tiles.get(5, 0)),
+                                   int(tiles.get("block_group", 0)))
             rc = L.rr_zscan_fused_opt(ctypes.byref(tgs), arr, len(tms), ptr(counter),
                                       ctypes.byref(opt), st.ptr, stream_handle(stream))
         else:

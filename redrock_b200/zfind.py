@@ -276,12 +276,10 @@ class DeviceFitzPlan:
         torch.cuda.synchronize()
         self.status.check("zfind warm-up")
         self.graph = None
+        self.outs = None
         if graph:
-            self.graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.graph):
-                self.outs = self._body(self.dbatch, self.rowpack)
-        else:
-            self.outs = None
+            from .device import capture_graph
+            self.graph, self.outs = capture_graph(lambda: self._body(self.dbatch, self.rowpack))
 
     def _body(self, dbatch, rowpack):
         from .engine import FitzCandidates, TargetPack, run_fused, run_pairs_device

@@ -415,7 +415,7 @@ def test_tile_shapes_bit_identical_and_autotuner(rr):
     pack = TargetPack(TargetBatch(tg, layout).to_device())
     ref, st = run_fused(pack, bases, tiles={4: 1, 5: 1})
     st.check("zt1")
-    for tiles in ({4: 2, 5: 2}, {4: 3, 5: 1}, {4: 3, 5: 2}):
+    for tiles in ({4: 2, 5: 2}, {4: 3, 5: 1}, {4: 3, 5: 2}, {4: 1, 5: 1, "block_group": 1}):
         res, st = run_fused(pack, bases, tiles=tiles)
         st.check(str(tiles))
         for a, b in zip(ref, res):
@@ -423,4 +423,5 @@ def test_tile_shapes_bit_identical_and_autotuner(rr):
             assert torch.equal(a.penalty, b.penalty)
     best = autotune.tune(pack, bases)
     assert best[4] in (1, 2, 3) and best[5] in (1, 2)
+    assert autotune.tiles_of(best).get("block_group", 0) in autotune.BLOCK_GROUPS
     assert autotune.choice(pack, bases) is best
