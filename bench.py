@@ -440,6 +440,14 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic_from_profile(args.workload,
                                                                   bool(args.ntargets or args.zsub)),
+                     "traffic_note": (
+                         "desi500: DRAM bytes of the three group launches from a full-size "
+                         "ncu capture (profiles/zscan_fused_traffic.json)"
+                         if args.workload == "desi500" else
+                         "not scaled from a small case: the L2 reuse of packed rows depends on "
+                         "how many running tiles share a target block; small-case bytes per tile "
+                         "and the bounds for the full launch in "
+                         "profiles/zscan_fused_traffic_uneven640.md"),
                      "kernel": "zscan_fused_kernel",
                      "kernel_ms": kernel_ms, "flops_per_launch": fused_flops,
                      "flops_note": ("FP64 FLOPs of F(n,P) done by this kernel"

@@ -86,44 +86,86 @@ class Chi2Scan(torch.autograd.Function):
         return gz, gf, None, None
 
 
-def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=8, tol=1e-8):
-    """Minimise chi2(z) for each pair from z0 inside [zlo, zhi] with
-    safeguarded Newton steps (a bracket shrinks on every step that does not
-    decrease chi2).  Returns (z, chi2, coeff, dchi2_dz, d2chi2_dz2, niter)."""
-    z = np.asarray(z0, dtype=np.float64).copy()
-    lo = np.asarray(zlo, dtype=np.float64).copy()
-    hi = np.asarray(zhi, dtype=np.float64).copy()
+def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10):
+    """Minimise chi2(z) for each pair inside [zlo, zhi], starting from z0
+    (the best fine-grid point; zlo, zhi its neighbours), with Newton steps
+    on dchi2/dz = 0.  The adjoint kernel's dchi2/dz is exact, so the
+    curvature of each step comes from exact gradient differences (the
+    secant of dchi2/dz across the current bracket) rather than from the
+    kernel's envelope curvature, which leaves out the template's second
+    derivative (narrow lines make that term large).  A bracket [a, b] with
+    dchi2/dz(a) <= 0 <= dchi2/dz(b) is kept throughout; a step landing
+    outside it, or a side of the bracket kept twice in a row, falls back to
+    the Illinois (modified regula falsi) step, so every iteration shrinks
+    the bracket.  One pair-gradient launch per iteration for the pairs still
+    moving.
+
+    Returns (z, chi2, coeff, dchi2_dz, d2chi2_dz2, iterations): z is the
+    evaluated point of lowest chi2 (the root of dchi2/dz once converged),
+    d2chi2_dz2 the secant curvature of the final bracket (> 0), or the
+    kernel's curvature where no bracket formed (minimum at a bracket edge:
+    z is then that edge)."""
     t = np.asarray(pair_target, dtype=np.int32)
-    chi2, coeff, _, g, h, _ = chi2_and_grad(ctx, t, z)
-    chi2 = chi2.cpu().numpy()
-    g = g.cpu().numpy()
-    h = h.cpu().numpy()
-    coeff = coeff.cpu().numpy()
-    active = np.ones(len(z), dtype=bool)
+    n = len(t)
+    z0 = np.asarray(z0, dtype=np.float64)
+    zlo = np.asarray(zlo, dtype=np.float64)
+    zhi = np.asarray(zhi, dtype=np.float64)
+    if n == 0:
+        e = np.zeros(0)
+        return e, e.copy(), np.zeros((0, ctx.src.nbasis)), e.copy(), e.copy(), 0
+    c3, co3, _, g3, h3, _ = chi2_and_grad(ctx, np.tile(t, 3), np.concatenate([zlo, z0, zhi]))
+    c3 = c3.cpu().numpy().reshape(3, n)
+    g3 = g3.cpu().numpy().reshape(3, n)
+    h3 = h3.cpu().numpy().reshape(3, n)
+    co3 = co3.cpu().numpy().reshape(3, n, -1)
+    zs = np.stack([zlo, z0, zhi])
+    # best evaluated point so far
+    k = np.argmin(c3, axis=0)
+    cols = np.arange(n)
+    zbest, cbest, gbest, hbest = zs[k, cols], c3[k, cols], g3[k, cols], h3[k, cols]
+    cobest = co3[k, cols]
+    # bracket on the side of z0 where dchi2/dz changes sign
+    right = g3[1] < 0
+    a = np.where(right, z0, zlo)
+    b = np.where(right, zhi, z0)
+    ga = np.where(right, g3[1], g3[0])
+    gb = np.where(right, g3[2], g3[1])
+    active = (ga <= 0) & (gb >= 0) & (b > a)
+    # Illinois weights: the stored end values used for the next step (the
+    # true gradients ga, gb are kept for the curvature)
+    wa, wb = ga.copy(), gb.copy()
+    last = np.zeros(n, dtype=np.int8)    # end replaced by the last step: -1 a, +1 b
     it = 0
     for it in range(1, niter + 1):
-        # Newton step where the curvature is positive, else a gradient step
-        # to the bracket's edge; never leave the bracket
-        step = np.where(h > 0, -g / np.where(h > 0, h, 1.0), -np.sign(g) * (hi - lo) / 4)
-        zn = np.clip(z + step, lo, hi)
-        idx = np.nonzero(active & (np.abs(zn - z) > tol * (1 + np.abs(z))))[0]
+        idx = np.nonzero(active & ((b - a) > tol * (1 + np.abs(a))))[0]
         if len(idx) == 0:
             break
-        c2, co, _, gn, hn, _ = chi2_and_grad(ctx, t[idx], zn[idx])
+        ai, bi, wai, wbi = a[idx], b[idx], wa[idx], wb[idx]
+        # the Newton step from a with the secant curvature of the bracket
+        # (the regula falsi point); midpoint if it would not be inside
+        den = wbi - wai
+        zn = np.where(den > 0, ai - wai * (bi - ai) / np.where(den > 0, den, 1.0),
+                      0.5 * (ai + bi))
+        zn = np.where((zn > ai) & (zn < bi), zn, 0.5 * (ai + bi))
+        c2, co, _, gn, hn, _ = chi2_and_grad(ctx, t[idx], zn)
         c2 = c2.cpu().numpy()
-        better = c2 <= chi2[idx]
-        acc = idx[better]
-        rej = idx[~better]
-        # accepted steps move the point; rejected ones shrink the bracket
-        # towards the current point
-        z[acc] = zn[acc]
-        chi2[acc] = c2[better]
-        g[acc] = gn.cpu().numpy()[better]
-        h[acc] = hn.cpu().numpy()[better]
-        coeff[acc] = co.cpu().numpy()[better]
-        up = zn[rej] > z[rej]
-        hi[rej[up]] = zn[rej[up]]
-        lo[rej[~up]] = zn[rej[~up]]
-        active[:] = False
-        active[idx] = True
-    return z, chi2, coeff, g, h, it
+        gn = gn.cpu().numpy()
+        co = co.cpu().numpy()
+        better = c2 < cbest[idx]
+        upd = idx[better]
+        zbest[upd], cbest[upd], gbest[upd] = zn[better], c2[better], gn[better]
+        cobest[upd] = co[better]
+        # the minimum lies above zn where dchi2/dz(zn) < 0, else below;
+        # an end kept twice in a row has its stored value halved (Illinois)
+        low = gn < 0
+        la, lb = idx[low], idx[~low]
+        a[la], ga[la], wa[la] = zn[low], gn[low], gn[low]
+        wb[la] = np.where(last[la] == -1, 0.5 * wb[la], wb[la])
+        last[la] = -1
+        b[lb], gb[lb], wb[lb] = zn[~low], gn[~low], gn[~low]
+        wa[lb] = np.where(last[lb] == 1, 0.5 * wa[lb], wa[lb])
+        last[lb] = 1
+        active[idx[gn == 0]] = False
+    curv = np.where((ga <= 0) & (gb >= 0) & (b > a),
+                    (gb - ga) / np.where(b > a, b - a, 1.0), hbest)
+    return zbest, cbest, cobest, gbest, curv, it

@@ -216,6 +216,45 @@ constexpr int kMaxRebinBasis = 16;
 // where y(e) is the redshifted interpolant at the bin edges -- the edge
 // values the trapezoid sum already forms.  (T itself is unchanged, bit for
 // bit, by the extra output.)
+// First j in [0, nx) with x[j] (1+z) > e (nx if none), x increasing.  A
+// guess from the mean sample spacing and a short walk find it with two or
+// three dependent loads on the (usually uniform) template grids; a binary
+// search over what is left covers uneven grids.  Every comparison is the
+// exactly rounded x[j] (1+z) <= e, so the result is the binary search's.
+__device__ __forceinline__ int64_t first_above(const double* __restrict__ x, int64_t nx,
+                                               double zp1, double e) {
+  int64_t lo = 0, hi = nx;  // the answer lies in [lo, hi]
+  const double x0 = x[0];
+  const double t = (e / zp1 - x0) / (x[nx - 1] - x0) * (double)(nx - 1);
+  if (t > 0.0 && t < (double)(nx - 1)) {
+    const int64_t g = (int64_t)t;
+    if (dmul(x[g], zp1) <= e) {
+      lo = g + 1;
+      for (int k = 0; k < 8 && lo < hi; ++k) {
+        if (dmul(x[lo], zp1) <= e) {
+          ++lo;
+        } else {
+          hi = lo;
+        }
+      }
+    } else {
+      hi = g;
+      for (int k = 0; k < 8 && lo < hi; ++k) {
+        if (dmul(x[hi - 1], zp1) > e) {
+          --hi;
+        } else {
+          lo = hi;
+        }
+      }
+    }
+  }
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (dmul(x[mid], zp1) <= e) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
 template <bool DZ = false>
 __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, int64_t nx,
                                                   const double* __restrict__ y, int64_t ystride,
@@ -223,12 +262,7 @@ __device__ __forceinline__ bool rebin_bin_strided(const double* __restrict__ x, 
                                                   double* res, double* dres = nullptr) {
   double ylo_e[DZ ? kMaxRebinBasis : 1], yhi_e[DZ ? kMaxRebinBasis : 1];
   // first j with x[j] (1+z) > e_lo
-  int64_t lo = 0, hi = nx;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (dmul(x[mid], zp1) <= e_lo) lo = mid + 1; else hi = mid;
-  }
-  int64_t j = lo;
+  int64_t j = first_above(x, nx, zp1, e_lo);
   if (j < 1 || j >= nx) return false;
   double xj = dmul(x[j], zp1);
   const double xjm1 = dmul(x[j - 1], zp1);
