@@ -135,7 +135,13 @@ def _zfind_worker(rank, world, port, q):
         single = None
         if rank == 0:
             single = Z.zfind(DistTargetsCopy(tg), tmpls, nminima=3)[1]
-        q.put((rank, local_ids, allzfit, single, None if allres is None else sorted(allres)))
+        # one target for two ranks: rank 1 has none, and still makes every
+        # collective call
+        one = DistTargetsCopy(tg[:1], comm=comm)
+        _, zf1 = Z.zfind(one, tmpls, nminima=3)
+        n1 = None if zf1 is None else len(zf1["targetid"])
+        q.put((rank, local_ids, allzfit, single, None if allres is None else sorted(allres),
+               len(one.local_target_ids()), n1))
     finally:
         dist.destroy_process_group()
 
@@ -150,8 +156,8 @@ def test_two_rank_zfind_gathers_on_rank0():
         p.start()
     out = {}
     for _ in range(2):
-        r, ids, zf, single, keys = q.get(timeout=180)
-        out[r] = (ids, zf, single, keys)
+        r, ids, zf, single, keys, nlocal1, n1 = q.get(timeout=180)
+        out[r] = (ids, zf, single, keys, nlocal1, n1)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -163,3 +169,5 @@ def test_two_rank_zfind_gathers_on_rank0():
     assert list(zf.keys()) == list(single.keys())
     for k in zf:
         np.testing.assert_array_equal(zf[k], single[k], err_msg=k)
+    assert out[0][4] + out[1][4] == 1 and min(out[0][4], out[1][4]) == 0
+    assert out[0][5] == 6 and out[1][5] is None   # 3 minima x 2 templates
