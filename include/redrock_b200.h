@@ -308,6 +308,10 @@ int rr_zscan_pairs(const rr_pair_template* tmpl, const rr_pair_segment* segs /* 
  *                u = (R dT/dz)^T W r, v = (R T)^T W (R dT/dz c))
  *   dchi2_dflux[pair][p] = 2 w_p r_p in the packed pixel order (optional;
  *                needs sw from rr_pack_rows; not with a prior).
+ *   dpenalty_dz = -oii . dc/dz where the [OII] penalty is active, else 0
+ *                (optional), with dc/dz = (M+P)^-1 (u-v): the derivative of
+ *                the objective fitz minimises, chi2 + penalty, is
+ *                dchi2_dz + dpenalty_dz.
  * dT/dz is exact for the trapezoid rebin (from the bin-edge values of the
  * redshifted interpolant) and includes the smooth z dependence of the
  * Inoue14 Lyman-continuum optical depth; on/off switches of IGM lines with z
@@ -318,7 +322,8 @@ int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_segment* seg
                         const double* wsum, int64_t npix_row, const int32_t* pair_target,
                         const double* pair_z, int64_t npairs, double* chi2, double* coeff,
                         double* penalty, double* dchi2_dz, double* d2chi2_dz2,
-                        double* dchi2_dflux, int* status, rr_stream_t stream);
+                        double* dchi2_dflux, double* dpenalty_dz, int* status,
+                        rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * fitz candidates on the device: replaces the host steps of redrock's fitz

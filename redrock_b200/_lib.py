@@ -127,7 +127,8 @@ _SIGNATURES = {
     "rr_zscan_pairs_grad": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment),
                                     c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
                                     c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
-                                    c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+                                    c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p]),
     "rr_zscan_pairs": (c_int, [ctypes.POINTER(PairTemplate), ctypes.POINTER(PairSegment), c_int,
                                c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_int64,
                                c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -57,6 +57,22 @@ def chi2_and_grad(ctx, pair_target, pair_z, want_dflux=False):
     return run_pairs_grad(ctx.rows, ctx.src, pair_target, pair_z, want_dflux=want_dflux)
 
 
+def objective_and_grad(ctx, pair_target, pair_z, penalty=False):
+    """(objective, coeff, d objective / dz, envelope curvature) host arrays
+    per pair: chi2, or with penalty=True chi2 + the [OII] penalty -- what
+    fitz ranks its fine-grid points by -- and its exact z derivative."""
+    ok = pair_ranges_ok(ctx.src, ctx.layout, pair_z)
+    if not np.all(ok):
+        raise ValueError('edges must be within input x range')
+    dp = [] if penalty else None
+    c2, co, pen, g, h, _ = run_pairs_grad(ctx.rows, ctx.src, pair_target, pair_z, dpen=dp)
+    c2, co, g, h = c2.cpu().numpy(), co.cpu().numpy(), g.cpu().numpy(), h.cpu().numpy()
+    if penalty:
+        c2 = c2 + pen.cpu().numpy()
+        g = g + dp[0].cpu().numpy()
+    return c2, co, g, h
+
+
 class Chi2Scan(torch.autograd.Function):
     """chi2 of pairs (target index, z) as a differentiable function of z
     (per pair) and of the packed flux (per target)."""
@@ -86,8 +102,9 @@ class Chi2Scan(torch.autograd.Function):
         return gz, gf, None, None
 
 
-def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10):
-    """Minimise chi2(z) for each pair inside [zlo, zhi], starting from z0
+def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10, penalty=False):
+    """Minimise chi2(z) -- chi2 + [OII] penalty with penalty=True, fitz's
+    objective -- for each pair inside [zlo, zhi], starting from z0
     (the best fine-grid point; zlo, zhi its neighbours), with Newton steps
     on dchi2/dz = 0.  The adjoint kernel's dchi2/dz is exact, so the
     curvature of each step comes from exact gradient differences (the
@@ -113,11 +130,12 @@ def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10):
     if n == 0:
         e = np.zeros(0)
         return e, e.copy(), np.zeros((0, ctx.src.nbasis)), e.copy(), e.copy(), 0
-    c3, co3, _, g3, h3, _ = chi2_and_grad(ctx, np.tile(t, 3), np.concatenate([zlo, z0, zhi]))
-    c3 = c3.cpu().numpy().reshape(3, n)
-    g3 = g3.cpu().numpy().reshape(3, n)
-    h3 = h3.cpu().numpy().reshape(3, n)
-    co3 = co3.cpu().numpy().reshape(3, n, -1)
+    c3, co3, g3, h3 = objective_and_grad(ctx, np.tile(t, 3), np.concatenate([zlo, z0, zhi]),
+                                         penalty)
+    c3 = c3.reshape(3, n)
+    g3 = g3.reshape(3, n)
+    h3 = h3.reshape(3, n)
+    co3 = co3.reshape(3, n, -1)
     zs = np.stack([zlo, z0, zhi])
     # best evaluated point so far
     k = np.argmin(c3, axis=0)
@@ -147,10 +165,7 @@ def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10):
         zn = np.where(den > 0, ai - wai * (bi - ai) / np.where(den > 0, den, 1.0),
                       0.5 * (ai + bi))
         zn = np.where((zn > ai) & (zn < bi), zn, 0.5 * (ai + bi))
-        c2, co, _, gn, hn, _ = chi2_and_grad(ctx, t[idx], zn)
-        c2 = c2.cpu().numpy()
-        gn = gn.cpu().numpy()
-        co = co.cpu().numpy()
+        c2, co, gn, _ = objective_and_grad(ctx, t[idx], zn, penalty)
         better = c2 < cbest[idx]
         upd = idx[better]
         zbest[upd], cbest[upd], gbest[upd] = zn[better], c2[better], gn[better]

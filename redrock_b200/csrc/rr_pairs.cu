@@ -48,6 +48,7 @@ struct PairsParams {
   double* dchi2_dz;     // [npairs]
   double* d2chi2_dz2;   // [npairs]
   double* dchi2_dflux;  // [npairs][npix_row] or NULL
+  double* dpen_dz;      // [npairs] d penalty / dz or NULL
   const double* sw;     // [ntarget][npix_row] sqrt(w), needed for dchi2_dflux
   int* status;
 };
@@ -296,6 +297,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
         if (GRAD) {
           p.dchi2_dz[pr] = nan("");
           p.d2chi2_dz2[pr] = nan("");
+          if (p.dpen_dz) p.dpen_dz[pr] = nan("");
         }
       }
       continue;
@@ -323,6 +325,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
         if (threadIdx.x == 0) {
           p.dchi2_dz[pr] = 0.0;
           p.d2chi2_dz2[pr] = 0.0;
+          if (p.dpen_dz) p.dpen_dz[pr] = 0.0;
         }
         __syncthreads();
         continue;
@@ -343,12 +346,24 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
 #pragma unroll
         for (int b = 0; b < NB; ++b) uv[b] = acc[3 + b] - acc[3 + NB + b];
         double q = 0.0;
-        if (ldlt_solve<NB>(mp, uv, x))
+        const bool xok = ldlt_solve<NB>(mp, uv, x);
+        if (xok)
 #pragma unroll
           for (int b = 0; b < NB; ++b) q = fma(uv[b], x[b], q);
         p.chi2[pr] = acc[0];
         p.dchi2_dz[pr] = -2.0 * acc[1];
         p.d2chi2_dz2[pr] = 2.0 * acc[2] - 2.0 * q;
+        if (p.dpen_dz) {
+          // x = dc/dz = (M + P)^-1 (u - v); the penalty -c.oii (when the
+          // [OII] model is negative) changes by -x.oii
+          double s = 0.0, ds = 0.0;
+          if (p.tm.oii)
+            for (int b = 0; b < NB; ++b) {
+              s = fma(sm.c[b], p.tm.oii[b], s);
+              ds = fma(xok ? x[b] : 0.0, p.tm.oii[b], ds);
+            }
+          p.dpen_dz[pr] = (p.wsum[t] != 0.0 && s < 0.0) ? -ds : 0.0;
+        }
       }
       __syncthreads();
       continue;
@@ -560,7 +575,7 @@ extern "C" int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_s
                                    const int32_t* pair_target, const double* pair_z,
                                    int64_t npairs, double* chi2, double* coeff, double* penalty,
                                    double* dchi2_dz, double* d2chi2_dz2, double* dchi2_dflux,
-                                   int* status, rr_stream_t stream) {
+                                   double* dpenalty_dz, int* status, rr_stream_t stream) {
   PairsParams p;
   int rc = pairs_params(p, tmpl, segs, nseg, rows, fwf, wsum, npix_row, pair_target, pair_z,
                         npairs, chi2, coeff, penalty, status);
@@ -570,6 +585,7 @@ extern "C" int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_s
   p.dchi2_dz = dchi2_dz;
   p.d2chi2_dz2 = d2chi2_dz2;
   p.dchi2_dflux = dchi2_dflux;
+  p.dpen_dz = dpenalty_dz;
   p.sw = sw;
   return dispatch_pairs<true>(p, tmpl->nbasis, (cudaStream_t)stream);
 }

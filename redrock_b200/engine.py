@@ -694,9 +694,12 @@ class FitzCandidates:
         _lib.check(rc, "rr_fitz_candidates")
 
 
-def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=None, status=None):
+def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=None, status=None,
+                   dpen=None):
     """chi2, coeff, penalty, dchi2/dz, d2chi2/dz2 (and dchi2/dflux
-    [n][npix_row] in the packed pixel order) device tensors for the pairs."""
+    [n][npix_row] in the packed pixel order) device tensors for the pairs.
+    dpen: a list that receives the d penalty / dz tensor (the [OII]
+    penalty's derivative, zero where the penalty is inactive)."""
     L = _lib.lib()
     dev = device()
     n = len(pair_z)
@@ -707,6 +710,9 @@ def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=N
     g = torch.empty(n, dtype=torch.float64, device=dev)
     h = torch.empty(n, dtype=torch.float64, device=dev)
     df = torch.zeros((n, rowpack.npix_row), dtype=torch.float64, device=dev) if want_dflux else None
+    dp = torch.zeros(n, dtype=torch.float64, device=dev) if dpen is not None else None
+    if dpen is not None:
+        dpen.append(dp)
     if n == 0:
         return chi2, coeff, pen, g, h, df
     dt = to_device(np.asarray(pair_target, dtype=np.int32), torch.int32)
@@ -719,7 +725,8 @@ def run_pairs_grad(rowpack, src, pair_target, pair_z, want_dflux=False, stream=N
     rc = L.rr_zscan_pairs_grad(ctypes.byref(tm), segs, len(rowpack.segments), ptr(rowpack.rows),
                                ptr(rowpack.sw), ptr(rowpack.fwf), ptr(rowpack.wsum),
                                rowpack.npix_row, ptr(dt), ptr(dz), n, ptr(chi2), ptr(coeff),
-                               ptr(pen), ptr(g), ptr(h), ptr(df), st.ptr, stream_handle(stream))
+                               ptr(pen), ptr(g), ptr(h), ptr(df), ptr(dp), st.ptr,
+                               stream_handle(stream))
     _lib.check(rc, "rr_zscan_pairs_grad")
     if status is None:
         torch.cuda.current_stream().synchronize()

@@ -375,18 +375,15 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
         ctx = newton_ctx.get("ctx")
         if ctx is None:
             ctx = newton_ctx["ctx"] = _NewtonCtx(ref)
+        # the objective of the fine grid: chi2 plus the [OII] penalty
         z, c2, co, g, h, _ = refine_newton(ctx, np.asarray(tj, dtype=np.int32), z3[:, 1],
-                                           z3[:, 0], z3[:, 2])
+                                           z3[:, 0], z3[:, 2], penalty=has_oii)
         zwarn = np.zeros(len(z), dtype=np.int64)
         pos_h = h > 0
         sigma = np.where(pos_h, np.sqrt(2.0 / np.where(pos_h, h, 1.0)), -1.0)
         zwarn[~pos_h] |= BAD_MINFIT
         zwarn[~((z3[:, 0] < z) & (z < z3[:, 2]))] |= BAD_MINFIT
-        pen = np.zeros(len(z))
-        if has_oii:
-            s_ = co @ np.asarray(ref.src.oii, dtype=np.float64)
-            pen = np.where(s_ < 0, -s_, 0.0)
-        return z, sigma, c2 + pen, zwarn
+        return z, sigma, c2, zwarn
 
     if pre is not None and any(use_pre):
         # the device-evaluated candidates: their fine grids and one batch of

@@ -128,3 +128,32 @@ def test_dchi2_dflux_fd_and_autograd():
     expect = torch.zeros_like(fl)
     expect.index_add_(0, torch.as_tensor(pt, dtype=torch.int64, device="cuda"), df2)
     torch.testing.assert_close(fl.grad, expect, rtol=1e-12, atol=1e-12)
+
+
+def test_dpenalty_dz_fd():
+    """The [OII] penalty's z derivative (-oii . dc/dz with dc/dz from the
+    kernel's (M+P)^-1 (u - v)) against central differences of the penalty
+    the kernel itself returns, where the penalty is active on both sides:
+    within 1e-4 relative + 1e-3 absolute; zero where the penalty is off."""
+    from redrock_b200.adjoint import objective_and_grad
+    from redrock_b200.engine import run_pairs_grad
+    tg, ts, ctx = _ctx("GALAXY", ntarget=6)
+    z = np.linspace(0.05, 1.4, 40)
+    pt = np.repeat(np.arange(len(tg)), len(z)).astype(np.int32)
+    zz = np.tile(z, len(tg))
+    dp = []
+    _, _, pen, _, _, _ = run_pairs_grad(ctx.rows, ctx.src, pt, zz, dpen=dp)
+    pen, dpen = pen.cpu().numpy(), dp[0].cpu().numpy()
+    h = 1e-6
+    pp = run_pairs_grad(ctx.rows, ctx.src, pt, zz + h)[2].cpu().numpy()
+    pm = run_pairs_grad(ctx.rows, ctx.src, pt, zz - h)[2].cpu().numpy()
+    on = (pen > 0) & (pp > 0) & (pm > 0)
+    assert on.sum() >= 5
+    fd = (pp - pm) / (2 * h)
+    assert np.all(np.abs(dpen[on] - fd[on]) <= 1e-4 * np.abs(fd[on]) + 1e-3)
+    assert np.all(dpen[pen == 0] == 0)
+    # the objective's derivative is chi2's plus the penalty's
+    f, _, g, _ = objective_and_grad(ctx, pt, zz, penalty=True)
+    c, _, g0, _ = objective_and_grad(ctx, pt, zz, penalty=False)
+    np.testing.assert_allclose(f, c + pen, rtol=0, atol=0)
+    np.testing.assert_allclose(g, g0 + dpen, rtol=0, atol=0)

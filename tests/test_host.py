@@ -313,8 +313,10 @@ def test_newton_refinement_logic_on_a_model_function(monkeypatch):
                 torch.zeros(n, dtype=torch.float64), torch.tensor(g),
                 torch.full((n,), 1e30, dtype=torch.float64), None)
 
-    monkeypatch.setattr(A, "chi2_and_grad", fake)
-    ctx = types.SimpleNamespace(src=types.SimpleNamespace(nbasis=3))
+    monkeypatch.setattr(A, "run_pairs_grad",
+                        lambda rows, src, t, z, want_dflux=False, dpen=None: fake(None, t, z))
+    monkeypatch.setattr(A, "pair_ranges_ok", lambda src, layout, z: np.ones(len(z), bool))
+    ctx = types.SimpleNamespace(src=types.SimpleNamespace(nbasis=3), rows=None, layout=None)
     step = 4e-5
     z0 = zmin + rng.uniform(-0.5, 0.5, nt) * step
     z, c, co, g, h, it = A.refine_newton(ctx, np.arange(nt), z0, z0 - step, z0 + step)
