@@ -501,7 +501,8 @@ def zfind_study(rtg, tms, torch, ntarget=500):
     t_graph, gra = timed(graph=True)
     t_newton, new = timed(refine="newton")
     same = all(np.array_equal(np.asarray(gra[k]), np.asarray(par[k])) for k in par)
-    # dense FP64 scans around each target's best GALAXY minimum
+    # dense FP64 scans of the fine-grid cell each target's best GALAXY
+    # minimum was refined in (the three fine-grid points around the best)
     gal = tms[0]
     src = TemplateSource.from_template(gal)
     rows = RowPack.from_targets(sub, dts[0].basis.layout)
@@ -510,26 +511,32 @@ def zfind_study(rtg, tms, torch, ntarget=500):
     err_p, err_n = [], []
     idx = {t.id: i for i, t in enumerate(sub)}
     for tab, errs in ((par, err_p), (new, err_n)):
-        m = (tab["znum"] == 0) & (tab["spectype"] == "GALAXY") & (tab["zwarn"] == 0)
-        tids = tab["targetid"][m]
-        zs = tab["z"][m]
-        if len(zs) == 0:
+        m = np.nonzero((tab["znum"] == 0) & (tab["spectype"] == "GALAXY")
+                       & (tab["zwarn"] == 0))[0]
+        if len(m) == 0:
             continue
-        off = np.linspace(-fine, fine, 401)
-        zd = (np.exp(np.log1p(zs)[:, None] + off[None, :]) - 1.0)
-        pt = np.repeat([idx[t] for t in tids], 401).astype(np.int32)
+        zs = tab["z"][m]
+        k = np.clip(np.argmin(tab["zzchi2"][m], axis=1), 1, tab["zz"].shape[1] - 2)
+        zd = np.linspace(tab["zz"][m, k - 1], tab["zz"][m, k + 1], 401, axis=1)
+        pt = np.repeat([idx[t] for t in tab["targetid"][m]], 401).astype(np.int32)
         c2, _, pen = run_pairs(rows, src, pt, zd.ravel())
-        c2 = (c2 + pen).cpu().numpy().reshape(len(zs), 401)
-        zbest = zd[np.arange(len(zs)), np.argmin(c2, axis=1)]
+        c2 = (c2 + pen).cpu().numpy().reshape(len(m), 401)
+        zbest = zd[np.arange(len(m)), np.argmin(c2, axis=1)]
+        # chi2 of the reported minimum: the parabola's is its fitted vertex,
+        # so it is evaluated at the reported z here for both
+        zrep = np.asarray(zs, dtype=np.float64)
+        cr, _, penr = run_pairs(rows, src, np.array([idx[t] for t in tab["targetid"][m]],
+                                                    dtype=np.int32), zrep)
+        cr = (cr + penr).cpu().numpy()
         # (|dln(1+z)| to the dense minimum, chi2 at the reported z minus the
         # dense minimum's chi2)
         errs.extend(zip(np.abs(np.log1p(zs) - np.log1p(zbest)).tolist(),
-                        (c2[:, 200] - c2.min(axis=1)).tolist()))
+                        (cr - c2.min(axis=1)).tolist()))
     return {"targets": len(sub), "templates": len(tms), "nminima": 3,
             "eager_s": t_eager, "graph_s": t_graph, "newton_s": t_newton,
             "graph_equals_eager": bool(same),
             "dense_grid_check": dict(
-                cases=len(err_n), grid="401 points over +-1 fine-grid step (FP64)",
+                cases=len(err_n), grid="401 points over the refined fine-grid cell (FP64)",
                 dense_grid_step_dlnz=float(2 * fine / 400),
                 **{f"{k}_{name}": (float(f(np.asarray(e)[:, col])) if e else None)
                    for name, e in (("parabola", err_p), ("newton", err_n))

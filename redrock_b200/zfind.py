@@ -235,6 +235,18 @@ def _finalise_target(tid, fits, nminima, arch=None):
 DEVICE_CANDIDATES_EXTRA = 2
 
 
+_warm_devices = set()
+
+
+class _PackShape:
+    """What the tile autotuner keys a choice on (grid layout, number of
+    target blocks), without packing the targets."""
+
+    def __init__(self, layout, nblock):
+        self.layout = layout
+        self.nblock = nblock
+
+
 class DeviceFitzPlan:
     """The device part of zfind for one target batch -- target packing, the
     fused coarse scan of every template, the K lowest chi2 minima of every
@@ -243,9 +255,9 @@ class DeviceFitzPlan:
     CUDA graph and replayed.  ``run()`` returns the coarse-scan results in
     calc_zchi2_targets' form and one ``fitz.PrecomputedFine`` per template.
 
-    Lazy one-time set-up (kernel attributes, constant tables, the tile
-    autotuner) happens in an eager warm-up on the first target block before
-    any capture."""
+    Lazy one-time set-up (kernel attributes, constant tables) happens in an
+    eager warm-up on the first target block before the first capture on a
+    device; the tile autotuner's choice is cached per batch shape."""
 
     def __init__(self, local, templates, layout, nminima=3, nfine=15, graph=True):
         import torch
@@ -265,16 +277,24 @@ class DeviceFitzPlan:
                      for t in self.templates]
         self.dbatch = TargetBatch(local, layout).to_device()
         self.rowpack = RowPack(self.dbatch)
-        pack0 = TargetPack(self.dbatch, status=self.status)
-        self.tiles = autotune.tiles_of(autotune.choice(pack0, self.bases)
-                                       or autotune.tune(pack0, self.bases))
-        del pack0
-        # warm-up on the first 32 targets: every kernel's lazy set-up
-        small = local[:32]
-        wb = TargetBatch(small, layout).to_device()
-        self._body(wb, RowPack(wb))
-        torch.cuda.synchronize()
-        self.status.check("zfind warm-up")
+        key = _PackShape(layout, self.dbatch.batch.nblock)
+        best = autotune.choice(key, self.bases)
+        if best is None:
+            pack0 = TargetPack(self.dbatch, status=self.status)
+            best = autotune.tune(pack0, self.bases)
+            del pack0
+        self.tiles = autotune.tiles_of(best)
+        dev = torch.cuda.current_device()
+        if dev not in _warm_devices:
+            # once per process and device, before any capture: every
+            # kernel's lazy set-up (attributes, constant tables), on the
+            # first 32 targets
+            small = local[:32]
+            wb = TargetBatch(small, layout).to_device()
+            self._body(wb, RowPack(wb))
+            torch.cuda.synchronize()
+            self.status.check("zfind warm-up")
+            _warm_devices.add(dev)
         self.graph = None
         self.outs = None
         if graph:

@@ -96,3 +96,28 @@ def test_direct_residual_resweep_vs_oracle():
     pe = res[0].penalty.cpu().numpy()
     for j in range(len(tg)):
         check_lane(zc[j], co[j], pe[j], ozc[j], oco[j], ope[j])
+
+
+def test_stress_high_snr_full_grids():
+    """Precision-stress targets (config 4's generator: 60 % QSO-like at z up
+    to 6 rendered with Inoue14, S/N 20-50 here) against the oracle on the
+    full GALAXY and QSO redshift grids: every evaluation, whether the
+    normal-equation chi2 passed its error bound or was re-swept as the direct
+    residual, within |dchi2| <= 2e-5, identical argmin."""
+    import bench
+    from redrock_b200 import targets as T, templates as TM, zscan
+
+    def trans(z, w):
+        return O.transmission_Lyman(np.array([z]), w, model="Inoue14")[0]
+    tg = synth.make_population(8, seed=131, qso_frac=0.6, snr_range=(20.0, 50.0),
+                               transmission=trans)
+    rtg = T.from_synth(tg)
+    dwave = T.DistTargetsCopy(rtg).wavegrids()
+    tset = synth.template_set()[:2]          # GALAXY, QSO on their full grids
+    dts = [TM.DistTemplate(TM.from_synth(ts), dwave) for ts in tset]
+    res = zscan.scan_device(rtg, dts, host=True)
+    for ts, r in zip(tset, res):
+        ozc, oco, ope = oracle_template(ts, tg)
+        for j in range(len(tg)):
+            check_lane(r.zchi2[j], r.zcoeff[j], r.penalty[j], ozc[j], oco[j], ope[j])
+    assert bench.WORKLOADS["stress20000"]["snr_range"] == (0.5, 50.0)

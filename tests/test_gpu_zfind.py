@@ -161,25 +161,27 @@ def test_zfind_newton_refinement(golden):
         # a fine-grid step: the 15-point grid spans two coarse steps
         assert dlnz.min() <= steps[new["spectype"][r]] * 2 / 14 + 1e-12
         assert new["zerr"][r] > 0
-    # each good GALAXY Newton minimum against a dense FP64 scan (201 points
-    # over +-1 fine-grid step around it): Newton lands on the minimum, to
-    # within the dense grid's own resolution
+    # each good GALAXY Newton minimum against a dense FP64 scan (201 points)
+    # of the fine-grid cell it searched -- the three fine-grid points around
+    # the best one: Newton lands on fitz's objective's minimum in that cell
+    # to within the dense grid's own resolution
     from redrock_b200.engine import RowPack, TemplateSource, run_pairs
     gal = [t for t in dts if t.template.full_type == "GALAXY"][0]
     local = list(dz.local())
     rows = RowPack.from_targets(local, gal.basis.layout)
     src = TemplateSource.from_template(gal.template)
     idx = {t.id: i for i, t in enumerate(local)}
-    m = (new["zwarn"] == 0) & (new["spectype"] == "GALAXY")
-    assert m.sum() >= 2
-    fine = steps["GALAXY"] * 2 / 14
-    off = np.linspace(-fine, fine, 201)
-    zs = new["z"][m]
-    zd = np.exp(np.log1p(zs)[:, None] + off[None, :]) - 1.0
+    m = np.nonzero((new["zwarn"] == 0) & (new["spectype"] == "GALAXY"))[0]
+    assert len(m) >= 2
+    k = np.clip(np.argmin(new["zzchi2"][m], axis=1), 1, new["zz"].shape[1] - 2)
+    lo = new["zz"][m, k - 1]
+    hi = new["zz"][m, k + 1]
+    zd = np.linspace(lo, hi, 201, axis=1)
     pt = np.repeat([idx[t] for t in new["targetid"][m]], 201).astype(np.int32)
     c2, _, pen = run_pairs(rows, src, pt, zd.ravel())
-    c2 = (c2 + pen).cpu().numpy().reshape(len(zs), 201)
-    assert np.all(c2[:, 100] - c2.min(axis=1) <= 1e-4), c2[:, 100] - c2.min(axis=1)
+    c2 = (c2 + pen).cpu().numpy().reshape(len(m), 201)
+    assert np.all((lo <= new["z"][m]) & (new["z"][m] <= hi))
+    assert np.all(new["chi2"][m] - c2.min(axis=1) <= 1e-4), new["chi2"][m] - c2.min(axis=1)
 
 
 def test_fitz_candidates_kernel_vs_find_minima():
