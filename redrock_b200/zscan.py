@@ -235,11 +235,12 @@ class _NoGC:
         return False
 
 
-def scan_device(targets, dtemplates, chunk=None, host=False):
+def scan_device(targets, dtemplates, chunk=None, host=False, on_host_ready=None):
     """Fused scan of every target against every template (see
     _scan_device), with the cyclic garbage collector paused."""
     with _NoGC():
-        out = _scan_device(targets, dtemplates, chunk=chunk, host=host)
+        out = _scan_device(targets, dtemplates, chunk=chunk, host=host,
+                           on_host_ready=on_host_ready)
     # bases built asynchronously (DistTemplate) report device errors here
     for dt in dtemplates:
         chk = getattr(dt, "check", None)
@@ -248,7 +249,7 @@ def scan_device(targets, dtemplates, chunk=None, host=False):
     return out
 
 
-def _scan_device(targets, dtemplates, chunk=None, host=False):
+def _scan_device(targets, dtemplates, chunk=None, host=False, on_host_ready=None):
     """Fused scan of every target against every template.
 
     Returns a list (one entry per template) of results with zchi2 (T, nz),
@@ -257,7 +258,10 @@ def _scan_device(targets, dtemplates, chunk=None, host=False):
     processed in chunks (a small first one, then CHUNK_TARGETS): the host
     packing and upload of chunk k + 1 run while the GPU scans chunk k, and
     with host=True chunk k's results are copied to pinned host memory on a
-    side stream while chunk k + 1 runs.
+    side stream while chunk k + 1 runs.  on_host_ready(hout) (host=True) is
+    called once the GPU has the first two chunks queued, with the host
+    result arrays (filled as the copies land, complete when this returns),
+    so that the caller can build its views of them meanwhile.
     """
     layout = _layout_for(dtemplates[0], targets)
     all_bases = _bases_for(dtemplates, layout)
@@ -309,6 +313,8 @@ def _scan_device(targets, dtemplates, chunk=None, host=False):
                 for h, r in zip(hout, res):
                     for dst, src in zip(h.t, (r.zchi2, r.zcoeff, r.penalty)):
                         dst[i0:i1].copy_(src, non_blocking=True)
+            if on_host_ready is not None and len(keep) == min(2, len(bounds)):
+                on_host_ready(hout)
         else:
             parts.append(res)
     main.synchronize()
@@ -363,13 +369,21 @@ def calc_zchi2_targets(targets, templates, mp_procs=1, use_gpu=True):
         sys.stdout.flush()
     if len(tids) == 0:
         return results
-    out = scan_device(data, list(templates), host=True)
-    for t, r in zip(templates, out):
-        ft = t.template.full_type
-        zc, co, pe = r.zchi2, r.zcoeff, r.penalty
-        for i, tid in enumerate(tids):
-            results.setdefault(tid, {})[ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i], penalty=pe[i],
-                                    zcoeff=co[i])
+
+    def fill(out):
+        # views of the pinned host results, built while the GPU scans
+        for t, r in zip(templates, out):
+            ft = t.template.full_type
+            zc, co, pe = r.zchi2, r.zcoeff, r.penalty
+            z = t.template.redshifts
+            for i, tid in enumerate(tids):
+                results.setdefault(tid, {})[ft] = dict(redshifts=z, zchi2=zc[i], penalty=pe[i],
+                                                       zcoeff=co[i])
+    done = []
+    out = scan_device(data, list(templates), host=True,
+                      on_host_ready=lambda hout: (fill(hout), done.append(True)))
+    if not done:
+        fill(out)
     return results
 
 
