@@ -905,7 +905,7 @@ def main():
     ap.add_argument("--plain-targets", type=int, default=8)
     ap.add_argument("--ref-zsub", type=int, default=10,
                     help="redshift subsampling of the cpu_baseline sample")
-    ap.add_argument("--ref-step-zsub", type=int, default=20,
+    ap.add_argument("--ref-step-zsub", type=int, default=10,
                     help="redshift subsampling of each --impl reference step")
     ap.add_argument("--ref-per-core", type=int, default=2,
                     help="targets per host core in a reference sample")

@@ -119,9 +119,9 @@ def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10, penalty=F
 
     Returns (z, chi2, coeff, dchi2_dz, d2chi2_dz2, iterations): z is the
     evaluated point of lowest chi2 (the root of dchi2/dz once converged),
-    d2chi2_dz2 the secant curvature of the final bracket (> 0), or the
-    kernel's curvature where no bracket formed (minimum at a bracket edge:
-    z is then that edge)."""
+    d2chi2_dz2 the secant curvature of the final bracket (> 0), or -1 where
+    no bracket formed (the minimum lies beyond [zlo, zhi]; z is then the best
+    point evaluated)."""
     t = np.asarray(pair_target, dtype=np.int32)
     n = len(t)
     z0 = np.asarray(z0, dtype=np.float64)
@@ -149,6 +149,35 @@ def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10, penalty=F
     ga = np.where(right, g3[1], g3[0])
     gb = np.where(right, g3[2], g3[1])
     active = (ga <= 0) & (gb >= 0) & (b > a)
+    # no sign change on that side although z0 is the best point: the
+    # objective has a bump between z0 and the neighbour, and a minimum on
+    # the way (descending from z0, then up and down again).  Probe the
+    # gradient at 1/4, 1/2, 3/4 of the way to find where it turns positive
+    # (negative, going left).
+    probe = np.nonzero(~active & (b > a))[0]
+    if len(probe):
+        fr = np.array([0.25, 0.5, 0.75])
+        rp = right[probe]
+        zp = np.where(rp[:, None], a[probe, None] + fr[None, :] * (b - a)[probe, None],
+                      b[probe, None] - fr[None, :] * (b - a)[probe, None])
+        cp, cop, gp, _ = objective_and_grad(ctx, np.repeat(t[probe], 3), zp.ravel(), penalty)
+        cp, gp = cp.reshape(-1, 3), gp.reshape(-1, 3)
+        cop = cop.reshape(len(probe), 3, -1)
+        for q, i in enumerate(probe):
+            kb = np.argmin(cp[q])
+            if cp[q, kb] < cbest[i]:
+                zbest[i], cbest[i], gbest[i], cobest[i] = zp[q, kb], cp[q, kb], gp[q, kb], cop[q, kb]
+            prev_z, prev_g = (a[i], ga[i]) if rp[q] else (b[i], gb[i])
+            for k in range(3):
+                turned = gp[q, k] >= 0 if rp[q] else gp[q, k] <= 0
+                if turned:
+                    if rp[q]:
+                        a[i], ga[i], b[i], gb[i] = prev_z, prev_g, zp[q, k], gp[q, k]
+                    else:
+                        a[i], ga[i], b[i], gb[i] = zp[q, k], gp[q, k], prev_z, prev_g
+                    active[i] = True
+                    break
+                prev_z, prev_g = zp[q, k], gp[q, k]
     # Illinois weights: the stored end values used for the next step (the
     # true gradients ga, gb are kept for the curvature)
     wa, wb = ga.copy(), gb.copy()
@@ -181,6 +210,8 @@ def refine_newton(ctx, pair_target, z0, zlo, zhi, niter=24, tol=1e-10, penalty=F
         wa[lb] = np.where(last[lb] == 1, 0.5 * wa[lb], wa[lb])
         last[lb] = 1
         active[idx[gn == 0]] = False
-    curv = np.where((ga <= 0) & (gb >= 0) & (b > a),
-                    (gb - ga) / np.where(b > a, b - a, 1.0), hbest)
+    bracketed = (ga <= 0) & (gb >= 0) & (b > a)
+    # no bracket at all: the best point is not a verified minimum (reported
+    # with a negative curvature, which fitz flags as BAD_MINFIT)
+    curv = np.where(bracketed, (gb - ga) / np.where(b > a, b - a, 1.0), -1.0)
     return zbest, cbest, cobest, gbest, curv, it
