@@ -262,6 +262,10 @@ int rr_zscan_fused_opt(const rr_scan_targets* targets, const rr_scan_template* t
  * Pairs whose redshift puts a bin edge outside the template range set
  * RR_ERANGE in status and get NaN outputs (check them on the host first:
  * edge_min >= x_first (1+z) and edge_max <= x_last (1+z)).
+ * method RR_SOLVE_PCA solves as the fused scan does; RR_SOLVE_NNLS and
+ * RR_SOLVE_BVLS (NMF templates) solve as rr_zchi2_batch_plain_ex does, with
+ * chi2 the direct residual sum w (f - Tb c)^2 and HUGE_CHI2 / zero
+ * coefficients where the solver fails (rr_zscan_pairs_grad: RR_ENOTSUP).
  * ---------------------------------------------------------------------- */
 typedef struct {
   const double* x;      /* device, template rest wavelengths [nx] */
@@ -273,6 +277,9 @@ typedef struct {
   int32_t pad_;
   const double* prior;  /* device nbasis*nbasis or NULL */
   const double* oii;    /* device nbasis [OII] window sums or NULL */
+  const double* bounds; /* HOST [2][nbasis] lower then upper bounds for
+                           RR_SOLVE_BVLS (solver_args['bounds']), or NULL
+                           for (-inf, inf); ignored by the other methods */
 } rr_pair_template;
 
 typedef struct {

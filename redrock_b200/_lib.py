@@ -84,7 +84,7 @@ class ScanTargets(ctypes.Structure):
 class PairTemplate(ctypes.Structure):
     _fields_ = [("x", c_void_p), ("nx", c_int64), ("y", c_void_p), ("nbasis", c_int32),
                 ("igm_model", c_int32), ("method", c_int32), ("pad_", c_int32),
-                ("prior", c_void_p), ("oii", c_void_p)]
+                ("prior", c_void_p), ("oii", c_void_p), ("bounds", c_void_p)]
 
 
 class PairSegment(ctypes.Structure):

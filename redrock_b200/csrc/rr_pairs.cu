@@ -20,6 +20,7 @@
 // beyond a bin edge runs on shared memory.
 #include <cstring>
 
+#include "rr_lsq_dev.cuh"
 #include "rr_rebin_dev.cuh"
 #include "rr_solve_dev.cuh"
 
@@ -51,6 +52,10 @@ struct PairsParams {
   double* dpen_dz;      // [npairs] d penalty / dz or NULL
   const double* sw;     // [ntarget][npix_row] sqrt(w), needed for dchi2_dflux
   int* status;
+  // RR_SOLVE_BVLS bounds (+-inf when the caller gives none); read in place
+  // by the solver, like the plain chain's
+  double lo[RR_MAX_NBASIS];
+  double hi[RR_MAX_NBASIS];
 };
 
 // first j with x[j] (1+z) > e over x[lo..hi) (global memory)
@@ -270,6 +275,32 @@ __device__ void block_sum(double* v, int n, PairSmem<NB>& sm) {
   __syncthreads();
 }
 
+// the plain chain's bounded solves (plain_lsq_kernel) on one pair's
+// packed M and y: the full symmetric M + prior, then NNLS or BVLS
+template <int NB>
+__device__ __noinline__ bool bounded_solve(const PairsParams& p, const double (&mm)[NB * (NB + 1) / 2],
+                                           const double (&yy)[NB], double (&c)[NB]) {
+  double full[NB][NB], b[NB];
+  for (int i = 0; i < NB; ++i) {
+    b[i] = yy[i];
+    for (int j = 0; j <= i; ++j) {
+      double v = mm[i * (i + 1) / 2 + j];
+      if (p.tm.prior) v += p.tm.prior[i * NB + j];
+      full[i][j] = full[j][i] = v;
+    }
+  }
+  bool ok;
+  if (p.tm.method == RR_SOLVE_NNLS)
+    ok = nnls_solve<NB>(full, b, c);
+  else if (p.tm.method == RR_SOLVE_BVLS)
+    ok = bvls_solve<NB>(full, b, p.lo, p.hi, c);
+  else
+    ok = false;
+  if (!ok)
+    for (int i = 0; i < NB; ++i) c[i] = 0.0;
+  return ok;
+}
+
 template <int NB, bool GRAD>
 __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __grid_constant__ PairsParams p) {
   extern __shared__ __align__(16) unsigned char pair_smem_raw[];
@@ -306,8 +337,19 @@ __global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __gr
     bool solved = false;
     if (threadIdx.x == 0) {
       double c[NB], chi2 = 0.0, err = 0.0;
-      solved = solve_eval<NB>(p.tm.method, p.tm.prior, mm, yy, p.fwf[t], p.wsum[t], c, chi2, err);
-      sm.fix = (solved && err > kChi2FixTol) ? 1 : 0;
+      if (GRAD || p.tm.method == RR_SOLVE_PCA) {
+        solved = solve_eval<NB>(p.tm.method, p.tm.prior, mm, yy, p.fwf[t], p.wsum[t], c, chi2,
+                                err);
+        sm.fix = (solved && err > kChi2FixTol) ? 1 : 0;
+      } else {
+        // NMF / NNLS / BVLS (calc_zchi2_batch's bounded branches): the
+        // solver on M + prior and y, then chi2 always as the direct
+        // residual (a constrained c is no stationary point of
+        // f^T W f - c^T y); a failed solve gives HUGE_CHI2, zero c
+        solved = bounded_solve<NB>(p, mm, yy, c);
+        chi2 = kHugeChi2;
+        sm.fix = solved ? 1 : 0;
+      }
       sm.bad = solved ? 0 : 1;
       for (int b = 0; b < NB; ++b) sm.c[b] = c[b];
       p.chi2[pr] = chi2;
@@ -515,8 +557,20 @@ static int pairs_params(PairsParams& p, const rr_pair_template* tmpl, const rr_p
     return RR_EINVAL;
   if (tmpl->igm_model < RR_IGM_NONE || tmpl->igm_model > RR_IGM_INOUE14) return RR_EINVAL;
   if (tmpl->oii && !penalty) return RR_EINVAL;
+  if (tmpl->method < RR_SOLVE_PCA || tmpl->method > RR_SOLVE_BVLS) return RR_EINVAL;
   memset(&p, 0, sizeof(p));
   p.tm = *tmpl;
+  for (int i = 0; i < RR_MAX_NBASIS; ++i) {
+    p.lo[i] = -INFINITY;
+    p.hi[i] = INFINITY;
+  }
+  if (tmpl->bounds)
+    for (int i = 0; i < tmpl->nbasis; ++i) {
+      p.lo[i] = tmpl->bounds[i];
+      p.hi[i] = tmpl->bounds[tmpl->nbasis + i];
+      if (!(p.lo[i] <= p.hi[i])) return RR_EINVAL;
+    }
+  p.tm.bounds = nullptr;  // host memory: not for the device
   p.nseg = nseg;
   for (int s = 0; s < nseg; ++s) {
     if (segs[s].npix < 1 || !segs[s].edges || !segs[s].wave || segs[s].row_offset < 0 ||
@@ -581,6 +635,7 @@ extern "C" int rr_zscan_pairs_grad(const rr_pair_template* tmpl, const rr_pair_s
                         npairs, chi2, coeff, penalty, status);
   if (rc || npairs == 0) return rc;
   if (!dchi2_dz || !d2chi2_dz2 || (dchi2_dflux && !sw)) return RR_EINVAL;
+  if (tmpl->method != RR_SOLVE_PCA) return RR_ENOTSUP;
   if (tmpl->prior && dchi2_dflux) return RR_ENOTSUP;
   p.dchi2_dz = dchi2_dz;
   p.d2chi2_dz2 = d2chi2_dz2;

@@ -616,9 +616,11 @@ def pair_ranges_ok(src, layout, z):
     return ok
 
 
-def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
+def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None, bounds=None):
     """chi2 (n,), coeff (n, nbasis), penalty (n,) device tensors for the
-    pairs (target index into the packed targets, redshift)."""
+    pairs (target index into the packed targets, redshift).  ``bounds``:
+    (lower, upper) per basis for a BVLS template (redrock's
+    solver_args['bounds']); None is unbounded."""
     L = _lib.lib()
     dev = device()
     n = len(pair_z)
@@ -632,8 +634,12 @@ def run_pairs(rowpack, src, pair_target, pair_z, stream=None, status=None):
     dz = to_device(np.asarray(pair_z, dtype=np.float64))
     oii = src.oii_dev
     prior = None if getattr(src, "prior", None) is None else to_device(src.prior)
+    hb = None
+    if bounds is not None:
+        hb = np.ascontiguousarray(np.broadcast_to(np.asarray(bounds, dtype=np.float64), (2, nb)))
     tm = _lib.PairTemplate(ptr(src.x), src.nx, ptr(src.y), nb, src.igm, src.method, 0,
-                           ptr(prior), ptr(oii))
+                           ptr(prior), ptr(oii),
+                           None if hb is None else hb.ctypes.data_as(ctypes.c_void_p))
     segs = (_lib.PairSegment * len(rowpack.segments))(*rowpack.segments)
     st = status or StatusWord(dev)
     rc = L.rr_zscan_pairs(ctypes.byref(tm), segs, len(rowpack.segments), ptr(rowpack.rows),

@@ -7,12 +7,12 @@ between its neighbours, fit a parabola to the three points around the best
 one, fit the template once more at the parabola minimum, set ZWARN bits, and
 return the results sorted by chi2.
 
-All chi2 evaluations of PCA templates run in the pair-scan kernel
-(``rr_zscan_pairs``): one launch per template evaluates the fine grids of
-every target's candidate minima (each target at its own redshifts), and one
-more launch does the single-z fits at the parabola minima.  Templates with a
-bounded solve (NMF / NNLS / BVLS) take redrock's own sequence per target on
-the GPU instead: rebin, IGM, and the plain chain with the device solvers.  The sequential candidate logic is
+All chi2 evaluations run in the pair-scan kernel (``rr_zscan_pairs``): one
+launch per template evaluates the fine grids of every target's candidate
+minima (each target at its own redshifts), and one more launch does the
+single-z fits at the parabola minima.  Templates with a bounded solve (NMF /
+NNLS / BVLS) use the same launches with the kernel's bounded solvers and
+the direct-residual chi2 of calc_zchi2_batch.  The sequential candidate logic is
 replayed on the host with the precomputed fine grids (candidates beyond the
 first batch are fetched in further launches only for targets that need
 them), so the decisions are redrock's.
@@ -197,60 +197,6 @@ class _Refiner:
         return chi2, coeff, pen, ok
 
 
-class _PlainRefiner:
-    """The same scan interface for templates with a bounded solve (NMF /
-    NNLS / BVLS): per target, redrock's own sequence on the GPU -- the
-    template rebinned at the target's redshifts (rr_trapz_rebin), times the
-    IGM transmission, then calc_zchi2_batch's plain chain with the
-    template's solver (fitz.py:218-258)."""
-
-    def __init__(self, targets, template, layout=None):
-        if layout is None:
-            dwave = {}
-            for t in targets:
-                for s in t.spectra:
-                    dwave.setdefault(s.wavehash, s.wave)
-            layout = GridLayout.from_dwave(dwave)
-        self.layout = layout
-        self.targets = targets
-        self.template = template
-        self.src = TemplateSource.from_template(template)
-        self.oii = getattr(template, "OIItemplate", None)
-
-    def scan(self, tidx, z):
-        from .igm import transmission_Lyman
-        from .rebin import rebin_template
-        from .zscan import calc_negOII_penalty, calc_zchi2_batch, spectral_data
-        z = np.asarray(z, dtype=np.float64)
-        tidx = np.asarray(tidx, dtype=np.int32)
-        ok = pair_ranges_ok(self.src, self.layout, z)
-        nb = self.template.nbasis
-        chi2 = np.full(len(z), np.nan)
-        pen = np.zeros(len(z))
-        coeff = np.full((len(z), nb), np.nan)
-        for j in np.unique(tidx):
-            sel = np.nonzero((tidx == j) & ok)[0]
-            if not len(sel):
-                continue
-            t = self.targets[j]
-            dwave = {s.wavehash: s.wave for s in t.spectra}
-            zs = z[sel]
-            binned = rebin_template(self.template, zs, dwave, use_gpu=True)
-            for k, wv in dwave.items():
-                T = transmission_Lyman(zs, wv, use_gpu=True, always_return_array=False,
-                                       model=self.template.igm_model)
-                if T is not None:
-                    binned[k] = binned[k] * T.reshape(len(zs), -1)[:, :, None]
-            w, f, wf = spectral_data(t.spectra)
-            c2, co = calc_zchi2_batch(t.spectra, binned, w, f, wf, len(zs), nb,
-                                      solve_matrices_algorithm=self.template.solve_matrices_algorithm)
-            chi2[sel] = c2
-            coeff[sel] = co
-            if self.oii is not None:
-                pen[sel] = calc_negOII_penalty(self.oii, co)
-        return chi2, coeff, pen, ok
-
-
 class PrecomputedFine:
     """Host copies of device-evaluated fitz candidates for one template
     (rr_fitz_candidates + one rr_zscan_pairs launch over their fine grids):
@@ -295,12 +241,10 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     redshifts = np.asarray(redshifts)
     nz = 15 if zminfit_npoints is None else zminfit_npoints
     maxv = MAX_VELO_DIFF_STAR if template.template_type == 'STAR' else MAX_VELO_DIFF
-    if solve_code(template) in (_lib.RR_SOLVE_NNLS, _lib.RR_SOLVE_BVLS):
-        if refine == "newton":
-            raise NotImplementedError("Newton refinement needs the PCA pair kernel")
-        ref = _PlainRefiner(targets, template, layout)
-    else:
-        ref = _Refiner(targets, template, layout, rowpack)
+    if refine == "newton" and solve_code(template) != _lib.RR_SOLVE_PCA:
+        raise NotImplementedError("Newton refinement needs a PCA template (the adjoint of a "
+                                  "bounded solve is not implemented)")
+    ref = _Refiner(targets, template, layout, rowpack)
     has_oii = ref.oii is not None
 
     ntg = len(targets)

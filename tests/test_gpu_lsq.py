@@ -87,8 +87,9 @@ def test_nmf_template_scan_vs_redrock():
 
 def test_nmf_template_fitz_vs_redrock():
     """fitz on the NMF template's coarse scan: the fine grids and the fits at
-    the parabola minima through rebin + IGM + the plain chain with NNLS, as
-    redrock's fitz does.  z |dz| <= 1e-7, ZWARN identical, chi2 |d| <= 1e-3,
+    the parabola minima in batched pair launches with the kernel's NNLS (the
+    template rebinned per pair, chi2 the direct residual), against redrock's
+    fitz (rebin + IGM + calc_zchi2_batch per minimum).  z |dz| <= 1e-7, ZWARN identical, chi2 |d| <= 1e-3,
     coefficients |dc| <= 1e-5 max|c|."""
     from redrock_b200 import fitz, targets as T, templates as TM
     g = np.load(GOLDEN)
@@ -110,3 +111,42 @@ def test_nmf_template_fitz_vs_redrock():
         assert np.max(np.abs(r["chi2"] - gz["chi2"])) <= 1e-3
         scale = np.maximum(np.abs(gz["coeff"]).max(axis=-1, keepdims=True), 1e-300)
         assert np.all(np.abs(r["coeff"] - gz["coeff"]) <= 1e-5 * scale)
+
+
+def test_pair_scan_bounded_solves_vs_redrock():
+    """rr_zscan_pairs with NNLS and BVLS (bounded and free): every (target,
+    redshift) pair of the fixture in one launch per method, each pair's
+    template rebinned inside the kernel, against redrock's calc_zchi2_batch
+    at the same redshifts; same bars and active sets as the plain chain."""
+    from redrock_b200 import targets as T
+    from redrock_b200 import templates as TM
+    from redrock_b200.adjoint import PairContext
+    from redrock_b200.engine import TemplateSource, run_pairs
+    g = np.load(GOLDEN)
+    tg = synth.make_targets(2, seed=11, amp=1.0)
+    gal = synth.template_set()[0]
+    zb = g["lsq_z"]
+    nb = gal.flux.shape[0]
+    lo, hi = g["lsq_bounds"]
+    rt = T.from_synth(tg)
+    tm = TM.Template(spectype="GALAXY", subtype="NMF", redshifts=zb, wave=gal.wave, flux=gal.flux,
+                     method="NMF", igm_model=gal.igm_model)
+    ctx = PairContext(rt, tm)
+    pt = np.repeat(np.arange(len(rt), dtype=np.int32), len(zb))
+    pz = np.tile(zb, len(rt))
+    for name, alg, bounds in (("nnls", "NNLS", None),
+                              ("bvls", "BVLS", (np.full(nb, lo), np.full(nb, hi))),
+                              ("bvls_free", "BVLS", None)):
+        src = TemplateSource(gal.wave, gal.flux, zb, gal.igm_model, method=TM.solve_code_of(alg))
+        c2, co, pe = run_pairs(ctx.rows, src, pt, pz, bounds=bounds)
+        c2 = c2.cpu().numpy().reshape(len(rt), len(zb))
+        co = co.cpu().numpy().reshape(len(rt), len(zb), nb)
+        for it in range(len(rt)):
+            gz, gc = g[f"lsq_{name}_{it}_zchi2"], g[f"lsq_{name}_{it}_zcoeff"]
+            _close(c2[it], co[it], gz, gc)
+            if name == "nnls":
+                np.testing.assert_array_equal(co[it] == 0, gc == 0)
+            if name == "bvls":
+                np.testing.assert_array_equal(np.abs(np.abs(co[it]) - hi) < 1e-9,
+                                              np.abs(np.abs(gc) - hi) < 1e-9)
+        assert not np.any(pe.cpu().numpy())
