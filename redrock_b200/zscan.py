@@ -30,7 +30,7 @@ import torch
 from . import _lib
 from .device import to_device, to_numpy
 from .engine import (DeviceBasis, GridLayout, IdCache, PlainTarget, ScanResult, TargetBatch,
-                     TargetPack, run_fused, run_plain)
+                     TargetPack, resolve_y, run_fused, run_plain)
 from .templates import oii_sums, solve_code, solve_code_of
 
 HUGE_CHI2 = 9999999.0
@@ -141,6 +141,7 @@ def _chunk_bounds(n, chunk):
 
 
 _side_streams = {}
+_lane_streams = {}
 
 
 def _side_stream():
@@ -148,6 +149,13 @@ def _side_stream():
     if d not in _side_streams:
         _side_streams[d] = torch.cuda.Stream()
     return _side_streams[d]
+
+
+def _lane_stream():
+    d = torch.cuda.current_device()
+    if d not in _lane_streams:
+        _lane_streams[d] = torch.cuda.Stream()
+    return _lane_streams[d]
 
 
 class HostResult:
@@ -204,10 +212,11 @@ _copy_streams = {}
 def _pack_overlapped(sub, layout, st, main):
     """TargetPack of one chunk whose host-to-device copies run on a copy
     stream, so that they overlap the previous chunk's scan instead of
-    queueing behind it on the main stream; the pack kernel waits for them.
-    The copy stream does not wait for the main stream: its buffers are new
-    allocations, and record_stream keeps them from reuse until the main
-    stream's kernels that read them are done."""
+    queueing behind it on the chunk's compute stream ``main``; the pack
+    kernel (launched on ``main``) waits for them.  The copy stream does not
+    wait for ``main``: its buffers are new allocations, and record_stream
+    keeps them from reuse until the kernels on ``main`` that read them are
+    done."""
     d = torch.cuda.current_device()
     if d not in _copy_streams:
         _copy_streams[d] = torch.cuda.Stream()
@@ -294,26 +303,45 @@ def _scan_device(targets, dtemplates, chunk=None, host=False, on_host_ready=None
     st = StatusWord()
     bounds = _chunk_bounds(len(targets), chunk)
     main = torch.cuda.current_stream()
+    # consecutive chunks alternate between two compute streams, so that a
+    # chunk's packing, y GEMMs and first scan launch need not wait for the
+    # previous chunk's last tiles: its CTAs take the SMs that the other
+    # chunk's last tile wave leaves idle (each chunk has its own outputs,
+    # tile counters and scratch, allocated on its own stream)
+    lanes = [main] if len(bounds) == 1 else [main, _lane_stream()]
+    if len(lanes) > 1:
+        # what the chunks share is made on main first: the bases and their
+        # INT8 digit planes for the y GEMM (cached on each basis)
+        if resolve_y(None, layout) == "int8x7":
+            kpad = int(_lib.lib().rr_ygemm_kpad(layout.pix_stride))
+            for b in bases:
+                b.i8_digits(kpad)
+        ev0 = torch.cuda.Event()
+        ev0.record(main)
+        lanes[1].wait_event(ev0)
     side = _side_stream() if host else None
     hout = [HostResult(len(targets), b) for b in bases] if host else None
     parts = []
     keep = []
-    for i0, i1 in bounds:
+    for k, (i0, i1) in enumerate(bounds):
         sub = targets[i0:i1]
-        if len(bounds) == 1:
-            pack = _pack(sub, layout)
-        else:
-            pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
-                                   lambda: _pack_overlapped(sub, layout, st, main))
-        tiles = None
-        if AUTOTUNE:
-            from . import autotune
-            tiles = autotune.tiles_of(autotune.choice(pack, bases) or autotune.tune(pack, bases))
-        res, _ = run_fused(pack, bases, status=st, tiles=tiles)
+        cs = lanes[k % len(lanes)]
+        with torch.cuda.stream(cs):
+            if len(bounds) == 1:
+                pack = _pack(sub, layout)
+            else:
+                pack = _pack_cache.get(("chunk", layout.signature, i0, len(sub)), sub,
+                                       lambda: _pack_overlapped(sub, layout, st, cs))
+            tiles = None
+            if AUTOTUNE:
+                from . import autotune
+                tiles = autotune.tiles_of(autotune.choice(pack, bases)
+                                          or autotune.tune(pack, bases))
+            res, _ = run_fused(pack, bases, status=st, tiles=tiles)
         keep.append((pack, res))
         if host:
             ev = torch.cuda.Event()
-            ev.record(main)
+            ev.record(cs)
             side.wait_event(ev)
             with torch.cuda.stream(side):
                 for h, r in zip(hout, res):
@@ -323,6 +351,16 @@ def _scan_device(targets, dtemplates, chunk=None, host=False, on_host_ready=None
                 on_host_ready(hout)
         else:
             parts.append(res)
+    if len(lanes) > 1:
+        ev1 = torch.cuda.Event()
+        ev1.record(lanes[1])
+        main.wait_event(ev1)
+        # device results of the lane's chunks are read on main from here on
+        for k, (_, res) in enumerate(keep):
+            if k % 2:
+                for r in res:
+                    for t in (r.zchi2, r.zcoeff, r.penalty):
+                        t.record_stream(main)
     main.synchronize()
     if host:
         side.synchronize()
