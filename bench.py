@@ -220,6 +220,10 @@ def run_ours(args, rank, world, local_rank):
                                        zsub=args.zsub, workload=args.workload)
     evals, flops, y_flops = evals_and_flops(rtg, tms)
     layout = GridLayout.from_dwave(synth.camera_grids())
+    if args.ygemm is None:
+        # the engine's own choice for this layout (what the public API runs)
+        from redrock_b200.engine import resolve_y
+        args.ygemm = resolve_y(None, layout)
     srcs = [TemplateSource.from_template(tm) for tm in tms]
     dbatch = TargetBatch(rtg, layout).to_device()
     bases_gb = sum(len(tm.redshifts) * layout.pix_stride * (tm.nbasis + tm.nbasis % 2) * 8
@@ -281,7 +285,7 @@ def run_ours(args, rank, world, local_rank):
     groups = {0 if tm.nbasis == 10 else 1 if tm.nbasis == 4 else 2 if tm.nbasis == 5 else 3
               for tm in tms}
     launches_per_step = sum(len(layout.keys) for _ in srcs) + 2 + len(groups)
-    if args.ygemm == "int8x7":
+    if args.ygemm in ("int8x7", "int8x6"):
         # rr_pack_g, rr_slice_g_i8; per template rr_basis_col_exp,
         # rr_slice_basis_i8, rr_ygemm_i8
         launches_per_step += 2 + 3 * len(srcs)
@@ -606,13 +610,13 @@ def archetype_study(tg, rtg, torch, narch=24):
 
 def ygemm_study(args, step, torch, evals):
     """Throughput and zchi2/zcoeff error of each y variant (FP64 in the
-    scan, or the tensor-core GEMM in bf16x3 / tf32x3 / int8x7), errors
+    scan, or the tensor-core GEMM in bf16x3 / tf32x3 / int8x7 / int8x6), errors
     against the FP64 path on the same workload."""
     huge = 9999999.0
     out = {}
     ref = None
     fwf = None
-    for v in ["fp64", "bf16x3", "tf32x3", "int8x7"]:
+    for v in ["fp64", "bf16x3", "tf32x3", "int8x7", "int8x6"]:
         step(False, ygemm=v)
         torch.cuda.synchronize()
         ev = []
@@ -878,9 +882,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=8,
                     help="end-to-end steps timed (at most --steps)")
-    ap.add_argument("--ygemm", default="int8x7", choices=["fp64", "bf16x3", "tf32x3", "int8x7"],
-                    help="y = Tb^T W f as a tensor-core GEMM (int8x7: exact, the default) or "
-                         "summed in the FP64 scan (fp64)")
+    ap.add_argument("--ygemm", default=None,
+                    choices=["fp64", "bf16x3", "tf32x3", "int8x7", "int8x6"],
+                    help="y = Tb^T W f as a tensor-core GEMM (int8x7 / int8x6: exact; the "
+                         "engine's default when not given) or summed in the FP64 scan (fp64)")
     ap.add_argument("--archetypes", action="store_true",
                     help="also time batched archetype refits of every target (24 archetypes)")
     ap.add_argument("--adjoint", action="store_true",

@@ -428,31 +428,37 @@ int rr_negoii_penalty(const double* coeff, int64_t nz, int32_t nbasis, const dou
  *                    power of two and rounded to a 49-bit integer of seven
  *                    base-128 digits; the 28 digit products of order <= 6
  *                    accumulate exactly in int32 and combine in FP64
- *                    (error <= K 2^-45 2^(e_t + e_n) per output)
+ *                    (error <= K 2^-45 2^(e_t + e_n) per output); K <= 65536
+ *   RR_YGEMM_INT8X6  the same with six base-256 digits of a 48-bit integer
+ *                    (|X| <= 127 2^40): 21 products of order <= 5, 80 output
+ *                    columns per tile instead of 64 (error <= K 2^-44
+ *                    2^(e_t + e_n)); K <= 21824
  * Flow: rr_pack_targets -> rr_pack_g (G, row_exp) -> per template
  *   BF16X3 / TF32X3: rr_ygemm
- *   INT8X7: rr_slice_g_i8 (once per target pack), rr_basis_col_exp +
- *           rr_slice_basis_i8 (once per basis), rr_ygemm_i8
+ *   INT8X7 / INT8X6: rr_slice_g_i8 (once per target pack), rr_basis_col_exp
+ *           + rr_slice_basis_i8 (once per basis), rr_ygemm_i8
  * -> rr_zscan_fused with y_ext = Y.
  * ---------------------------------------------------------------------- */
 enum rr_ygemm_variant {
   RR_YGEMM_NONE = 0,   /* y summed in FP64 inside the scan (default) */
   RR_YGEMM_BF16X3 = 1,
   RR_YGEMM_TF32X3 = 2,
-  RR_YGEMM_INT8X7 = 3
+  RR_YGEMM_INT8X7 = 3,
+  RR_YGEMM_INT8X6 = 4
 };
 
 /* padded pixel count (rows of G) for a basis of pix_stride rows */
 int64_t rr_ygemm_kpad(int64_t pix_stride);
 
 /* G[kpad][npos] (row q = padded basis pixel, column = block * 32 + lane)
- * and row_exp[npos] (biased power-of-two exponents of each column's max,
- * or NULL).  npos: a multiple of 128, >= nblock * 32.  The call zeroes G
+ * and row_exp[npos] (biased power-of-two exponents e of each column with
+ * max |G| < 127/128 2^e <= 2 max |G|, or NULL).  npos: a multiple of 128, >= nblock * 32.  The call zeroes G
  * and row_exp first. */
 int rr_pack_g(const rr_scan_targets* targets, int64_t pix_stride, int64_t kpad, int64_t npos,
               double* g, int* row_exp, int* status, rr_stream_t stream);
 
-/* col_exp[nz * nbasis]: biased exponent of max_q |basis[z][q][i]| */
+/* col_exp[nz * nbasis]: biased exponent e of max_q |basis[z][q][i]| with
+ * the same 127/128 margin */
 int rr_basis_col_exp(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
                      int basis_stride, int* col_exp, rr_stream_t stream);
 
@@ -461,20 +467,23 @@ int rr_ygemm(int variant, const double* g, int64_t npos, int64_t kpad, const dou
              int64_t nz, int64_t pix_stride, int nbasis, int basis_stride, double* y,
              int* status, rr_stream_t stream);
 
-/* RR_YGEMM_INT8X7: digit planes of G and of a basis, laid out as the
- * GEMM's shared-memory tiles (16-byte aligned buffers of the sizes
- * returned by the _bytes queries, -1 for invalid arguments) */
-int64_t rr_ygemm_i8_g_bytes(int64_t npos, int64_t kpad);
-int64_t rr_ygemm_i8_basis_bytes(int64_t nz, int nbasis, int64_t kpad);
-int rr_slice_g_i8(const double* g, const int* row_exp, int64_t npos, int64_t kpad,
+/* RR_YGEMM_INT8X7 / RR_YGEMM_INT8X6 (variant): digit planes of G and of a
+ * basis, laid out as the GEMM's shared-memory tiles (16-byte aligned
+ * buffers of the sizes returned by the _bytes queries, -1 for invalid
+ * arguments); digits and GEMM must use the same variant */
+int64_t rr_ygemm_i8_g_bytes(int variant, int64_t npos, int64_t kpad);
+int64_t rr_ygemm_i8_basis_bytes(int variant, int64_t nz, int nbasis, int64_t kpad);
+/* largest kpad whose int32 accumulation stays exact (-1: not an INT8 variant) */
+int64_t rr_ygemm_i8_max_kpad(int variant);
+int rr_slice_g_i8(int variant, const double* g, const int* row_exp, int64_t npos, int64_t kpad,
                   void* g_digits, rr_stream_t stream);
-int rr_slice_basis_i8(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
-                      int basis_stride, int64_t kpad, const int* col_exp, void* basis_digits,
-                      rr_stream_t stream);
-/* y[npos][nz][nbasis]; RR_ENOTSUP when kpad > 65536 (int32 headroom) */
-int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t kpad,
-                const void* basis_digits, const int* col_exp, int64_t nz, int nbasis,
-                double* y, int* status, rr_stream_t stream);
+int rr_slice_basis_i8(int variant, const double* basis, int64_t nz, int64_t pix_stride,
+                      int nbasis, int basis_stride, int64_t kpad, const int* col_exp,
+                      void* basis_digits, rr_stream_t stream);
+/* y[npos][nz][nbasis]; RR_ENOTSUP when kpad > rr_ygemm_i8_max_kpad(variant) */
+int rr_ygemm_i8(int variant, const void* g_digits, const int* row_exp, int64_t npos,
+                int64_t kpad, const void* basis_digits, const int* col_exp, int64_t nz,
+                int nbasis, double* y, int* status, rr_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Coadd of a target's exposures per wavelength grid (targets.py:267-373,

@@ -16,9 +16,10 @@ LIBPATH = os.path.join(HERE, "librr_b200.so")
 RR_OK, RR_EINVAL, RR_ERANGE, RR_ECUDA, RR_ETIMEOUT, RR_ENOTSUP, RR_ESCRATCH = range(7)
 RR_IGM_NONE, RR_IGM_CALURA12, RR_IGM_KAMBLE20, RR_IGM_INOUE14 = range(4)
 RR_SOLVE_PCA, RR_SOLVE_UNSUPPORTED, RR_SOLVE_NNLS, RR_SOLVE_BVLS = 0, 1, 2, 3
-RR_YGEMM_NONE, RR_YGEMM_BF16X3, RR_YGEMM_TF32X3, RR_YGEMM_INT8X7 = range(4)
+RR_YGEMM_NONE, RR_YGEMM_BF16X3, RR_YGEMM_TF32X3, RR_YGEMM_INT8X7, RR_YGEMM_INT8X6 = range(5)
 YGEMM_VARIANTS = {"fp64": RR_YGEMM_NONE, "bf16x3": RR_YGEMM_BF16X3, "tf32x3": RR_YGEMM_TF32X3,
-                  "int8x7": RR_YGEMM_INT8X7}
+                  "int8x7": RR_YGEMM_INT8X7, "int8x6": RR_YGEMM_INT8X6}
+I8_VARIANTS = (RR_YGEMM_INT8X7, RR_YGEMM_INT8X6)
 HALF_BAND = 5
 LANES = 32
 RW = 12
@@ -169,13 +170,14 @@ _SIGNATURES = {
     "rr_basis_col_exp": (c_int, [c_void_p, c_int64, c_int64, c_int, c_int, c_void_p, c_void_p]),
     "rr_ygemm": (c_int, [c_int, c_void_p, c_int64, c_int64, c_void_p, c_int64, c_int64, c_int,
                          c_int, c_void_p, c_void_p, c_void_p]),
-    "rr_ygemm_i8_g_bytes": (c_int64, [c_int64, c_int64]),
-    "rr_ygemm_i8_basis_bytes": (c_int64, [c_int64, c_int, c_int64]),
-    "rr_slice_g_i8": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
-    "rr_slice_basis_i8": (c_int, [c_void_p, c_int64, c_int64, c_int, c_int, c_int64, c_void_p,
-                                  c_void_p, c_void_p]),
-    "rr_ygemm_i8": (c_int, [c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_int64,
-                            c_int, c_void_p, c_void_p, c_void_p]),
+    "rr_ygemm_i8_g_bytes": (c_int64, [c_int, c_int64, c_int64]),
+    "rr_ygemm_i8_basis_bytes": (c_int64, [c_int, c_int64, c_int, c_int64]),
+    "rr_ygemm_i8_max_kpad": (c_int64, [c_int]),
+    "rr_slice_g_i8": (c_int, [c_int, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p]),
+    "rr_slice_basis_i8": (c_int, [c_int, c_void_p, c_int64, c_int64, c_int, c_int, c_int64,
+                                  c_void_p, c_void_p, c_void_p]),
+    "rr_ygemm_i8": (c_int, [c_int, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_void_p,
+                            c_int64, c_int, c_void_p, c_void_p, c_void_p]),
 }
 
 

@@ -44,6 +44,7 @@ constexpr int kTileM = 128;  // targets per tile (MMA M)
 constexpr int kThreads = 256;
 constexpr int kKpadAlign = 64;  // G rows padded to a multiple of every stage depth
 constexpr int kExpBias = 4096;  // stored exponents are biased; 0 = all-zero row/column
+constexpr double kExpMargin = 128.0 / 127.0;  // exponents bound max |x| by 127/128 2^e
 
 // ---------------------------------------------------------------------------
 // tcgen05 / descriptor helpers
@@ -381,58 +382,95 @@ static int launch_ygemm(YParams p, cudaStream_t stream) {
 // INT8X7: pre-sliced operands, exact integer accumulation
 // ===========================================================================
 namespace i8 {
-constexpr int kDigits = 7;
 constexpr int kKt = 32;                    // pixels per stage = one MMA K step
 constexpr int kNkg = kKt / 16;             // 2 core matrices along K
 constexpr int kSbo = kNkg * 128;           // 256 B between 8-row groups
-constexpr int kN = 64;                     // MMA N: 7 accumulators x 64 columns <= 512
-#ifndef RR_I8_STAGES
-#define RR_I8_STAGES 4
-#endif
-constexpr int kStages = RR_I8_STAGES;  // copy pipeline depth (43 KB per stage)
 constexpr int kASlice = kTileM * kKt;      // bytes of one digit plane of a G block
-constexpr int kBSlice = kN * kKt;
-constexpr int kABlock = kDigits * kASlice;  // 28672 B per (target tile, chunk)
-constexpr int kBBlock = kDigits * kBSlice;  // 14336 B per (z tile, chunk)
-constexpr int kStageBytes = kABlock + kBBlock;
 constexpr uint32_t kFmt = (2u << 4) | (1u << 7) | (1u << 10);  // D s32, A/B signed 8-bit
 
-__host__ __device__ constexpr int zt_of(int nbasis) { return kN / nbasis; }
+// The two digit schemes (rr_ygemm_variant):
+//   INT8X7: X = rint(x 2^(48 - e)), seven balanced base-128 digits, the 28
+//           products of order <= 6 -> 7 int32 accumulators of N = 64
+//           columns; |digit| <= 64, so K <= 65536 keeps them exact.
+//   INT8X6: X = rint(x 2^(47 - e)), six balanced base-256 digits, the 21
+//           products of order <= 5 -> 6 accumulators of N = 80 columns
+//           (480 of the 512 TMEM columns); |digit| <= 128, so K <= 21845.
+// e is the column's exponent with a 128/127 margin (max |x| < 127/128 2^e),
+// which keeps the leading base-256 digit within int8: |X| <= 127 2^40.
+// Y = sum_d acc_d 2^(-bits d) 2^(e_t + e_n + shift), shift = 2 bits
+// (digits - 1) - 2 mant.
+template <int V>
+struct Scheme;
+template <>
+struct Scheme<RR_YGEMM_INT8X7> {
+  static constexpr int kDigits = 7, kBits = 7, kMant = 48, kN = 64, kStages = 4;
+  static constexpr int64_t kMaxK = 65536;
+};
+template <>
+struct Scheme<RR_YGEMM_INT8X6> {
+  static constexpr int kDigits = 6, kBits = 8, kMant = 47, kN = 80, kStages = 5;
+  static constexpr int64_t kMaxK = 21824;  // 6 * 128^2 * K < 2^31, K a multiple of 64
+};
+template <int V>
+struct Tile {
+  using S = Scheme<V>;
+  static constexpr int kBSlice = S::kN * kKt;
+  static constexpr int kABlock = S::kDigits * kASlice;  // bytes per (target tile, chunk)
+  static constexpr int kBBlock = S::kDigits * kBSlice;  // bytes per (z tile, chunk)
+  static constexpr int kStageBytes = kABlock + kBBlock;
+  static constexpr int kShift = 2 * S::kBits * (S::kDigits - 1) - 2 * S::kMant;
+  static_assert(S::kDigits * S::kN <= 512, "accumulators exceed TMEM");
+  static_assert(S::kN % 16 == 0 && (S::kN / 2) % 8 == 0, "MMA N / epilogue split");
+};
 
-// Base-128 digits of X = rint(x 2^(48 - e)), |x| < 2^e, so |X| < 2^48 and
-// X = sum_k a_k 128^(6 - k): six balanced low digits in [-64, 63] and a
-// leading digit |a_0| <= 64.  One FP64 -> int64 conversion; the digits are
-// integer shifts and masks.  Digit k of element j goes to byte j of plane k.
+__host__ __device__ constexpr int zt_of(int v, int nbasis) {
+  return (v == RR_YGEMM_INT8X6 ? Scheme<RR_YGEMM_INT8X6>::kN : Scheme<RR_YGEMM_INT8X7>::kN) /
+         nbasis;
+}
+__host__ __device__ constexpr bool is_i8(int v) {
+  return v == RR_YGEMM_INT8X7 || v == RR_YGEMM_INT8X6;
+}
+
+// Balanced digits of X = rint(x 2^(mant - e)): kDigits - 1 low digits in
+// [-base/2, base/2 - 1] and the leading digit (|a_0| <= 64 for INT8X7,
+// <= 127 for INT8X6 under the exponent margin).  One FP64 -> int64
+// conversion; the digits are integer shifts and masks.  Digit k of element
+// j goes to byte j of plane k.
+template <int V>
 __device__ __forceinline__ void digits16(const double (&v)[16], int e, unsigned char* dst,
                                          int plane_bytes) {
-  // 2^(48 - e) as two factors so that neither overflows for tiny columns
-  const int sh = 48 - e;
+  using S = Scheme<V>;
+  constexpr long long kHalf = 1ll << (S::kBits - 1);
+  constexpr long long kMask = (1ll << S::kBits) - 1;
+  // 2^(mant - e) as two factors so that neither overflows for tiny columns
+  const int sh = S::kMant - e;
   const double f1 = ldexp(1.0, sh / 2), f2 = ldexp(1.0, sh - sh / 2);
-  uint32_t w[kDigits][4];
+  uint32_t w[S::kDigits][4];
 #pragma unroll
-  for (int k = 0; k < kDigits; ++k)
+  for (int k = 0; k < S::kDigits; ++k)
 #pragma unroll
     for (int j = 0; j < 4; ++j) w[k][j] = 0;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     long long x = __double2ll_rn((v[j] * f1) * f2);
 #pragma unroll
-    for (int k = kDigits - 1; k >= 1; --k) {
-      const long long a = ((x + 64) & 127) - 64;  // in [-64, 63]
-      x = (x - a) >> 7;                           // exact: x - a is a multiple of 128
+    for (int k = S::kDigits - 1; k >= 1; --k) {
+      const long long a = ((x + kHalf) & kMask) - kHalf;
+      x = (x - a) >> S::kBits;  // exact: x - a is a multiple of the base
       w[k][j >> 2] |= ((uint32_t)a & 0xFFu) << (8 * (j & 3));
     }
-    // the rest is the leading digit: |X| < 2^48 and the six lower digits sum
-    // to within (-0.504, 0.496) 128^6, so |x| <= 64 (no wrap here, which
-    // would drop a carry)
+    // the rest is the leading digit: the low digits sum to within about
+    // +-base^(digits-1) / 2, so it stays inside int8 (no wrap, which would
+    // drop a carry)
     w[0][j >> 2] |= ((uint32_t)x & 0xFFu) << (8 * (j & 3));
   }
 #pragma unroll
-  for (int k = 0; k < kDigits; ++k)
+  for (int k = 0; k < S::kDigits; ++k)
     *reinterpret_cast<uint4*>(dst + k * plane_bytes) = make_uint4(w[k][0], w[k][1], w[k][2], w[k][3]);
 }
 
 // G digits: one block per (target tile, chunk), one thread per unit
+template <int V>
 __global__ void __launch_bounds__(256) slice_g_kernel(const double* __restrict__ g,
                                                       const int* __restrict__ row_exp,
                                                       int64_t npos, int64_t nchunk,
@@ -447,14 +485,16 @@ __global__ void __launch_bounds__(256) slice_g_kernel(const double* __restrict__
   double v[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) v[j] = __ldg(src + (int64_t)j * npos);
-  digits16(v, unbias(row_exp[t]), out + (tile * nchunk + c) * kABlock + u * 16, kASlice);
+  digits16<V>(v, unbias(row_exp[t]), out + (tile * nchunk + c) * Tile<V>::kABlock + u * 16,
+              kASlice);
 }
 
 // basis digits: one block per (z tile, chunk), one thread per unit
-__global__ void __launch_bounds__(128) slice_basis_kernel(
+template <int V>
+__global__ void __launch_bounds__(Scheme<V>::kN * kNkg) slice_basis_kernel(
     const double* __restrict__ basis, int nz, int64_t pix_stride, int nbasis, int basis_stride,
     const int* __restrict__ col_exp, int64_t nchunk, unsigned char* __restrict__ out) {
-  const int zt = zt_of(nbasis);
+  const int zt = zt_of(V, nbasis);
   const int64_t tile = blockIdx.x;
   const int64_t c = blockIdx.y;
   const int u = threadIdx.x;  // < kN * kNkg
@@ -477,7 +517,7 @@ __global__ void __launch_bounds__(128) slice_basis_kernel(
 #pragma unroll
     for (int j = 0; j < 16; ++j) v[j] = 0.0;
   }
-  digits16(v, e, out + (tile * nchunk + c) * kBBlock + u * 16, kBSlice);
+  digits16<V>(v, e, out + (tile * nchunk + c) * Tile<V>::kBBlock + u * 16, Tile<V>::kBSlice);
 }
 
 struct Params {
@@ -493,7 +533,12 @@ struct Params {
 
 // grid (npos / 128, ztiles), 256 threads: thread 0 streams the digit blocks
 // (1-D bulk copies), thread 32 issues the MMAs, all eight warps read TMEM.
+template <int V>
 __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constant__ Params p) {
+  using S = Scheme<V>;
+  using Gm = Tile<V>;
+  constexpr int kStages = S::kStages;
+  constexpr int kN = S::kN;
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
@@ -539,13 +584,14 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
         s_fail = 1;
         break;
       }
-      unsigned char* st = sm + s * kStageBytes;
-      mbar_arrive_expect_tx(&full[s], kStageBytes);
-      bulk_g2s(st, p.ga + (mt * p.nchunk + c) * kABlock, kABlock, &full[s]);
-      bulk_g2s(st + kABlock, p.tb + (ztile * p.nchunk + c) * kBBlock, kBBlock, &full[s]);
+      unsigned char* st = sm + s * Gm::kStageBytes;
+      mbar_arrive_expect_tx(&full[s], Gm::kStageBytes);
+      bulk_g2s(st, p.ga + (mt * p.nchunk + c) * Gm::kABlock, Gm::kABlock, &full[s]);
+      bulk_g2s(st + Gm::kABlock, p.tb + (ztile * p.nchunk + c) * Gm::kBBlock, Gm::kBBlock,
+               &full[s]);
     }
   } else if (threadIdx.x == 32) {
-    // MMA issuer: digit products (i, j), i + j = d <= 6, into accumulator d
+    // MMA issuer: digit products (i, j), i + j = d < digits, into accumulator d
     const uint32_t idesc = instr_desc(kFmt, kN, kTileM);
     for (int64_t c = 0; c < p.nchunk; ++c) {
       const int s = (int)(c % kStages);
@@ -555,14 +601,14 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
         break;
       }
       tc_fence_after();
-      const uint32_t a0 = smem_u32(sm + s * kStageBytes);
-      const uint32_t b0 = a0 + kABlock;
+      const uint32_t a0 = smem_u32(sm + s * Gm::kStageBytes);
+      const uint32_t b0 = a0 + Gm::kABlock;
 #pragma unroll 1
-      for (int d = 0; d < kDigits; ++d)
+      for (int d = 0; d < S::kDigits; ++d)
 #pragma unroll 1
         for (int i = 0; i <= d; ++i) {
           const uint64_t da = smem_desc(a0 + i * kASlice, kSbo);
-          const uint64_t db = smem_desc(b0 + (d - i) * kBSlice, kSbo);
+          const uint64_t db = smem_desc(b0 + (d - i) * Gm::kBSlice, kSbo);
           mma<kI8>(tmem + d * kN, da, db, idesc, (c > 0 || i > 0) ? 1u : 0u);
         }
       mma_commit(&empty[s]);
@@ -585,18 +631,19 @@ __global__ void __launch_bounds__(kThreads, 1) ygemm_kernel(const __grid_constan
       double out[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) out[j] = 0.0;
-      // X_t X_n = sum_d D_d 128^(12 - d) (d <= 6 kept); smallest terms first
+      // X_t X_n = sum_d acc_d base^(2 (digits - 1) - d); smallest terms first
 #pragma unroll 1
-      for (int d = kDigits - 1; d >= 0; --d) {
+      for (int d = S::kDigits - 1; d >= 0; --d) {
         uint32_t v[8];
         tmem_ld8(tl + d * kN + c0, v);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 8; ++j) out[j] += ldexp((double)(int)v[j], -7 * d);
+        for (int j = 0; j < 8; ++j) out[j] += ldexp((double)(int)v[j], -S::kBits * d);
       }
 #pragma unroll
       for (int j = 0; j < 8; ++j)
-        if (c0 + j < nused) yrow[c0 + j] = ldexp(out[j], s_rexp[row] + s_cexp[c0 + j] - 12);
+        if (c0 + j < nused)
+          yrow[c0 + j] = ldexp(out[j], s_rexp[row] + s_cexp[c0 + j] + Gm::kShift);
     }
   }
   tc_fence_before();
@@ -645,7 +692,9 @@ __global__ void __launch_bounds__(256) pack_g_kernel(const __grid_constant__ GPa
   if (p.row_exp) {
     int e = 0;
     if (acc != 0.0) {
-      frexp(acc, &e);
+      // exponent of |acc| 128/127: max |G| < 127/128 2^e (the digit
+      // schemes' margin)
+      frexp(fabs(acc) * kExpMargin, &e);
       e += kExpBias;
     }
     s_e[threadIdx.y][lane] = e;
@@ -689,7 +738,7 @@ __global__ void __launch_bounds__(256) col_exp_kernel(const double* __restrict__
     int e = 0;
     const double mx = s_m[threadIdx.x][0];
     if (mx > 0.0) {
-      frexp(mx, &e);
+      frexp(mx * kExpMargin, &e);
       e += kExpBias;
     }
     col_exp[z * nbasis + threadIdx.x] = e;
@@ -774,63 +823,107 @@ extern "C" int rr_ygemm(int variant, const double* g, int64_t npos, int64_t kpad
   switch (variant) {
     case RR_YGEMM_BF16X3: return yg::launch_ygemm<RR_YGEMM_BF16X3>(p, st);
     case RR_YGEMM_TF32X3: return yg::launch_ygemm<RR_YGEMM_TF32X3>(p, st);
-    default: return RR_EINVAL;  // RR_YGEMM_INT8X7 runs through rr_ygemm_i8
+    default: return RR_EINVAL;  // the INT8 schemes run through rr_ygemm_i8
   }
 }
 
-extern "C" int64_t rr_ygemm_i8_g_bytes(int64_t npos, int64_t kpad) {
+extern "C" int64_t rr_ygemm_i8_g_bytes(int variant, int64_t npos, int64_t kpad) {
+  if (!yg::i8::is_i8(variant)) return -1;
   if (npos < 0 || kpad < 0 || npos % yg::kTileM || kpad % yg::i8::kKt) return -1;
-  return (npos / yg::kTileM) * (kpad / yg::i8::kKt) * (int64_t)yg::i8::kABlock;
+  const int64_t ablock = variant == RR_YGEMM_INT8X6 ? yg::i8::Tile<RR_YGEMM_INT8X6>::kABlock
+                                                    : yg::i8::Tile<RR_YGEMM_INT8X7>::kABlock;
+  return (npos / yg::kTileM) * (kpad / yg::i8::kKt) * ablock;
 }
 
-extern "C" int64_t rr_ygemm_i8_basis_bytes(int64_t nz, int nbasis, int64_t kpad) {
+extern "C" int64_t rr_ygemm_i8_basis_bytes(int variant, int64_t nz, int nbasis, int64_t kpad) {
+  if (!yg::i8::is_i8(variant)) return -1;
   if (nz < 0 || nbasis < 1 || nbasis > RR_MAX_NBASIS || kpad < 0 || kpad % yg::i8::kKt) return -1;
-  const int zt = yg::i8::zt_of(nbasis);
-  return ((nz + zt - 1) / zt) * (kpad / yg::i8::kKt) * (int64_t)yg::i8::kBBlock;
+  const int zt = yg::i8::zt_of(variant, nbasis);
+  const int64_t bblock = variant == RR_YGEMM_INT8X6 ? yg::i8::Tile<RR_YGEMM_INT8X6>::kBBlock
+                                                    : yg::i8::Tile<RR_YGEMM_INT8X7>::kBBlock;
+  return ((nz + zt - 1) / zt) * (kpad / yg::i8::kKt) * bblock;
 }
 
-extern "C" int rr_slice_g_i8(const double* g, const int* row_exp, int64_t npos, int64_t kpad,
-                             void* g_digits, rr_stream_t stream) {
+extern "C" int64_t rr_ygemm_i8_max_kpad(int variant) {
+  if (variant == RR_YGEMM_INT8X7) return yg::i8::Scheme<RR_YGEMM_INT8X7>::kMaxK;
+  if (variant == RR_YGEMM_INT8X6) return yg::i8::Scheme<RR_YGEMM_INT8X6>::kMaxK;
+  return -1;
+}
+
+extern "C" int rr_slice_g_i8(int variant, const double* g, const int* row_exp, int64_t npos,
+                             int64_t kpad, void* g_digits, rr_stream_t stream) {
+  if (!yg::i8::is_i8(variant)) return RR_EINVAL;
   if (!g || !row_exp || !g_digits || npos < yg::kTileM || npos % yg::kTileM) return RR_EINVAL;
   if (kpad < yg::kKpadAlign || kpad % yg::kKpadAlign || kpad / yg::i8::kKt > 65535) return RR_EINVAL;
   if ((reinterpret_cast<uintptr_t>(g_digits) & 15) != 0) return RR_EINVAL;
   const int64_t nchunk = kpad / yg::i8::kKt;
   dim3 grid((unsigned)(npos / yg::kTileM), (unsigned)nchunk);
-  yg::i8::slice_g_kernel<<<grid, yg::kTileM * yg::i8::kNkg, 0, (cudaStream_t)stream>>>(
-      g, row_exp, npos, nchunk, (unsigned char*)g_digits);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (variant == RR_YGEMM_INT8X6)
+    yg::i8::slice_g_kernel<RR_YGEMM_INT8X6><<<grid, yg::kTileM * yg::i8::kNkg, 0, st>>>(
+        g, row_exp, npos, nchunk, (unsigned char*)g_digits);
+  else
+    yg::i8::slice_g_kernel<RR_YGEMM_INT8X7><<<grid, yg::kTileM * yg::i8::kNkg, 0, st>>>(
+        g, row_exp, npos, nchunk, (unsigned char*)g_digits);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
 
-extern "C" int rr_slice_basis_i8(const double* basis, int64_t nz, int64_t pix_stride, int nbasis,
-                                 int basis_stride, int64_t kpad, const int* col_exp,
+extern "C" int rr_slice_basis_i8(int variant, const double* basis, int64_t nz, int64_t pix_stride,
+                                 int nbasis, int basis_stride, int64_t kpad, const int* col_exp,
                                  void* basis_digits, rr_stream_t stream) {
+  if (!yg::i8::is_i8(variant)) return RR_EINVAL;
   if (!basis || !col_exp || !basis_digits || nz < 0 || nz > INT_MAX || pix_stride < 1)
     return RR_EINVAL;
   if (nbasis < 1 || nbasis > RR_MAX_NBASIS || basis_stride < nbasis) return RR_EINVAL;
   if (kpad < pix_stride || kpad % yg::kKpadAlign || kpad / yg::i8::kKt > 65535) return RR_EINVAL;
   if ((reinterpret_cast<uintptr_t>(basis_digits) & 15) != 0) return RR_EINVAL;
   if (nz == 0) return RR_OK;
-  const int zt = yg::i8::zt_of(nbasis);
+  const int zt = yg::i8::zt_of(variant, nbasis);
   const int64_t nchunk = kpad / yg::i8::kKt;
   dim3 grid((unsigned)((nz + zt - 1) / zt), (unsigned)nchunk);
-  yg::i8::slice_basis_kernel<<<grid, yg::i8::kN * yg::i8::kNkg, 0, (cudaStream_t)stream>>>(
-      basis, (int)nz, pix_stride, nbasis, basis_stride, col_exp, nchunk,
-      (unsigned char*)basis_digits);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (variant == RR_YGEMM_INT8X6)
+    yg::i8::slice_basis_kernel<RR_YGEMM_INT8X6>
+        <<<grid, yg::i8::Scheme<RR_YGEMM_INT8X6>::kN * yg::i8::kNkg, 0, st>>>(
+            basis, (int)nz, pix_stride, nbasis, basis_stride, col_exp, nchunk,
+            (unsigned char*)basis_digits);
+  else
+    yg::i8::slice_basis_kernel<RR_YGEMM_INT8X7>
+        <<<grid, yg::i8::Scheme<RR_YGEMM_INT8X7>::kN * yg::i8::kNkg, 0, st>>>(
+            basis, (int)nz, pix_stride, nbasis, basis_stride, col_exp, nchunk,
+            (unsigned char*)basis_digits);
   RR_CHECK_LAUNCH();
   return RR_OK;
 }
 
-extern "C" int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npos, int64_t kpad,
-                           const void* basis_digits, const int* col_exp, int64_t nz, int nbasis,
-                           double* y, int* status, rr_stream_t stream) {
+namespace rr {
+namespace yg {
+namespace i8 {
+template <int V>
+static int launch_ygemm_i8(const Params& p, int64_t npos, cudaStream_t st) {
+  const size_t smem = (size_t)Scheme<V>::kStages * Tile<V>::kStageBytes;
+  RR_CUDA_TRY(cudaFuncSetAttribute(ygemm_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+  dim3 grid((unsigned)(npos / kTileM), (unsigned)((p.nz + p.zt - 1) / p.zt));
+  ygemm_kernel<V><<<grid, kThreads, smem, st>>>(p);
+  RR_CHECK_LAUNCH();
+  return RR_OK;
+}
+}  // namespace i8
+}  // namespace yg
+}  // namespace rr
+
+extern "C" int rr_ygemm_i8(int variant, const void* g_digits, const int* row_exp, int64_t npos,
+                           int64_t kpad, const void* basis_digits, const int* col_exp, int64_t nz,
+                           int nbasis, double* y, int* status, rr_stream_t stream) {
+  if (!yg::i8::is_i8(variant)) return RR_EINVAL;
   if (!g_digits || !row_exp || !basis_digits || !col_exp || !y) return RR_EINVAL;
   if (npos < yg::kTileM || npos % yg::kTileM || nz < 0 || nz > INT_MAX) return RR_EINVAL;
   if (nbasis < 1 || nbasis > RR_MAX_NBASIS) return RR_EINVAL;
   if (kpad < yg::kKpadAlign || kpad % yg::kKpadAlign) return RR_EINVAL;
-  // exact int32 accumulation: |digit| <= 64, at most 7 products per
-  // accumulator and pixel
-  if (kpad > 65536) return RR_ENOTSUP;
+  // exact int32 accumulation: the scheme's pixel limit
+  if (kpad > rr_ygemm_i8_max_kpad(variant)) return RR_ENOTSUP;
   if (((reinterpret_cast<uintptr_t>(g_digits) | reinterpret_cast<uintptr_t>(basis_digits)) & 15) != 0)
     return RR_EINVAL;
   if (nz == 0) return RR_OK;
@@ -844,13 +937,10 @@ extern "C" int rr_ygemm_i8(const void* g_digits, const int* row_exp, int64_t npo
   p.nchunk = kpad / yg::i8::kKt;
   p.nz = (int)nz;
   p.nbasis = nbasis;
-  p.zt = yg::i8::zt_of(nbasis);
+  p.zt = yg::i8::zt_of(variant, nbasis);
   p.status = status;
-  const size_t smem = (size_t)yg::i8::kStages * yg::i8::kStageBytes;
-  RR_CUDA_TRY(cudaFuncSetAttribute(yg::i8::ygemm_kernel,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)(npos / yg::kTileM), (unsigned)((nz + p.zt - 1) / p.zt));
-  yg::i8::ygemm_kernel<<<grid, yg::kThreads, smem, (cudaStream_t)stream>>>(p);
-  RR_CHECK_LAUNCH();
-  return RR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (variant == RR_YGEMM_INT8X6)
+    return yg::i8::launch_ygemm_i8<RR_YGEMM_INT8X6>(p, npos, st);
+  return yg::i8::launch_ygemm_i8<RR_YGEMM_INT8X7>(p, npos, st);
 }

@@ -201,10 +201,12 @@ class DeviceBasis:
         z = np.zeros(nz) if redshifts is None else redshifts
         return cls(basis, layout, nb, z, **kw)
 
-    def i8_digits(self, kpad, stream=None):
+    def i8_digits(self, kpad, stream=None, variant=_lib.RR_YGEMM_INT8X7):
         """(digit planes, column exponents) of this basis for the exact
-        tensor-core y (rr_basis_col_exp + rr_slice_basis_i8), cached."""
-        cached = getattr(self, "_i8", None)
+        tensor-core y of an INT8 scheme (rr_basis_col_exp +
+        rr_slice_basis_i8), cached per scheme."""
+        cache = self.__dict__.setdefault("_i8", {})
+        cached = cache.get(variant)
         if cached is not None and cached[0] == kpad:
             return cached[1], cached[2]
         L = _lib.lib()
@@ -214,12 +216,12 @@ class DeviceBasis:
         rc = L.rr_basis_col_exp(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
                                 self.stride, ptr(ce), sh)
         _lib.check(rc, "rr_basis_col_exp")
-        nbytes = int(L.rr_ygemm_i8_basis_bytes(self.nz, self.nbasis, kpad))
+        nbytes = int(L.rr_ygemm_i8_basis_bytes(variant, self.nz, self.nbasis, kpad))
         digits = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=dev)
-        rc = L.rr_slice_basis_i8(ptr(self.basis), self.nz, self.layout.pix_stride, self.nbasis,
-                                 self.stride, kpad, ptr(ce), ptr(digits), sh)
+        rc = L.rr_slice_basis_i8(variant, ptr(self.basis), self.nz, self.layout.pix_stride,
+                                 self.nbasis, self.stride, kpad, ptr(ce), ptr(digits), sh)
         _lib.check(rc, "rr_slice_basis_i8")
-        self._i8 = (kpad, digits, ce)
+        cache[variant] = (kpad, digits, ce)
         return digits, ce
 
     def data_dict(self, as_numpy=True):
@@ -431,9 +433,10 @@ class ScanResult:
 class YGemm:
     """y = Tb^T W f of every (target, z) on the tensor cores: G = R^T W f of
     a target pack (rr_pack_g) and, per template, Y = G^T . basis.
-    variant: "int8x7" (exact Ozaki scheme; rr_slice_g_i8 once here, the
-    basis digits cached on the DeviceBasis, rr_ygemm_i8), or the FP32-
-    accumulated "bf16x3" / "tf32x3" (rr_ygemm)."""
+    variant: "int8x6" / "int8x7" (exact Ozaki schemes of six base-256 or
+    seven base-128 digits; rr_slice_g_i8 once here, the basis digits cached
+    on the DeviceBasis, rr_ygemm_i8), or the FP32-accumulated "bf16x3" /
+    "tf32x3" (rr_ygemm)."""
 
     def __init__(self, pack, variant, stream=None, status=None):
         L = _lib.lib()
@@ -445,7 +448,7 @@ class YGemm:
         self.npos = round_up(pack.nblock * _lib.LANES, 128)
         self.kpad = int(L.rr_ygemm_kpad(pack.layout.pix_stride))
         self.g = torch.empty((self.kpad, self.npos), dtype=torch.float64, device=dev)
-        exact = self.variant == _lib.RR_YGEMM_INT8X7
+        exact = self.variant in _lib.I8_VARIANTS
         self.row_exp = torch.empty(self.npos, dtype=torch.int32, device=dev) if exact else None
         self._status = status or StatusWord(dev)
         tgs = pack.scan_targets_struct()
@@ -455,10 +458,10 @@ class YGemm:
         _lib.check(rc, "rr_pack_g")
         self.g_digits = None
         if exact:
-            nbytes = int(L.rr_ygemm_i8_g_bytes(self.npos, self.kpad))
+            nbytes = int(L.rr_ygemm_i8_g_bytes(self.variant, self.npos, self.kpad))
             self.g_digits = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-            rc = L.rr_slice_g_i8(ptr(self.g), ptr(self.row_exp), self.npos, self.kpad,
-                                 ptr(self.g_digits), sh)
+            rc = L.rr_slice_g_i8(self.variant, ptr(self.g), ptr(self.row_exp), self.npos,
+                                 self.kpad, ptr(self.g_digits), sh)
             _lib.check(rc, "rr_slice_g_i8")
 
     def y(self, basis, stream=None):
@@ -467,10 +470,10 @@ class YGemm:
         sh = stream_handle(stream)
         y = torch.empty((self.npos, basis.nz, basis.nbasis), dtype=torch.float64,
                         device=self.g.device)
-        if self.variant == _lib.RR_YGEMM_INT8X7:
-            digits, col = basis.i8_digits(self.kpad, stream)
-            rc = L.rr_ygemm_i8(ptr(self.g_digits), ptr(self.row_exp), self.npos, self.kpad,
-                               ptr(digits), ptr(col), basis.nz, basis.nbasis, ptr(y),
+        if self.variant in _lib.I8_VARIANTS:
+            digits, col = basis.i8_digits(self.kpad, stream, self.variant)
+            rc = L.rr_ygemm_i8(self.variant, ptr(self.g_digits), ptr(self.row_exp), self.npos,
+                               self.kpad, ptr(digits), ptr(col), basis.nz, basis.nbasis, ptr(y),
                                self._status.ptr, sh)
             _lib.check(rc, "rr_ygemm_i8")
         else:
@@ -481,19 +484,24 @@ class YGemm:
         return y
 
 
-# y = Tb^T W f of the fused scan: "int8x7" (tensor-core GEMM, exact integer
-# accumulation; the fastest), "fp64" (summed inside the scan), or the
-# FP32-accumulated "bf16x3" / "tf32x3" (precision-study variants: they miss
-# |dchi2| <= 1e-3 at DESI S/N)
-DEFAULT_Y = "int8x7"
-_I8_MAX_KPAD = 65536  # int32 headroom of rr_ygemm_i8
+# y = Tb^T W f of the fused scan: "int8x6" (tensor-core GEMM, exact integer
+# accumulation of six base-256 digit planes; the fastest), "int8x7" (seven
+# base-128 planes: one bit more, 1.6x the GEMM time), "fp64" (summed inside
+# the scan), or the FP32-accumulated "bf16x3" / "tf32x3" (precision-study
+# variants: they miss |dchi2| <= 1e-3 at DESI S/N)
+DEFAULT_Y = "int8x6"
 
 
 def resolve_y(ygemm, layout):
-    """The y variant actually used: the default unless given; int8x7 falls
-    back to fp64 when the padded pixel count exceeds its int32 headroom."""
+    """The y variant actually used: the default unless given; an INT8
+    scheme beyond its exact int32 pixel limit falls back to int8x7 (K <=
+    65536), then to fp64."""
     v = DEFAULT_Y if ygemm is None else ygemm
-    if v == "int8x7" and int(_lib.lib().rr_ygemm_kpad(layout.pix_stride)) > _I8_MAX_KPAD:
+    L = _lib.lib()
+    kpad = int(L.rr_ygemm_kpad(layout.pix_stride))
+    if v == "int8x6" and kpad > int(L.rr_ygemm_i8_max_kpad(_lib.RR_YGEMM_INT8X6)):
+        v = "int8x7"
+    if v == "int8x7" and kpad > int(L.rr_ygemm_i8_max_kpad(_lib.RR_YGEMM_INT8X7)):
         v = "fp64"
     return v
 
@@ -508,7 +516,7 @@ def _record(ev, stream):
 def run_fused(pack, bases, stream=None, status=None, ygemm=None, kernel_events=None,
               tiles=None, external_events=False):
     """One persistent launch over every (target, template, z).  ygemm:
-    None (DEFAULT_Y), "fp64", "int8x7", "bf16x3" or "tf32x3"; other than
+    None (DEFAULT_Y), "fp64", "int8x6", "int8x7", "bf16x3" or "tf32x3"; other than
     "fp64", y is computed on the tensor cores first (YGemm).  kernel_events:
     a list that gets a (start, end) CUDA event pair around the scan launches
     alone (timing).  tiles: redshifts per thread {nbasis: ZT} for the small

@@ -312,10 +312,11 @@ def _scan_device(targets, dtemplates, chunk=None, host=False, on_host_ready=None
     if len(lanes) > 1:
         # what the chunks share is made on main first: the bases and their
         # INT8 digit planes for the y GEMM (cached on each basis)
-        if resolve_y(None, layout) == "int8x7":
+        yv = _lib.YGEMM_VARIANTS[resolve_y(None, layout)]
+        if yv in _lib.I8_VARIANTS:
             kpad = int(_lib.lib().rr_ygemm_kpad(layout.pix_stride))
             for b in bases:
-                b.i8_digits(kpad)
+                b.i8_digits(kpad, variant=yv)
         ev0 = torch.cuda.Event()
         ev0.record(main)
         lanes[1].wait_event(ev0)

@@ -6,10 +6,11 @@
   operands, relative to S = sum_q |G| |T| (the natural scale of a dot
   product's rounding error):
     INT8X7 (Ozaki, exact int32 accumulation)   <= 1e-12 S
+    INT8X6 (six base-256 digits, one bit less)  <= 4e-12 S
     BF16X3 / TF32X3 (FP32 accumulation in TMEM) <= K 2^-24 S with K the
       padded pixel count (~5e-4 S at K = 8064), the worst-case bound of a
       K-term FP32 sum
-* The fused scan fed with the INT8X7 y keeps the FP64 path's bounds
+* The fused scan fed with either INT8 y keeps the FP64 path's bounds
   against the oracle (|dchi2| <= 2e-5, identical argmin, coefficients
   1e-5).  With the FP32-accumulated variants chi2 = f^T W f - c^T y moves
   by about 2 c^T dy (first order), so they are held to
@@ -28,7 +29,11 @@ pytestmark = [pytest.mark.gpu,
 from oracle import oracle as O  # noqa: E402
 from redrock_b200 import synth  # noqa: E402
 
-VARIANTS = ["int8x7", "bf16x3", "tf32x3"]
+VARIANTS = ["int8x7", "int8x6", "bf16x3", "tf32x3"]
+I8 = ("int8x7", "int8x6")
+TOL_S = {"int8x7": 1e-12, "int8x6": 4e-12}
+# per-output error bound K 2^(e_t + e_n - BOUND_SHIFT) of each INT8 scheme
+BOUND_SHIFT = {"int8x7": 45, "int8x6": 44}
 
 
 def _case(ntarget, zsub, seed):
@@ -76,13 +81,15 @@ def test_pack_g_matches_numpy():
     assert np.all(g[layout.pix_stride:] == 0) and np.all(g[:, npos:] == 0)
     scale = np.maximum(np.abs(gref).max(axis=0), 1e-300)
     assert np.all(np.abs(g[:layout.pix_stride, :npos] - gref) <= 1e-12 * scale)
-    # exponents: max |G| of each target in (2^(e-1), 2^e]
+    # exponents with the digit schemes' margin: 128/127 max |G| of each
+    # target in [2^(e-1), 2^e), so max |G| < 127/128 2^e
     e = yg.row_exp.cpu().numpy()[:npos].astype(np.int64)
     m = np.abs(gref).max(axis=0)
     nz = m > 0
     assert np.all(e[~nz] == 0)
     ee = e[nz] - 4096
-    assert np.all(m[nz] < np.ldexp(1.0, ee)) and np.all(m[nz] >= np.ldexp(0.5, ee))
+    assert np.all(m[nz] < np.ldexp(127.0 / 128.0, ee))
+    assert np.all(m[nz] * (128.0 / 127.0) >= np.ldexp(0.5, ee) * (1 - 1e-15))
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -98,53 +105,67 @@ def test_ygemm_matches_fp64_product(variant):
         ref = torch.einsum("qp,zqi->pzi", g, t)
         s = torch.einsum("qp,zqi->pzi", g.abs(), t.abs())
         torch.cuda.synchronize()
-        tol = 1e-12 if variant == "int8x7" else yg.kpad * 2.0 ** -24
+        tol = TOL_S[variant] if variant in I8 else yg.kpad * 2.0 ** -24
         err = ((y - ref).abs() / s.clamp_min(1e-300))[:pack.nblock * 32]
         assert torch.isfinite(y[:pack.nblock * 32]).all()
         assert float(err.max()) <= tol, (variant, b.nbasis, float(err.max()))
 
 
-def test_i8_digits_edge_values():
-    """Entries at and just below a power of two (where the leading base-128
-    digit reaches +-64) and of both signs: the error stays within the
-    scheme's bound K 2^-45 2^(e_t + e_n) (rounding to 49-bit integers plus
-    the dropped digit products of order >= 7).  A lost carry would be an
-    error of the order of 2^(e_t + e_n) itself."""
+@pytest.mark.parametrize("variant", I8)
+def test_i8_digits_edge_values(variant):
+    """Entries at and just below a power of two and just below the 127/128
+    margin of the exponents (where the leading digit reaches +-64 in base
+    128 and +-127 in base 256), of both signs: the error stays within the
+    scheme's bound K 2^-45 (base 128) or K 2^-44 (base 256) times
+    2^(e_t + e_n) -- rounding to 49- / 48-bit integers plus the dropped
+    digit products.  A lost carry would be an error of the order of
+    2^(e_t + e_n) itself."""
     import torch
     from redrock_b200 import _lib
     from redrock_b200.device import ptr
     from redrock_b200.engine import YGemm
     tg, tset, layout, pack, bases = _case(33, 401, seed=34)
-    yg = YGemm(pack, "int8x7")
+    yg = YGemm(pack, variant)
     rng = np.random.default_rng(5)
     g = yg.g.cpu().numpy()
     npos = pack.nblock * 32
     for t in range(npos):
         e = int(rng.integers(-20, 20))
-        q = rng.choice(layout.pix_stride, size=6, replace=False)
-        g[q[0], t] = np.ldexp(1.0 - 2.0 ** -40, e)
-        g[q[1], t] = -np.ldexp(1.0 - 2.0 ** -40, e)
-        g[q[2], t] = np.ldexp(0.996, e)
-        g[q[3], t] = -np.ldexp(0.9961, e)
+        q = rng.choice(layout.pix_stride, size=8, replace=False)
+        if t % 2:
+            # rows whose maximum sits at or just below a power of two
+            g[q[0], t] = np.ldexp(1.0 - 2.0 ** -40, e)
+            g[q[1], t] = -np.ldexp(1.0 - 2.0 ** -40, e)
+            g[q[2], t] = np.ldexp(0.996, e)
+            g[q[3], t] = -np.ldexp(0.9961, e)
+        else:
+            # rows whose maximum sits just below the 127/128 margin
+            g[q[0], t] = np.ldexp(127.0 / 128.0 * (1.0 - 2.0 ** -40), e)
+            g[q[1], t] = -np.ldexp(127.0 / 128.0 * (1.0 - 2.0 ** -40), e)
+            g[q[2], t] = np.ldexp(0.9921, e)
+            g[q[3], t] = -np.ldexp(0.99218, e)
         g[q[4], t] = np.ldexp(0.5, e)
         g[q[5], t] = -np.ldexp(0.75, e)
+        g[q[6], t] = np.ldexp(0.5 * 127.0 / 128.0, e)
+        g[q[7], t] = -np.ldexp(0.25 * (1.0 - 2.0 ** -30), e)
     gt = torch.as_tensor(g, device=yg.g.device)
     yg.g.copy_(gt)
     m = np.abs(g).max(axis=0)
-    et = np.where(m > 0, np.frexp(m)[1], 0)
+    et = np.where(m > 0, np.frexp(m * (128.0 / 127.0))[1], 0)
     ex = np.where(m > 0, et + 4096, 0).astype(np.int32)
     yg.row_exp.copy_(torch.as_tensor(ex, device=yg.g.device))
     L = _lib.lib()
-    assert L.rr_slice_g_i8(ptr(yg.g), ptr(yg.row_exp), yg.npos, yg.kpad, ptr(yg.g_digits),
-                           None) == 0
+    assert L.rr_slice_g_i8(yg.variant, ptr(yg.g), ptr(yg.row_exp), yg.npos, yg.kpad,
+                           ptr(yg.g_digits), None) == 0
     for b in bases:
         y = yg.y(b)
         t = b.basis[:, :, :b.nbasis]
         ref = torch.einsum("qp,zqi->pzi", gt[:layout.pix_stride], t)
         err = (y - ref).abs()[:npos].cpu().numpy()
-        ce = b.i8_digits(yg.kpad)[1].cpu().numpy()[:b.nz * b.nbasis].reshape(b.nz, b.nbasis)
+        ce = b.i8_digits(yg.kpad, variant=yg.variant)[1].cpu().numpy()
+        ce = ce[:b.nz * b.nbasis].reshape(b.nz, b.nbasis)
         en = np.where(ce > 0, ce - 4096, 0)
-        bound = yg.kpad * np.ldexp(1.0, et[:npos, None, None] + en[None] - 45)
+        bound = yg.kpad * np.ldexp(1.0, et[:npos, None, None] + en[None] - BOUND_SHIFT[variant])
         assert np.all(err <= bound), float(np.max(err / bound))
 
 
@@ -167,7 +188,7 @@ def test_fused_with_tensor_core_y_vs_oracle():
         for ts, r, r0, b in zip(tset, res, ref, bases):
             zc, co = r.zchi2.cpu().numpy(), r.zcoeff.cpu().numpy()
             zc0 = r0.zchi2.cpu().numpy()
-            if variant == "int8x7":
+            if variant in I8:
                 tdata = O.template_basis(ts.wave, ts.flux, ts.redshifts, grids, ts.igm_model)
                 oii = O.oii_template(ts.wave, ts.flux) if ts.spectype == "GALAXY" else None
                 ospecs = [[O.OSpectrum(s.band, s.wave, s.flux, s.ivar, s.rdata, s.roffsets)
