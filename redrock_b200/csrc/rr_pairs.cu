@@ -58,16 +58,6 @@ struct PairsParams {
   double hi[RR_MAX_NBASIS];
 };
 
-// first j with x[j] (1+z) > e over x[lo..hi) (global memory)
-__device__ __forceinline__ int64_t first_beyond(const double* __restrict__ x, int64_t lo, int64_t hi,
-                                                double zp1, double e) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (dmul(x[mid], zp1) <= e) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
 // odd row stride (doubles) of the shared basis rows: conflict-free 64-bit
 // reads by consecutive threads
 template <int NB>
@@ -81,7 +71,7 @@ struct PairSmem {
   double ys[NB * kPairWin];                     // staged template fluxes
   double red[kPairThreads / 32][NB * (NB + 1) / 2 + NB];
   double c[NB];
-  int64_t jlo, win;
+  int64_t jlo, jhi, win;
   int fix;
   int bad;
 };
@@ -96,16 +86,20 @@ __device__ bool fill_rows(const PairsParams& p, const rr_pair_segment& sg, int64
   const rr_pair_template& tm = p.tm;
   const int64_t first = c0 - kHalfBand;
   const int64_t last = min(c0 + kPairChunk + kHalfBand, sg.npix);  // exclusive
+  // samples needed: from the one before the first edge to the one after
+  // the last edge; the two searches (guess from the near-uniform sample
+  // spacing, then a short walk: a few dependent loads instead of a binary
+  // search's ~16) run in two warps at once
   if (threadIdx.x == 0) {
-    // samples needed: from the one before the first edge to the one after
-    // the last edge
     const int64_t e0 = max(first, (int64_t)0);
-    int64_t jlo = first_beyond(tm.x, 0, tm.nx, zp1, sg.edges[e0]) - 2;
-    int64_t jhi = first_beyond(tm.x, 0, tm.nx, zp1, sg.edges[last]) + 2;
-    jlo = max(jlo, (int64_t)0);
-    jhi = min(jhi, tm.nx);
-    sm.jlo = jlo;
-    sm.win = (jhi - jlo <= kPairWin) ? (jhi - jlo) : 0;  // 0: use global arrays
+    sm.jlo = max(first_above(tm.x, tm.nx, zp1, sg.edges[e0]) - 2, (int64_t)0);
+  } else if (threadIdx.x == 32) {
+    sm.jhi = min(first_above(tm.x, tm.nx, zp1, sg.edges[last]) + 2, tm.nx);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int64_t span = sm.jhi - sm.jlo;
+    sm.win = (span > 0 && span <= kPairWin) ? span : 0;  // 0: use global arrays
   }
   __syncthreads();
   const int64_t jlo = sm.jlo, win = sm.win;
