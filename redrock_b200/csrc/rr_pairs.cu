@@ -296,7 +296,7 @@ __device__ __noinline__ bool bounded_solve(const PairsParams& p, const double (&
 }
 
 template <int NB, bool GRAD>
-__global__ void __launch_bounds__(kPairThreads, 1) zscan_pairs_kernel(const __grid_constant__ PairsParams p) {
+__global__ void __launch_bounds__(kPairThreads, (NB <= 5 ? 2 : 1)) zscan_pairs_kernel(const __grid_constant__ PairsParams p) {
   extern __shared__ __align__(16) unsigned char pair_smem_raw[];
   PairSmem<NB>& sm = *reinterpret_cast<PairSmem<NB>*>(pair_smem_raw);
   constexpr int kTri = NB * (NB + 1) / 2;
