@@ -37,13 +37,17 @@ HUGE_CHI2 = 9999999.0
 
 _pack_cache = IdCache(64)
 _basis_cache = IdCache(32)
+# zfind(graph=True): the captured device plan of the last target batch
+_plan_cache = IdCache(1)
 
 
 def clear_caches():
-    """Drop the device copies of packed targets and template bases (needed
-    after a caller modifies those objects' arrays in place)."""
+    """Drop the device copies of packed targets and template bases, and
+    zfind's captured plan (needed after a caller modifies those objects'
+    arrays in place)."""
     _pack_cache.clear()
     _basis_cache.clear()
+    _plan_cache.clear()
 
 
 def spectral_data(spectra):

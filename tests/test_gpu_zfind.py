@@ -262,3 +262,21 @@ def test_zfind_graph_equals_eager():
     for tid in res_e:
         for ft in res_e[tid]:
             np.testing.assert_array_equal(res_g[tid][ft]["zchi2"], res_e[tid][ft]["zchi2"])
+    # a repeated call on the same objects replays the cached plan's graph
+    from redrock_b200 import zscan
+    plan = next(iter(zscan._plan_cache.d.values()))[1]
+    _, graph2 = zfind(dz, dts, nminima=3, graph=True)
+    assert next(iter(zscan._plan_cache.d.values()))[1] is plan
+    for k in eager:
+        np.testing.assert_array_equal(graph2[k], eager[k], err_msg=k)
+    # after an in-place change of a target and clear_caches(), both paths
+    # see the new contents (and agree again)
+    t0 = dz.local()[0]
+    for s in t0.spectra:
+        s.flux[:] = s.flux * 1.5
+    zscan.clear_caches()
+    _, eager3 = zfind(dz, dts, nminima=3)
+    _, graph3 = zfind(dz, dts, nminima=3, graph=True)
+    assert not np.array_equal(eager3["chi2"], eager["chi2"])
+    for k in eager3:
+        np.testing.assert_array_equal(graph3[k], eager3[k], err_msg=k)
