@@ -253,10 +253,13 @@ class _PackShape:
 class DeviceFitzPlan:
     """The device part of zfind for one target batch -- target packing, the
     fused coarse scan of every template, the K lowest chi2 minima of every
-    (target, template) and the chi2 of their fine redshift grids -- as one
-    stream of launches with no host round trip, optionally captured as a
-    CUDA graph and replayed.  ``run()`` returns the coarse-scan results in
-    calc_zchi2_targets' form and one ``fitz.PrecomputedFine`` per template.
+    (target, template) and the chi2 of their fine redshift grids -- as
+    launches with no host round trip, optionally captured as CUDA graphs
+    (one for the scan, one per template) and replayed.  ``launch()`` starts
+    it; ``coarse()`` returns the coarse-scan results in calc_zchi2_targets'
+    form once the scan is done, ``fine(k)`` template k's
+    ``fitz.PrecomputedFine`` once its fine grids are done, so the host can
+    refine one template while the device still works on the next.
 
     Lazy one-time set-up (kernel attributes, constant tables) happens in an
     eager warm-up on the first target block before the first capture on a
@@ -294,54 +297,141 @@ class DeviceFitzPlan:
             # first 32 targets
             small = local[:32]
             wb = TargetBatch(small, layout).to_device()
-            self._body(wb, RowPack(wb))
+            wres = self._scan(wb)
+            wrows = RowPack(wb)
+            for k in range(len(self.templates)):
+                self._fine(k, wres[k], wrows)
             torch.cuda.synchronize()
             self.status.check("zfind warm-up")
             _warm_devices.add(dev)
-        self.graph = None
-        self.outs = None
+        # graph mode: one graph for packing + the fused scan, one per
+        # template for its candidates and fine-grid scans, replayed back to
+        # back with an event after each, so the host can read one
+        # template's results while the next graphs run
+        self.graphs = None
         if graph:
             from .device import capture_graph
-            self.graph, self.outs = capture_graph(lambda: self._body(self.dbatch, self.rowpack))
+            g_scan, self.res = capture_graph(lambda: self._scan(self.dbatch))
+            self.graphs = [g_scan]
+            self.fouts = []
+            for k in range(len(self.templates)):
+                g, out = capture_graph(lambda k=k: self._fine(k, self.res[k], self.rowpack))
+                self.graphs.append(g)
+                self.fouts.append(out)
 
-    def _body(self, dbatch, rowpack):
-        from .engine import FitzCandidates, TargetPack, run_fused, run_pairs_device
+    def _scan(self, dbatch):
+        from .engine import TargetPack, run_fused
         pack = TargetPack(dbatch, status=self.status)
         res, _ = run_fused(pack, self.bases, status=self.status, tiles=self.tiles)
-        outs = []
-        for b, r, src, zd in zip(self.bases, res, self.srcs, self.zdev):
-            fc = FitzCandidates(r.zchi2, r.penalty if b.oii is not None else None, zd, self.K,
-                                self.nfine)
-            c2, _, pen = run_pairs_device(rowpack, src, fc.pair_t, fc.pair_z, self.status)
-            outs.append((r, fc, c2, pen))
-        return outs
+        return res
 
-    def run(self):
+    def _fine(self, k, r, rowpack):
+        from .engine import FitzCandidates, run_pairs_device
+        b = self.bases[k]
+        fc = FitzCandidates(r.zchi2, r.penalty if b.oii is not None else None, self.zdev[k],
+                            self.K, self.nfine)
+        c2, _, pen = run_pairs_device(rowpack, self.srcs[k], fc.pair_t, fc.pair_z, self.status)
+        return fc, c2, pen
+
+    def launch(self):
+        """Start the plan's device work (the graph replays, or the eager
+        launches) without waiting for it; an event follows the scan and
+        each template's fine-grid scans."""
         import torch
-        if self.graph is not None:
-            self.graph.replay()
-            outs = self.outs
+        if self.graphs is not None:
+            self.graphs[0].replay()
+            res = self.res
         else:
-            outs = self._body(self.dbatch, self.rowpack)
-        torch.cuda.synchronize()
-        self.status.check("zfind device plan")
+            res = self._scan(self.dbatch)
+        ev_scan = torch.cuda.Event()
+        ev_scan.record()
+        outs = []
+        for k in range(len(self.templates)):
+            if self.graphs is not None:
+                self.graphs[k + 1].replay()
+                fc, c2, pen = self.fouts[k]
+            else:
+                fc, c2, pen = self._fine(k, res[k], self.rowpack)
+            ev = torch.cuda.Event()
+            ev.record()
+            outs.append((res[k], fc, c2, pen, ev))
+        self._cur = (ev_scan, outs)
+        self._read = torch_side_stream()
+
+    def _to_host(self, ev, tensors):
+        """Host copies of device tensors once `ev` has completed, made on a
+        side stream, so that they do not wait for the work queued after
+        `ev` on the launching stream; the status word is read with them."""
+        import torch
+        side = self._read
+        side.wait_event(ev)
+        with torch.cuda.stream(side):
+            out = [t.cpu().numpy() for t in tensors]
+            code = int(self.status.t.item())
+        if code:
+            from . import _lib as L
+            L.check(code, "zfind device plan")
+        return out
+
+    def coarse(self):
+        """calc_zchi2_targets' results of the batch (after launch()): waits
+        for the fused scan only."""
+        ev_scan, outs = self._cur
         results = {t.id: {} for t in self.local}
-        pres = []
-        for t, b, (r, fc, c2, pen) in zip(self.templates, self.bases, outs):
+        for t, (r, fc, c2, pen, ev) in zip(self.templates, outs):
             ft = t.template.full_type
-            zc, co, pe = r.zchi2.cpu().numpy(), r.zcoeff.cpu().numpy(), r.penalty.cpu().numpy()
+            zc, co, pe = self._to_host(ev_scan, (r.zchi2, r.zcoeff, r.penalty))
             for i, tg in enumerate(self.local):
                 results[tg.id][ft] = dict(redshifts=t.template.redshifts, zchi2=zc[i],
                                           penalty=pe[i], zcoeff=co[i])
-            T = len(self.local)
-            shape = (T, self.K, self.nfine)
-            c2h = c2.cpu().numpy().reshape(shape)
-            if b.oii is not None:
-                c2h = c2h + pen.cpu().numpy().reshape(shape)
-            pres.append(_fitz.PrecomputedFine(fc.cand.cpu().numpy(), fc.count.cpu().numpy(),
-                                              fc.tie.cpu().numpy(),
-                                              fc.pair_z.cpu().numpy().reshape(shape), c2h))
-        return results, pres
+        return results
+
+    def fine(self, k):
+        """fitz.PrecomputedFine of template k (after launch()): waits for
+        that template's candidates and fine-grid scans only."""
+        ev_scan, outs = self._cur
+        r, fc, c2, pen, ev = outs[k]
+        cand, count, tie, pz, c2h, peh = self._to_host(
+            ev, (fc.cand, fc.count, fc.tie, fc.pair_z, c2, pen))
+        shape = (len(self.local), self.K, self.nfine)
+        c2h = c2h.reshape(shape)
+        if self.bases[k].oii is not None:
+            c2h = c2h + peh.reshape(shape)
+        return _fitz.PrecomputedFine(cand, count, tie, pz.reshape(shape), c2h)
+
+    def run(self):
+        """(coarse results, [PrecomputedFine per template]) of the batch."""
+        self.launch()
+        results = self.coarse()
+        return results, [self.fine(k) for k in range(len(self.templates))]
+
+
+class _LazyFine:
+    """fitz.PrecomputedFine per template full_type, read back from the plan
+    when first asked for (so the host refines one template while the
+    device still scans the fine grids of the next ones)."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        self.index = {t.template.full_type: k for k, t in enumerate(plan.templates)}
+        self.done = {}
+
+    def get(self, ft):
+        if ft not in self.done:
+            self.done[ft] = self.plan.fine(self.index[ft])
+        return self.done[ft]
+
+
+_read_streams = {}
+
+
+def torch_side_stream():
+    """One stream per device for the plan's read-backs."""
+    import torch
+    d = torch.cuda.current_device()
+    if d not in _read_streams:
+        _read_streams[d] = torch.cuda.Stream()
+    return _read_streams[d]
 
 
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
@@ -370,8 +460,9 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
         plan = _plan_cache.get(key, list(local) + list(templates),
                                lambda: DeviceFitzPlan(local, templates, layout, nminima=nminima,
                                                       nfine=nfine))
-        results, plist = plan.run()
-        pres = {t.template.full_type: p for t, p in zip(templates, plist)}
+        plan.launch()
+        results = plan.coarse()
+        pres = _LazyFine(plan)
     elif chi2_scan is None:
         results = calc_zchi2_targets(targets, templates, mp_procs=mp_procs)
     else:
@@ -384,8 +475,12 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
             for ft in results[tg].keys():
                 results[tg][ft]['zchi2'] += priors.eval(tg, results[tg][ft]['redshifts'])
     # the targets' packed rows for the fine-grid pair scans do not depend on
-    # the template: pack them once for every template's refinement
-    rowpack = RowPack.from_targets(local, layout) if local else None
+    # the template: pack them once for every template's refinement (the
+    # device plan has them already)
+    if pres is not None:
+        rowpack, layout = pres.plan.rowpack, pres.plan.layout
+    else:
+        rowpack = RowPack.from_targets(local, layout) if local else None
     sort = np.array([t.template.full_type for t in templates]).argsort()
     arch = None
     if archetypes:
