@@ -342,7 +342,8 @@ def run_ours(args, rank, world, local_rank):
 
     study = ygemm_study(args, step, torch, evals) if args.ygemm_study else None
     adj = adjoint_study(rtg, tms, torch) if (args.adjoint and rank == 0) else None
-    zst = zfind_study(rtg, tms, torch) if (args.zfind and rank == 0) else None
+    zst = zfind_study(rtg, tms, torch, ntarget=args.zfind_targets) \
+        if (args.zfind and rank == 0) else None
     arc = archetype_study(tg, rtg, torch) if (args.archetypes and rank == 0) else None
 
     # ---- end to end through the public API, host buffers ------------------
@@ -480,9 +481,10 @@ def run_ours(args, rank, world, local_rank):
 
 def zfind_study(rtg, tms, torch, ntarget=500):
     """zfind on the first ntarget targets of the workload against all 7
-    templates (3 minima each, config 2's 500 x 7 x 3): wall time of the
-    eager path, of the CUDA-graph path (scan + candidates + fine grids as one
-    graph) and of batched Newton refinement; and, for every target's best
+    templates (3 minima each; config 2's 500 x 7 x 3 by default): wall time
+    of the eager path, of the CUDA-graph path (scan, then each template's
+    candidates + fine grids, as captured graphs) and of batched Newton
+    refinement; and, for every target's best
     GALAXY minimum with ZWARN 0, the distance of the parabola and Newton
     redshifts to the minimum of a dense FP64 scan (401 points spanning two
     fine-grid steps around it, rr_zscan_pairs)."""
@@ -902,8 +904,10 @@ def main():
     ap.add_argument("--adjoint", action="store_true",
                     help="also time the adjoint pair kernel on 3 redshifts per target and template")
     ap.add_argument("--zfind", action="store_true",
-                    help="also time zfind (eager, CUDA graph, Newton) on 500 targets and check "
-                         "the refined redshifts against dense FP64 scans")
+                    help="also time zfind (eager, CUDA graph, Newton) on --zfind-targets targets "
+                         "and check the refined redshifts against dense FP64 scans")
+    ap.add_argument("--zfind-targets", type=int, default=500,
+                    help="targets of the workload the zfind study uses (default 500)")
     ap.add_argument("--tiles", default=None,
                     help='fixed tile choice as JSON, e.g. \'{"4": 3, "5": 2, "block_group": 4}\' '
                          "(skips the autotuner)")
