@@ -51,6 +51,31 @@ def prior_on_coeffs(n_nbh, deg_legendre, sigma, ncamera):
     return prior
 
 
+def _stack_rows(vals):
+    """np.vstack of one result column over many minima, when every value
+    has the same type (and, for strings, length; for arrays, shape):
+    scalars -> (n, 1), 1-D arrays -> (n, len), 2-D arrays concatenated.
+    None for a mixed column."""
+    if not vals:
+        return None
+    v0 = vals[0]
+    t0 = type(v0)
+    if isinstance(v0, _SCALARS):
+        if isinstance(v0, (str, np.str_)):
+            n0 = len(v0)
+            if not all(type(v) is t0 and len(v) == n0 for v in vals):
+                return None
+        elif not all(type(v) is t0 for v in vals):
+            return None
+        return np.array(vals).reshape(len(vals), 1)
+    if isinstance(v0, np.ndarray) and v0.ndim in (1, 2):
+        sh, dt = v0.shape, v0.dtype
+        if not all(type(v) is np.ndarray and v.shape == sh and v.dtype == dt for v in vals):
+            return None
+        return np.stack(vals) if v0.ndim == 1 else np.concatenate(vals, axis=0)
+    return None
+
+
 def _vstack(vals):
     """np.vstack of the values, with a faster path for all-scalar lists
     (the same (n, 1) array and dtype)."""
@@ -414,6 +439,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                             deg_legendre, per_camera, n_nearest, prior_sigma)
 
     out = []
+    rows, spans = [], []   # every target's sorted minima; (index, first, end)
     for j, t in enumerate(targets):
         res = results[j]
         ii = np.argsort([tmp['chi2'] for tmp in res])
@@ -430,10 +456,22 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             npix += (np.asarray(s.ivar) > 0.).sum()
         for r in res:
             r['npixels'] = npix
+        spans.append((len(out), len(rows), len(rows) + len(res)))
+        rows.extend(res)
+        out.append(None)
+    # each column stacked once over all targets' minima, then sliced per
+    # target: the same arrays as a per-target np.vstack wherever the column
+    # has one type and shape throughout (else per target, as before)
+    keys = list(rows[0].keys()) if rows else []
+    if not all(list(r.keys()) == keys for r in rows):
+        keys = []
+    cols = {k: _stack_rows([r[k] for r in rows]) for k in keys}
+    for j, a, b in spans:
         tmp = {}
-        for k in res[0].keys():
-            tmp[k] = _vstack([r[k] for r in res])
-        out.append(tmp)
+        for k in rows[a].keys():
+            col = cols.get(k)
+            tmp[k] = col[a:b] if col is not None else _vstack([r[k] for r in rows[a:b]])
+        out[j] = tmp
     return out
 
 

@@ -186,7 +186,12 @@ def _finalise_target(tid, fits, nminima, arch=None):
                 val = np.zeros_like(ref)
             # otherwise the previous row's value repeats, as in redrock's loop
             vals.append(val)
-        out[k] = np.vstack(vals)
+        # np.vstack of 2-D arrays is their concatenation (without vstack's
+        # per-call promotion overhead)
+        if all(type(v) is np.ndarray and v.ndim == 2 for v in vals):
+            out[k] = np.concatenate(vals, axis=0)
+        else:
+            out[k] = np.vstack(vals)
         if k != 'coeff' and out[k].shape[1] == 1:
             out[k] = out[k].flatten()
     n = len(out['chi2'])
@@ -434,6 +439,26 @@ def torch_side_stream():
     return _read_streams[d]
 
 
+
+def _refine_all(templates, sort, local, results, archetypes, nminima, use_gpu, deg_legendre,
+                zminfit_npoints, per_camera, n_nearest, prior_sigma, layout, rowpack, refine,
+                pres):
+    """fitz of every template over the local targets (zfind.py:330-363),
+    in redrock's template order; each result goes to results[id][ft]['zfit']."""
+    for t in np.array(list(templates), dtype=object)[sort] if local else []:
+        ft = t.template.full_type
+        archetype = archetypes.get(t.template._rrtype) if archetypes else None
+        chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
+        fits = _fitz.fitz_targets(chi2, t.template.redshifts, local, t.template,
+                                  nminima=nminima, archetype=archetype, use_gpu=use_gpu,
+                                  deg_legendre=deg_legendre, zminfit_npoints=zminfit_npoints,
+                                  per_camera=per_camera, n_nearest=n_nearest,
+                                  prior_sigma=prior_sigma, layout=layout, rowpack=rowpack,
+                                  refine=refine, pre=None if pres is None else pres.get(ft))
+        for tg, zf in zip(local, fits):
+            results[tg.id][ft]['zfit'] = zf
+
+
 def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=None,
           chi2_scan=None, use_gpu=True, zminfit_npoints=15, per_camera=None, deg_legendre=None,
           n_nearest=None, prior_sigma=None, ncamera=None, refine="parabola", graph=False):
@@ -490,18 +515,20 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
                 all_spectypes.append(t.template.template_type)
         arch = dict(spectypes=list(archetypes.keys()), all_spectypes=all_spectypes,
                     n_nearest=n_nearest)
-    for t in np.array(list(templates), dtype=object)[sort] if local else []:
-        ft = t.template.full_type
-        archetype = archetypes.get(t.template._rrtype) if archetypes else None
-        chi2 = [results[tg.id][ft]['zchi2'] + results[tg.id][ft]['penalty'] for tg in local]
-        fits = _fitz.fitz_targets(chi2, t.template.redshifts, local, t.template,
-                                  nminima=nminima, archetype=archetype, use_gpu=use_gpu,
-                                  deg_legendre=deg_legendre, zminfit_npoints=zminfit_npoints,
-                                  per_camera=per_camera, n_nearest=n_nearest,
-                                  prior_sigma=prior_sigma, layout=layout, rowpack=rowpack,
-                                  refine=refine, pre=None if pres is None else pres.get(ft))
-        for tg, zf in zip(local, fits):
-            results[tg.id][ft]['zfit'] = zf
+    # with the device plan, the host-driven pair launches of the refinement
+    # (further candidates, single-z fits) go to the plan's read-back stream:
+    # they need only the packed rows and template arrays, so they need not
+    # queue behind the graphs of the templates not yet refined
+    import contextlib
+    import torch
+    on_side = torch.cuda.stream(pres.plan._read) if pres is not None \
+        else contextlib.nullcontext()
+    with on_side:
+        _refine_all(templates, sort, local, results, archetypes, nminima, use_gpu, deg_legendre,
+                    zminfit_npoints, per_camera, n_nearest, prior_sigma, layout, rowpack,
+                    refine, pres)
+    if pres is not None:
+        torch.cuda.current_stream().wait_stream(pres.plan._read)
     for tg in local:
         results[tg.id]['meta'] = tg.meta
     if comm is not None and comm.size > 1:

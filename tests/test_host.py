@@ -323,3 +323,32 @@ def test_newton_refinement_logic_on_a_model_function(monkeypatch):
     assert it < 24
     assert np.all(np.abs(z - zmin) <= 1e-4 * sig)
     np.testing.assert_allclose(h * sig ** 2 / 2, 1.0, rtol=1e-3)
+
+
+def test_fitz_column_stacking_matches_per_target_vstack():
+    """fitz_targets stacks each result column once over all targets' minima
+    and slices it per target: the slices equal a per-target np.vstack
+    (values, dtype, shape); a column of mixed types or shapes is left to
+    the per-target path."""
+    import numpy as np
+    from redrock_b200.fitz import _stack_rows, _vstack
+    rng = np.random.default_rng(0)
+    rows, spans = [], []
+    for j in range(40):
+        a = len(rows)
+        for _ in range(int(rng.integers(1, 4))):
+            rows.append(dict(z=float(rng.random()), zerr=float(rng.random()),
+                             zwarn=int(rng.integers(0, 5)), chi2=float(rng.random()),
+                             zz=rng.random(15), zzchi2=rng.random(15), coeff=rng.random((1, 10)),
+                             fitmethod='PCA', npixels=np.int64(7000 + j)))
+        spans.append((a, len(rows)))
+    cols = {k: _stack_rows([r[k] for r in rows]) for k in rows[0]}
+    for a, b in spans:
+        for k in rows[0]:
+            ref = _vstack([r[k] for r in rows[a:b]])
+            got = cols[k][a:b]
+            assert got.dtype == ref.dtype and got.shape == ref.shape
+            assert np.array_equal(got, ref), k
+    assert _stack_rows([np.zeros(10), np.zeros((1, 10))]) is None
+    assert _stack_rows([1, 2.0]) is None
+    assert _stack_rows(['PCA', 'NMF3']) is None
