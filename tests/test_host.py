@@ -352,3 +352,34 @@ def test_fitz_column_stacking_matches_per_target_vstack():
     assert _stack_rows([np.zeros(10), np.zeros((1, 10))]) is None
     assert _stack_rows([1, 2.0]) is None
     assert _stack_rows(['PCA', 'NMF3']) is None
+
+
+def test_resolve_y_falls_back_by_pixel_count(monkeypatch):
+    """The default tensor-core y scheme (INT8X6) gives way to INT8X7 when the
+    padded pixel count is beyond its exact int32 range, and INT8X7 to the
+    FP64 sum inside the scan beyond its own; explicit choices are kept."""
+    from redrock_b200 import _lib, engine
+
+    class FakeLib:
+        kpad = 8064
+
+        def rr_ygemm_kpad(self, pix_stride):
+            return self.kpad
+
+        def rr_ygemm_i8_max_kpad(self, variant):
+            return {_lib.RR_YGEMM_INT8X6: 21824, _lib.RR_YGEMM_INT8X7: 65536}.get(variant, -1)
+
+    fake = FakeLib()
+    monkeypatch.setattr(_lib, "lib", lambda: fake)
+
+    class Layout:
+        pix_stride = 0
+
+    assert engine.DEFAULT_Y == "int8x6"
+    assert engine.resolve_y(None, Layout) == "int8x6"
+    fake.kpad = 21824 + 64
+    assert engine.resolve_y(None, Layout) == "int8x7"
+    assert engine.resolve_y("int8x6", Layout) == "int8x7"
+    fake.kpad = 65536 + 64
+    assert engine.resolve_y(None, Layout) == "fp64"
+    assert engine.resolve_y("bf16x3", Layout) == "bf16x3"
