@@ -383,3 +383,40 @@ def test_resolve_y_falls_back_by_pixel_count(monkeypatch):
     fake.kpad = 65536 + 64
     assert engine.resolve_y(None, Layout) == "fp64"
     assert engine.resolve_y("bf16x3", Layout) == "bf16x3"
+
+
+def test_int8_digit_schemes_reconstruct_exactly():
+    """The digit decompositions the INT8 y GEMM slices its operands into
+    (restated in numpy): X = rint(x 2^(mant - e)) with e the exponent of
+    128/127 max |x| splits into balanced digits that all fit int8 -- seven
+    base-128 digits (|digit| <= 64) or six base-256 digits (the leading
+    one within +-127 thanks to the margin) -- and the digits sum back to X
+    exactly, including values just below the margin and at +-max."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+
+    def digits(X, nd, bits):
+        half, mask = 1 << (bits - 1), (1 << bits) - 1
+        out, x = [], X.copy()
+        for _ in range(nd - 1):
+            a = ((x + half) & mask) - half
+            x = (x - a) >> bits
+            out.append(a)
+        out.append(x)
+        return out[::-1]
+
+    for nd, bits, mant, lim in ((7, 7, 48, 64), (6, 8, 47, 127)):
+        for trial in range(50):
+            x = rng.uniform(-1, 1, 4096) * 10.0 ** rng.uniform(-30, 30)
+            m = np.abs(x).max()
+            x[:4] = [m, -m, m * (1 - 2.0 ** -40), -m * 127 / 128]
+            e = np.frexp(np.abs(x).max() * (128.0 / 127.0))[1]
+            X = np.rint(np.ldexp(x, mant - e)).astype(np.int64)
+            d = digits(X, nd, bits)
+            half = 1 << (bits - 1)
+            for di in d[1:]:      # low digits: balanced, [-base/2, base/2)
+                assert int(di.min()) >= -half and int(di.max()) < half
+            assert int(np.abs(d[0]).max()) <= lim
+            assert all(int(di.min()) >= -128 and int(di.max()) <= 127 for di in d)
+            rec = sum(di * (1 << (bits * (nd - 1 - k))) for k, di in enumerate(d))
+            assert np.array_equal(rec, X)
