@@ -234,6 +234,137 @@ def _finalise_target(tid, fits, nminima, arch=None):
     return out
 
 
+def _deltachi2_batch(chi2, z, okfit, dvlimit, first, n):
+    """_deltachi2_f64 of many targets at once: target i owns rows
+    first[i] .. first[i] + n[i] - 1.  The rows are laid out as a padded
+    [target][row][row] block and every pair gets the same IEEE operations
+    as the per-target loop: deltachi2[i] is the minimum of c_j - c_i over
+    the later good fits farther than the velocity limit (NaN if one of
+    them is NaN, 0 if there is none); setzwarn[i] flags another good fit
+    within MIN_DELTACHI2 and at least the velocity limit away."""
+    nt, m = len(n), int(n.max()) if len(n) else 0
+    rows = first[:, None] + np.arange(m)[None, :]
+    valid = np.arange(m)[None, :] < n[:, None]
+    rows = np.where(valid, rows, 0)
+    c, zz, ok, dl = chi2[rows], z[rows], okfit[rows] & valid, dvlimit[rows]
+    dv = np.abs(_fitz.C_KMS * (zz[:, None, :] - zz[:, :, None]) / (1.0 + zz[:, :, None]))
+    lim = np.minimum(dl[:, :, None], dl[:, None, :])
+    d = c[:, None, :] - c[:, :, None]           # [t][i][j] = c_j - c_i
+    later = np.arange(m)[None, :] > np.arange(m)[:, None]
+    far = ok[:, None, :] & later[None] & (dv > lim)
+    dmin = np.where(far, d, np.inf).min(axis=2)
+    has_nan = (far & np.isnan(d)).any(axis=2)
+    dmin = np.where(has_nan, np.nan, dmin)
+    dmin = np.where(far.any(axis=2), dmin, 0.0)
+    other = ~np.eye(m, dtype=bool)[None]
+    near = (ok[:, None, :] & other & (np.abs(d) < MIN_DELTACHI2) & (dv >= lim)).any(axis=2)
+    deltachi2 = dmin[valid]
+    setzwarn = near[valid]
+    return deltachi2, setzwarn
+
+
+def _finalise_batch(tids, fits_list, nminima):
+    """The zfit table of many targets at once -- the concatenation of
+    _finalise_target(tid, fits, nminima) over the targets (no archetypes),
+    as column arrays -- or None when the batch needs the per-target path
+    (a target without minima for some template, or templates in different
+    orders or with differently shaped columns).
+
+    The same steps as _finalise_target, over all rows: the derived columns
+    per template, ZWARN's NODATA / LITTLE_COVERAGE bits, the stable
+    (badfit, chi2) order within each target, the first nminima fits per
+    spectype kept (a target that loses fits is re-sorted from the
+    spectype-grouped order, as the per-target code does), znum, and
+    calc_deltachi2 per target."""
+    if not tids:
+        return None
+    fts = [ft for ft, _ in fits_list[0]]
+    for fits in fits_list:
+        if [ft for ft, _ in fits] != fts:
+            return None
+        for _, z in fits:
+            if len(z['chi2']) == 0:
+                return None
+    keys = list(fits_list[0][0][1].keys())
+    if any(list(z.keys()) != keys for fits in fits_list for _, z in fits):
+        return None
+    nt, ntm = len(tids), len(fts)
+    counts = np.array([[len(z['chi2']) for _, z in fits] for fits in fits_list], dtype=np.int64)
+    ncoeffs = [fits_list[0][k][1]['coeff'].shape[1] for k in range(ntm)]
+    if any(z['coeff'].ndim != 2 or z['coeff'].shape[1] != ncoeffs[k]
+           for fits in fits_list for k, (_, z) in enumerate(fits)):
+        return None
+    maxncoeff = max(ncoeffs)
+    out = {}
+    # rows in target-major order: target, then template, then minimum
+    for k in keys:
+        vals = [z[k] for fits in fits_list for _, z in fits]
+        if k == 'coeff':
+            vals = [v if v.shape[1] == maxncoeff else
+                    np.append(v, np.zeros((v.shape[0], maxncoeff - v.shape[1])), axis=1)
+                    for v in vals]
+        if not all(type(v) is np.ndarray and v.ndim == 2 for v in vals):
+            return None
+        col = np.concatenate(vals, axis=0)
+        out[k] = col.flatten() if (k != 'coeff' and col.shape[1] == 1) else col
+    n_tm = counts.ravel()  # rows per (target, template), target-major
+    spec_sub = [parse_fulltype(ft) for ft in fts]
+    tm_idx = np.tile(np.arange(ntm), nt)
+    spectype = np.repeat(np.array([st for st, _ in spec_sub])[tm_idx], n_tm)
+    subtype = np.repeat(np.array([sb for _, sb in spec_sub])[tm_idx], n_tm)
+    ncoeff = np.repeat(np.array(ncoeffs, dtype=np.int64)[tm_idx], n_tm)
+    mvd = np.repeat(np.array([MAX_VELO_DIFF_STAR if st.upper() == 'STAR' else MAX_VELO_DIFF
+                              for st, _ in spec_sub])[tm_idx], n_tm)
+    out['spectype'], out['subtype'], out['ncoeff'] = spectype, subtype, ncoeff
+    n_t = counts.sum(axis=1)
+    tix = np.repeat(np.arange(nt), n_t)
+    out['targetid'] = np.repeat(np.asarray(tids), n_t)
+    zwarn = out['zwarn']
+    zwarn[out['npixels'] == 0] |= NODATA
+    zwarn[out['npixels'] < 10 * out['ncoeff']] |= LITTLE_COVERAGE
+    badfit = (zwarn & BADFIT_MASK) != 0
+    chi2 = out['chi2']
+    # stable (badfit, chi2) order within each target
+    order = np.lexsort((chi2, badfit, tix))
+    # the first nminima of each (target, spectype) in that order
+    scode = np.unique(spectype, return_inverse=True)[1].ravel()
+    g = tix[order] * (scode.max() + 1) + scode[order]
+    gs = np.argsort(g, kind='stable')
+    gsorted = g[gs]
+    start = np.r_[0, np.nonzero(np.diff(gsorted))[0] + 1]
+    rank_sorted = np.arange(len(g)) - np.repeat(start, np.diff(np.r_[start, len(g)]))
+    rank = np.empty_like(rank_sorted)
+    rank[gs] = rank_sorted
+    keep = rank < nminima
+    kept = order[keep]
+    # targets that lost fits: ties in (badfit, chi2) follow the spectype
+    # grouping their kept rows were put in before the second sort
+    lost = np.zeros(nt, dtype=bool)
+    lost[tix[order[~keep]]] = True
+    pos = np.empty(len(order), dtype=np.int64)
+    pos[order] = np.arange(len(order))
+    sec = np.where(lost[tix[kept]], scode[kept], 0)
+    final = kept[np.lexsort((pos[kept], sec, chi2[kept], badfit[kept], tix[kept]))]
+    res = {k: v[final] for k, v in out.items()}
+    res['max_velo_diff'] = mvd[final]
+    ft_t = tix[final]
+    n_keep = np.bincount(ft_t, minlength=nt)
+    first = np.r_[0, np.cumsum(n_keep)[:-1]]
+    res['znum'] = np.arange(len(final)) - np.repeat(first, n_keep)
+    okfit = (res['zwarn'] & BADFIT_MASK) == 0
+    deltachi2, setzwarn = _deltachi2_batch(np.asarray(res['chi2'], dtype=np.float64),
+                                           np.asarray(res['z'], dtype=np.float64), okfit,
+                                           np.asarray(res['max_velo_diff'], dtype=np.float64),
+                                           first, n_keep)
+    res['deltachi2'] = deltachi2
+    res['zwarn'][setzwarn] |= SMALL_DELTA_CHI2
+    del res['max_velo_diff']
+    # the per-target path's column order: the fit columns, the derived
+    # ones, then targetid, znum, deltachi2 (zfind puts targetid first)
+    cols = keys + ['spectype', 'subtype', 'ncoeff', 'targetid', 'znum', 'deltachi2']
+    return {k: res[k] for k in cols}
+
+
 # candidates per target and template evaluated on the device in the graph
 # path (rr_fitz_candidates): nminima plus this many spares for candidates
 # that fall within max_velo_diff of a better one.  Rows that need more are
@@ -542,18 +673,25 @@ def zfind(targets, templates, mp_procs=1, nminima=3, archetypes=None, priors=Non
             allresults.update(part)
     else:
         allresults = results
-    rows = []
-    for tid in targets.all_target_ids:
-        fits = [(ft, allresults[tid][ft]['zfit']) for ft in allresults[tid] if ft != 'meta']
+    tids = list(targets.all_target_ids)
+    fits_list = []
+    for tid in tids:
+        fits_list.append([(ft, allresults[tid][ft]['zfit']) for ft in allresults[tid]
+                          if ft != 'meta'])
         for ft in allresults[tid]:
             if ft != 'meta':
                 del allresults[tid][ft]['zfit']
-        rows.append(_finalise_target(tid, fits, nminima, arch))
-    # stack the per-target tables (astropy.table.vstack equivalent)
-    cols = ['targetid'] + [k for k in rows[0] if k != 'targetid']
-    allzfit = {}
-    for k in cols:
-        allzfit[k] = np.concatenate([r[k] for r in rows], axis=0)
+    batch = _finalise_batch(tids, fits_list, nminima) if arch is None else None
+    if batch is not None:
+        allzfit = {'targetid': batch['targetid']}
+        allzfit.update((k, v) for k, v in batch.items() if k != 'targetid')
+    else:
+        rows = [_finalise_target(tid, fits, nminima, arch) for tid, fits in zip(tids, fits_list)]
+        # stack the per-target tables (astropy.table.vstack equivalent)
+        cols = ['targetid'] + [k for k in rows[0] if k != 'targetid']
+        allzfit = {}
+        for k in cols:
+            allzfit[k] = np.concatenate([r[k] for r in rows], axis=0)
     for k in list(allzfit):
         if 'pca' in k.lower():
             allzfit[k] = allzfit.pop(k)

@@ -420,3 +420,88 @@ def test_int8_digit_schemes_reconstruct_exactly():
             assert all(int(di.min()) >= -128 and int(di.max()) <= 127 for di in d)
             rec = sum(di * (1 << (bits * (nd - 1 - k))) for k, di in enumerate(d))
             assert np.array_equal(rec, X)
+
+
+def _zfit_rows(rng, nmin, nz_fine, nb, npix, tie_chi2=None):
+    """One template's fitz result for one target (the columns fitz returns)."""
+    import numpy as np
+    from redrock_b200 import zfind as ZF
+    chi2 = rng.uniform(9000, 9100, nmin)
+    if tie_chi2 is not None:
+        chi2[:] = tie_chi2
+    z = rng.uniform(0, 2, nmin)
+    if nmin > 1 and rng.random() < 0.3:
+        z[1] = z[0] * (1 + 1e-5)          # within max_velo_diff
+        chi2[1] = chi2[0] + 1.0            # and within MIN_DELTACHI2
+    zwarn = np.where(rng.random(nmin) < 0.2, ZF.BAD_MINFIT, 0).astype(np.int64)
+    return dict(z=z[:, None], zerr=rng.random((nmin, 1)), zwarn=zwarn[:, None],
+                chi2=chi2[:, None], zz=rng.random((nmin, nz_fine)),
+                zzchi2=rng.random((nmin, nz_fine)), coeff=rng.random((nmin, nb)),
+                fitmethod=np.full((nmin, 1), 'PCA'), npixels=np.full((nmin, 1), npix))
+
+
+def test_batched_zfind_finalisation_matches_per_target():
+    """zfind's batched finalisation gives the concatenation of the
+    per-target tables (redrock's per-target logic) column for column:
+    values, order (stable chi2 order, the nminima-per-spectype cut and the
+    re-sort of targets that lose fits, ties included), znum, deltachi2 and
+    every ZWARN bit, with NODATA / LITTLE_COVERAGE targets in the batch."""
+    import numpy as np
+    from redrock_b200 import zfind as ZF
+    rng = np.random.default_rng(11)
+    fts = ['GALAXY', 'QSO', 'STAR:::A', 'STAR:::F', 'STAR:::K']
+    nbs = [10, 4, 5, 5, 5]
+    for trial in range(6):
+        nminima = 3
+        tids = list(range(1000, 1000 + 60))
+        fits_list = []
+        for i, tid in enumerate(tids):
+            npix = 0 if i % 17 == 3 else (30 if i % 13 == 5 else 7000)
+            tie = 9050.0 if i % 11 == 2 else None
+            fits = []
+            for ft, nb in zip(fts, nbs):
+                nmin = int(rng.integers(1, 4))
+                fits.append((ft, _zfit_rows(rng, nmin, 15, nb, npix, tie)))
+            fits_list.append(fits)
+        copies = [[(ft, {k: v.copy() for k, v in z.items()}) for ft, z in fits]
+                  for fits in fits_list]
+        rows = [ZF._finalise_target(tid, fits, nminima) for tid, fits in zip(tids, copies)]
+        ref = {k: np.concatenate([r[k] for r in rows], axis=0) for k in rows[0]}
+        got = ZF._finalise_batch(tids, fits_list, nminima)
+        assert got is not None
+        assert list(got) == list(rows[0])
+        for k in ref:
+            assert got[k].shape == ref[k].shape, k
+            assert got[k].dtype.kind == ref[k].dtype.kind, k
+            assert np.array_equal(got[k], ref[k]), k
+        assert np.any(ref['zwarn'] & ZF.SMALL_DELTA_CHI2)
+        assert np.any(ref['zwarn'] & ZF.NODATA) and np.any(ref['zwarn'] & ZF.LITTLE_COVERAGE)
+    # a target without minima for a template goes the per-target way
+    fits_list[0][1] = (fts[1], _zfit_rows(rng, 0, 15, 4, 7000))
+    assert ZF._finalise_batch(tids, fits_list, 3) is None
+
+
+def test_batched_deltachi2_matches_per_target_loop():
+    """The padded all-targets deltachi2 gives the per-target loop's values
+    and flags, NaN chi2, bad fits and velocity-limit edges included."""
+    import numpy as np
+    from redrock_b200 import zfind as ZF
+    rng = np.random.default_rng(5)
+    n = rng.integers(1, 10, 300)
+    first = np.r_[0, np.cumsum(n)[:-1]]
+    tot = int(n.sum())
+    chi2 = rng.uniform(100, 130, tot)
+    chi2[rng.random(tot) < 0.02] = np.nan
+    z = rng.uniform(0, 3, tot)
+    # pairs at and near the velocity limit
+    for a in first[:100]:
+        if a + 1 < tot:
+            z[a + 1] = z[a] + 1000.0 / ZF._fitz.C_KMS * (1 + z[a]) * rng.choice([0.5, 1.0, 2.0])
+    okfit = rng.random(tot) < 0.85
+    dl = np.where(rng.random(tot) < 0.5, ZF.MAX_VELO_DIFF, ZF.MAX_VELO_DIFF_STAR).astype(float)
+    d_b, s_b = ZF._deltachi2_batch(chi2, z, okfit, dl, first, n)
+    for i in range(len(n)):
+        a, b = first[i], first[i] + n[i]
+        d, sz = ZF._deltachi2_f64(chi2[a:b], z[a:b], okfit[a:b], dl[a:b])
+        np.testing.assert_array_equal(d_b[a:b], d)
+        np.testing.assert_array_equal(s_b[a:b], sz)
