@@ -492,7 +492,7 @@ class DeviceFitzPlan:
             ev.record()
             outs.append((res[k], fc, c2, pen, ev))
         self._cur = (ev_scan, outs)
-        self._read = torch_side_stream()
+        self._read = _read_stream()
 
     def _to_host(self, ev, tensors):
         """Host copies of device tensors once `ev` has completed, made on a
@@ -535,12 +535,6 @@ class DeviceFitzPlan:
             c2h = c2h + peh.reshape(shape)
         return _fitz.PrecomputedFine(cand, count, tie, pz.reshape(shape), c2h)
 
-    def run(self):
-        """(coarse results, [PrecomputedFine per template]) of the batch."""
-        self.launch()
-        results = self.coarse()
-        return results, [self.fine(k) for k in range(len(self.templates))]
-
 
 class _LazyFine:
     """fitz.PrecomputedFine per template full_type, read back from the plan
@@ -561,7 +555,7 @@ class _LazyFine:
 _read_streams = {}
 
 
-def torch_side_stream():
+def _read_stream():
     """One stream per device for the plan's read-backs."""
     import torch
     d = torch.cuda.current_device()
