@@ -102,11 +102,16 @@ def get_dv(z, zref):
 
 
 def find_minima(x):
-    """Indices of local minima including edges, sorted by value (fitz.py:46-67)."""
+    """Indices of local minima including edges, sorted by value (fitz.py:46-67):
+    x[i] <= both neighbours (<=: plateaus count), the first and last point
+    compared with their one neighbour, ordered by np.argsort of the values."""
     x = np.asarray(x)
-    ii = np.where(np.r_[True, x[1:] <= x[:-1]] & np.r_[x[:-1] <= x[1:], True])[0]
-    jj = np.argsort(x[ii])
-    return ii[jj]
+    is_min = np.ones(len(x), dtype=bool)
+    if len(x) > 1:
+        is_min[1:] = x[1:] <= x[:-1]
+        is_min[:-1] &= x[:-1] <= x[1:]
+    ii = np.flatnonzero(is_min)
+    return ii[np.argsort(x[ii])]
 
 
 def minfit(x, y):

@@ -505,3 +505,24 @@ def test_batched_deltachi2_matches_per_target_loop():
         d, sz = ZF._deltachi2_f64(chi2[a:b], z[a:b], okfit[a:b], dl[a:b])
         np.testing.assert_array_equal(d_b[a:b], d)
         np.testing.assert_array_equal(s_b[a:b], sz)
+
+
+def test_find_minima_definition():
+    """fitz's candidate minima: every index whose value is <= both
+    neighbours (edges against their one neighbour), ordered by np.argsort
+    of the values -- checked against that definition written out directly,
+    on rows with plateaus, ties and NaN."""
+    import numpy as np
+    from redrock_b200.fitz import find_minima
+    rng = np.random.default_rng(9)
+    assert list(find_minima([1, 1, 1, 2, 2, 2])) == [0, 1, 2, 4, 5]
+    assert list(find_minima([3.0])) == [0]
+    for _ in range(200):
+        x = np.round(rng.normal(size=int(rng.integers(2, 60))), 1)
+        if rng.random() < 0.2:
+            x[rng.integers(0, len(x))] = np.nan
+        n = len(x)
+        idx = [i for i in range(n)
+               if (i == 0 or x[i] <= x[i - 1]) and (i == n - 1 or x[i] <= x[i + 1])]
+        idx = np.array(idx, dtype=np.int64)
+        np.testing.assert_array_equal(find_minima(x), idx[np.argsort(x[idx])])
