@@ -292,12 +292,28 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
     done = [False] * ntg
     want = nminima + batch_extra
 
-    def refine_fits(tj, zz3, c23):
+    def refine_fits(tj, zz3, c23, zzall, c2all):
+        """Per candidate (z, zerr, zwarn, chi2, zmin) after the refinement
+        and redrock's checks on it (fitz.py:263-280): a minimum outside the
+        fine grid is BAD_MINFIT and replaced by the grid's first lowest
+        point; Z_FITLIMIT when it or the refined minimum is outside
+        redshifts[1:-1]."""
         if refine == "newton":
             fx0, ferr, fy0, fzw = newton_batch(tj, zz3)
         else:
             fx0, ferr, fy0, fzw = minfit_batch(zz3, c23)
-        return list(zip(fx0.tolist(), ferr.tolist(), fy0.tolist(), fzw.tolist()))
+        fzw = np.asarray(fzw, dtype=np.int64)
+        rows = np.arange(len(fx0))
+        kmin = np.argmin(c2all, axis=1)
+        off = (fx0 < zzall[:, 0]) | (fx0 > zzall[:, -1])
+        zbest = np.where(off, zzall[rows, kmin], fx0)
+        chi2b = np.where(off, c2all[rows, kmin], fy0)
+        zw = fzw | np.where(off, BAD_MINFIT, 0)
+        lim = (zbest < redshifts[1]) | (zbest > redshifts[-2]) | \
+            (fx0 < redshifts[1]) | (fx0 > redshifts[-2])
+        zw = zw | np.where(lim, Z_FITLIMIT, 0)
+        return list(zip(zbest.tolist(), ferr.tolist(), zw.tolist(), chi2b.tolist(),
+                        fx0.tolist()))
 
     def fetch(tlist, count):
         tid, key = [], []
@@ -336,7 +352,8 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             ib = np.clip(np.argmin(c2all, axis=1), 1, nz - 2)
             cols = ib[:, None] + np.arange(-1, 2)[None, :]
             rows = np.arange(len(key))[:, None]
-            fits = refine_fits([k[0] for k in key], zzall[rows, cols], c2all[rows, cols])
+            fits = refine_fits([k[0] for k in key], zzall[rows, cols], c2all[rows, cols],
+                               zzall, c2all)
         for n_, (j, imin) in enumerate(key):
             fine[j][imin] = (zzall[n_], c2all[n_], fits[n_])
 
@@ -373,7 +390,7 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
             ib = np.clip(np.argmin(c2p, axis=1), 1, nz - 2)
             cols = ib[:, None] + np.arange(-1, 2)[None, :]
             rows = np.arange(len(key))[:, None]
-            fits = refine_fits(jj.tolist(), zzp[rows, cols], c2p[rows, cols])
+            fits = refine_fits(jj.tolist(), zzp[rows, cols], c2p[rows, cols], zzp, c2p)
         for n_, (j, imin) in enumerate(key):
             fine[j][imin] = (zzp[n_], c2p[n_], fits[n_])
 
@@ -394,22 +411,22 @@ def fitz_targets(zchi2_list, redshifts, targets, template, nminima=3, archetype=
                 if _near_any(redshifts[imin], zprev, maxv):
                     continue
                 zz, zzchi2, fit = fine[j][imin]
-                i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
                 if fit is not None:
-                    zmin, sigma, chi2min, zwarn = fit
+                    zbest, zerr, zwarn, chi2min, zmin = fit
                 else:
+                    i = min(max(np.argmin(zzchi2), 1), len(zz) - 2)
                     zmin, sigma, chi2min, zwarn = minfit(zz[i - 1:i + 2], zzchi2[i - 1:i + 2])
-                zbest = zmin
-                zerr = sigma
-                if zbest < zz[0] or zbest > zz[-1]:
-                    zwarn |= BAD_MINFIT
-                    k = np.where(zzchi2 == np.min(zzchi2))[0][0]
-                    zbest = zz[k]
-                    chi2min = zzchi2[k]
-                if zbest < redshifts[1] or zbest > redshifts[-2]:
-                    zwarn |= Z_FITLIMIT
-                if zmin < redshifts[1] or zmin > redshifts[-2]:
-                    zwarn |= Z_FITLIMIT
+                    zbest = zmin
+                    zerr = sigma
+                    if zbest < zz[0] or zbest > zz[-1]:
+                        zwarn |= BAD_MINFIT
+                        k = np.where(zzchi2 == np.min(zzchi2))[0][0]
+                        zbest = zz[k]
+                        chi2min = zzchi2[k]
+                    if zbest < redshifts[1] or zbest > redshifts[-2]:
+                        zwarn |= Z_FITLIMIT
+                    if zmin < redshifts[1] or zmin > redshifts[-2]:
+                        zwarn |= Z_FITLIMIT
                 if _near_any(zbest, zprev, maxv):
                     continue
                 r = dict(z=zbest, zerr=zerr, zwarn=zwarn, chi2=chi2min, zz=zz, zzchi2=zzchi2,
