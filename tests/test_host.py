@@ -526,3 +526,64 @@ def test_find_minima_definition():
                if (i == 0 or x[i] <= x[i - 1]) and (i == n - 1 or x[i] <= x[i + 1])]
         idx = np.array(idx, dtype=np.int64)
         np.testing.assert_array_equal(find_minima(x), idx[np.argsort(x[idx])])
+
+
+def test_fitz_post_fit_checks_batched(monkeypatch):
+    """fitz_targets applies redrock's checks after each parabola fit
+    (fitz.py:263-280) to whole batches of candidates: every reported
+    minimum equals the scalar sequence -- the parabola through the three
+    fine-grid points around the lowest one, BAD_MINFIT and the grid's
+    first lowest point when the vertex leaves the fine grid, Z_FITLIMIT
+    outside redshifts[1:-1] -- on monotone, constant and regular fine
+    grids (a stand-in for the pair scan, no GPU)."""
+    import numpy as np
+    from redrock_b200 import fitz as F
+
+    class FakeRef:
+        def __init__(self, targets, template, layout=None, rowpack=None):
+            self.oii = None
+            self.src = type("S", (), {"nbasis": template.nbasis})()
+
+        def scan(self, tidx, z):
+            z = np.asarray(z, dtype=np.float64)
+            t = np.asarray(tidx)
+            c = 100 + 1e6 * (z - 0.5 - 0.01 * (t % 7)) ** 2 + 3 * np.sin(z * 3000 + t)
+            c = np.where(t % 13 == 4, 100 + 50 * z, c)
+            return c, np.ones((len(z), self.src.nbasis)), np.zeros(len(z)), np.ones(len(z), bool)
+
+    monkeypatch.setattr(F, "_Refiner", FakeRef)
+
+    class Tg:
+        def __init__(self):
+            self.spectra = [type("Sp", (), {"ivar": np.ones(4)})()]
+
+    class Tm:
+        nbasis, method, igm_model, solve_matrices_algorithm = 10, 'PCA', None, 'PCA'
+        template_type = 'GALAXY'
+
+    zg = np.linspace(-0.005, 1.5, 3311)
+    n = 300
+    chi2 = [100 + 1e3 * (zg - 0.7 - 0.01 * (i % 7)) ** 2 + 50 * np.sin(zg * (200 + i) + i)
+            for i in range(n)]
+    chi2[5][:] = 1e10
+    out = F.fitz_targets(chi2, zg, [Tg() for _ in range(n)], Tm(), nminima=3)
+    checked = 0
+    for res in out:
+        for m in range(len(res['z'])):
+            zz, c2 = res['zz'][m], res['zzchi2'][m]
+            i = min(max(int(np.argmin(c2)), 1), len(zz) - 2)
+            x0, xerr, y0, zw = (float(v[0]) for v in F.minfit_batch(zz[None, i - 1:i + 2],
+                                                                     c2[None, i - 1:i + 2]))
+            zw = int(zw)
+            zbest, chi2min = x0, y0
+            if zbest < zz[0] or zbest > zz[-1]:
+                zw |= F.BAD_MINFIT
+                k = int(np.where(c2 == np.min(c2))[0][0])
+                zbest, chi2min = zz[k], c2[k]
+            if zbest < zg[1] or zbest > zg[-2] or x0 < zg[1] or x0 > zg[-2]:
+                zw |= F.Z_FITLIMIT
+            assert res['z'][m, 0] == zbest and res['chi2'][m, 0] == chi2min
+            assert res['zerr'][m, 0] == xerr and res['zwarn'][m, 0] == zw
+            checked += 1
+    assert checked > 3 * n - 10
+    assert any(res['zwarn'][:, 0].any() for res in out)
