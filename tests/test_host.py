@@ -587,3 +587,17 @@ def test_fitz_post_fit_checks_batched(monkeypatch):
             checked += 1
     assert checked > 3 * n - 10
     assert any(res['zwarn'][:, 0].any() for res in out)
+
+
+def test_pipelined_chunk_bounds():
+    """The pipelined scan's target chunks: one launch for small batches, else
+    a small first chunk and then chunks of the chosen size, covering every
+    target exactly once in order."""
+    from redrock_b200 import zscan
+    assert zscan._chunk_bounds(300, 224) == [(0, 300)]
+    for n, chunk in ((500, 224), (5000, 448), (20000, 448), (449, 224), (4097, 448)):
+        b = zscan._chunk_bounds(n, chunk)
+        assert b[0] == (0, min(zscan.FIRST_CHUNK, chunk))
+        assert b[-1][1] == n
+        assert all(b[i][1] == b[i + 1][0] for i in range(len(b) - 1))
+        assert all(0 < j - i <= chunk for i, j in b)
